@@ -1,0 +1,269 @@
+/*
+ * ORACLE -- test infrastructure only.
+ *
+ * Driver for the reference itself: this file is compiled together with the
+ * reference's own sources (left in place; see oracle/Makefile) into
+ * oracle/_ref/glamer_ref.  It reads one command per line on stdin, runs the
+ * reference code path named by the command and writes raw little-endian
+ * float64 arrays.  Used by tests/ to pin the C restatement (oracle.c) and by
+ * bench.py's reference arm as the CPU baseline.
+ *
+ * Commands (files are raw arrays; particles are 24-byte ParticleType<float>):
+ *   tree PFILE N BUCKET THETA INV_AREA MAX_RANGE PERIODIC INV_SCREEN RFILE NR OUT [EXPORT]
+ *        TreeQuadParticles ctor + force2D_recur at NR rays -> OUT: per ray
+ *        alpha[2] kappa gamma[3] phi.  EXPORT: 16 doubles per branch (preorder).
+ *   nfw MASS RSIZE Z CONC FRATIO PA XFILE N OUT      LensHaloNFW::force_halo
+ *   nsie MASS Z SIGMA RCORE FRATIO PA XFILE N OUT    LensHaloRealNSIE::force_halo
+ *   lens ZSOURCE                                     new Lens (replaces previous)
+ *   particles PFILE N Z INV_AREA MAX_RANGE TX TY     moveinMainHalo(LensHaloParticles, true)
+ *   addnfw MASS RSIZE Z CONC TX TY                   insertMainHalo(LensHaloNFW, true)
+ *   addnsie MASS Z SIGMA RCORE FRATIO PA TX TY       insertMainHalo(LensHaloRealNSIE, true)
+ *   haloforce I XFILE N OUT                          force_halo of the lens's i-th main halo
+ *   planes OUT                                       z, Dl, dDl of every plane (+ source)
+ *   grid N CX CY RANGE OUT TIMEFILE                  GridMap ctor -> per ray y[2] A[4];
+ *                                                    TIMEFILE gets the ctor wall seconds
+ *   rays XFILE N ZFILE OUT TIMEFILE                  rayshooterInternal(N, RAY*) with per-ray z
+ *   points XFILE N OUT TIMEFILE                      rayshooterInternal(N, Point*)
+ */
+#include "slsimlib.h"
+#include "particle_halo.h"
+#include "gridmap.h"
+#include "oracle.h"
+
+#include <chrono>
+#include <cstdio>
+#include <fstream>
+#include <memory>
+#include <sstream>
+#include <string>
+#include <vector>
+
+/* The flat LambdaCDM distances of the oracle, shared with the restatement. */
+double COSMOLOGY::coorDist(double z) const { return orc_coordist(z); }
+double COSMOLOGY::invCoorDist(double d) const { return orc_invcoordist(d); }
+
+typedef ParticleType<float> PT;
+
+template <typename T>
+static std::vector<T> read_arr(const std::string &f, size_t n) {
+  std::vector<T> v(n);
+  if (n == 0) return v;
+  FILE *fp = fopen(f.c_str(), "rb");
+  if (!fp || fread(v.data(), sizeof(T), n, fp) != n) {
+    fprintf(stderr, "glamer_ref: cannot read %s\n", f.c_str());
+    exit(2);
+  }
+  fclose(fp);
+  return v;
+}
+static void write_arr(const std::string &f, const std::vector<double> &v) {
+  FILE *fp = fopen(f.c_str(), "wb");
+  if (!fp) { fprintf(stderr, "glamer_ref: cannot write %s\n", f.c_str()); exit(2); }
+  fwrite(v.data(), sizeof(double), v.size(), fp);
+  fclose(fp);
+}
+static void write_time(const std::string &f, double s) {
+  if (f == "-") return;
+  write_arr(f, std::vector<double>(1, s));
+}
+
+/* Exposes the protected tree for the branch export. */
+struct ExportTree : public TreeQuadParticles<PT> {
+  using TreeQuadParticles<PT>::TreeQuadParticles;
+  void export_branches(std::vector<double> &out) {
+    out.clear();
+    QBranchNB *b = tree->top;
+    while (b) {
+      bool leaf = !b->child0 && !b->child1 && !b->child2 && !b->child3;
+      double w = b->boundary_p2[0] - b->boundary_p1[0];
+      double v[16] = {(double)b->level, b->boundary_p1[0], b->boundary_p1[1], b->boundary_p2[0],
+                      b->boundary_p2[1], (double)b->nparticles, (double)b->Nbig_particles, b->mass,
+                      b->center[0], b->center[1], b->quad[0], b->quad[1], b->quad[2],
+                      b->r2crit_angle, (double)leaf, w * w};
+      out.insert(out.end(), v, v + 16);
+      b = b->child0 ? b->child0 : b->brother;
+    }
+  }
+};
+
+/* The LensHaloRealNSIE constructor resets the mass of a cored halo by 1D
+ * integration (MultiPlane/lens_halos.cpp:1073-1075) before it assigns `units`
+ * (:1077), so that integral reads an indeterminate value.  Repeat the
+ * integration once `units` is set, which is the mass the constructor intends. */
+static void fix_cored_nsie_mass(LensHaloRealNSIE &h, float nominal_mass) {
+  if (h.get_rcore() > 0.0) {
+    h.setMass(nominal_mass);
+    h.setMass(h.MassBy1DIntegation(h.getRsize()));
+  }
+}
+
+int main() {
+  COSMOLOGY cosmo;
+  long seed = 1;
+  std::unique_ptr<Lens> lens;
+  std::string line;
+  while (std::getline(std::cin, line)) {
+    std::istringstream in(line);
+    std::string cmd;
+    if (!(in >> cmd)) continue;
+    if (cmd == "tree") {
+      std::string pf, rf, out, exp;
+      size_t n, nr;
+      int bucket, periodic;
+      double theta, inv_area, max_range, inv_screen;
+      in >> pf >> n >> bucket >> theta >> inv_area >> max_range >> periodic >> inv_screen >> rf >> nr >> out >> exp;
+      std::vector<PT> p = read_arr<PT>(pf, n);
+      std::vector<double> r = read_arr<double>(rf, 2 * nr);
+      ExportTree t(p.data(), n, -1, -1, inv_area, bucket, theta, periodic != 0, inv_screen, max_range);
+      std::vector<double> o(7 * nr);
+      for (size_t i = 0; i < nr; ++i) {
+        double a[2], k, g[3], ph;
+        t.force2D_recur(&r[2 * i], a, &k, g, &ph);
+        double v[7] = {a[0], a[1], k, g[0], g[1], g[2], ph};
+        std::copy(v, v + 7, &o[7 * i]);
+      }
+      write_arr(out, o);
+      if (!exp.empty()) {
+        std::vector<double> e;
+        t.export_branches(e);
+        write_arr(exp, e);
+      }
+    } else if (cmd == "nfw" || cmd == "nsie") {
+      std::unique_ptr<LensHalo> h;
+      std::string xf, out;
+      size_t n;
+      if (cmd == "nfw") {
+        float mass, rsize, conc, fratio, pa;
+        double z;
+        in >> mass >> rsize >> z >> conc >> fratio >> pa >> xf >> n >> out;
+        h.reset(new LensHaloNFW(mass, rsize, z, conc, fratio, pa, cosmo));
+      } else {
+        float mass, sigma, rcore, fratio, pa;
+        double z;
+        in >> mass >> z >> sigma >> rcore >> fratio >> pa >> xf >> n >> out;
+        LensHaloRealNSIE *nh = new LensHaloRealNSIE(mass, z, sigma, rcore, fratio, pa, cosmo);
+        fix_cored_nsie_mass(*nh, mass);
+        h.reset(nh);
+      }
+      std::vector<double> x = read_arr<double>(xf, 2 * n), o(7 * n + 3);
+      for (size_t i = 0; i < n; ++i) {
+        double a[2] = {0, 0}, k = 0, g[3] = {0, 0, 0}, ph = 0;
+        h->force_halo(a, &k, g, &ph, &x[2 * i]);
+        double v[7] = {a[0], a[1], k, g[0], g[1], g[2], ph};
+        std::copy(v, v + 7, &o[7 * i]);
+      }
+      o[7 * n] = h->get_mass();
+      o[7 * n + 1] = h->getRsize();
+      o[7 * n + 2] = h->get_Rmax();
+      write_arr(out, o);
+    } else if (cmd == "lens") {
+      double zs;
+      in >> zs;
+      lens.reset(new Lens(&seed, zs, cosmo));
+    } else if (cmd == "particles") {
+      std::string pf;
+      size_t n;
+      double z, inv_area, max_range, tx, ty;
+      in >> pf >> n >> z >> inv_area >> max_range >> tx >> ty;
+      std::vector<PT> p = read_arr<PT>(pf, n);
+      LensHaloParticles<PT> h(p, (float)z, cosmo, Point_2d(0, 0), false, inv_area, 0, max_range);
+      h.setTheta(tx, ty);
+      lens->moveinMainHalo(h, true);
+    } else if (cmd == "addnfw") {
+      float mass, rsize, conc;
+      double z, tx, ty;
+      in >> mass >> rsize >> z >> conc >> tx >> ty;
+      LensHaloNFW h(mass, rsize, z, conc, 1.0f, 0.0f, cosmo);
+      h.setTheta(tx, ty);
+      lens->insertMainHalo(h, true);
+    } else if (cmd == "addnsie") {
+      float mass, sigma, rcore, fratio, pa;
+      double z, tx, ty;
+      in >> mass >> z >> sigma >> rcore >> fratio >> pa >> tx >> ty;
+      LensHaloRealNSIE h(mass, z, sigma, rcore, fratio, pa, cosmo);
+      fix_cored_nsie_mass(h, mass);
+      h.setTheta(tx, ty);
+      lens->insertMainHalo(h, true);
+    } else if (cmd == "haloforce") {
+      /* force_halo of the lens's i-th main halo at physical positions */
+      std::string xf, out;
+      size_t i, n;
+      in >> i >> xf >> n >> out;
+      std::vector<double> x = read_arr<double>(xf, 2 * n), o(7 * n);
+      LensHalo *h = lens->getMainHalo(i);
+      for (size_t k = 0; k < n; ++k) {
+        double a[2] = {0, 0}, kk = 0, g[3] = {0, 0, 0}, ph = 0;
+        h->force_halo(a, &kk, g, &ph, &x[2 * k]);
+        double v[7] = {a[0], a[1], kk, g[0], g[1], g[2], ph};
+        std::copy(v, v + 7, &o[7 * k]);
+      }
+      write_arr(out, o);
+    } else if (cmd == "planes") {
+      std::string out;
+      in >> out;
+      std::vector<double> o;
+      /* z, Dl and dDl are protected; rebuild them from the public accessors */
+      int np = lens->getNplanes();
+      std::vector<PosType> zz = lens->get_plane_redshifts();
+      o.push_back(np);
+      for (auto z : zz) o.push_back(z);
+      write_arr(out, o);
+    } else if (cmd == "grid") {
+      size_t N;
+      double c[2], range;
+      std::string out, tf;
+      in >> N >> c[0] >> c[1] >> range >> out >> tf;
+      auto t0 = std::chrono::steady_clock::now();
+      GridMap gm(lens.get(), N, c, range);
+      double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      std::vector<double> o(6 * N * N);
+      for (size_t i = 0; i < N * N; ++i) {
+        RAY r = gm.ray(i);
+        double v[6] = {r.y[0], r.y[1], r.A.a[0], r.A.a[1], r.A.a[2], r.A.a[3]};
+        std::copy(v, v + 6, &o[6 * i]);
+      }
+      write_arr(out, o);
+      write_time(tf, secs);
+    } else if (cmd == "rays" || cmd == "points") {
+      std::string xf, zf, out, tf;
+      size_t n;
+      if (cmd == "rays") in >> xf >> n >> zf >> out >> tf;
+      else in >> xf >> n >> out >> tf;
+      std::vector<double> x = read_arr<double>(xf, 2 * n), o(6 * n);
+      double secs;
+      if (cmd == "rays") {
+        std::vector<double> z = read_arr<double>(zf, n);
+        std::vector<RAY> rays(n);
+        for (size_t i = 0; i < n; ++i) { rays[i].x[0] = x[2 * i]; rays[i].x[1] = x[2 * i + 1]; rays[i].z = z[i]; }
+        auto t0 = std::chrono::steady_clock::now();
+        lens->rayshooterInternal(n, rays.data());
+        secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        for (size_t i = 0; i < n; ++i) {
+          double v[6] = {rays[i].y[0], rays[i].y[1], rays[i].A.a[0], rays[i].A.a[1], rays[i].A.a[2], rays[i].A.a[3]};
+          std::copy(v, v + 6, &o[6 * i]);
+        }
+      } else {
+        std::vector<Point> ip(n), sp(n);
+        for (size_t i = 0; i < n; ++i) {
+          ip[i].x[0] = x[2 * i]; ip[i].x[1] = x[2 * i + 1];
+          ip[i].image = &sp[i]; sp[i].image = &ip[i];
+        }
+        auto t0 = std::chrono::steady_clock::now();
+        lens->rayshooterInternal(n, ip.data());
+        secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        for (size_t i = 0; i < n; ++i) {
+          double v[6] = {sp[i].x[0], sp[i].x[1], ip[i].A.a[0], ip[i].A.a[1], ip[i].A.a[2], ip[i].A.a[3]};
+          std::copy(v, v + 6, &o[6 * i]);
+        }
+      }
+      write_arr(out, o);
+      write_time(tf, secs);
+    } else {
+      fprintf(stderr, "glamer_ref: unknown command %s\n", cmd.c_str());
+      return 2;
+    }
+    printf("ok\n");
+    fflush(stdout);
+  }
+  return 0;
+}

@@ -1,0 +1,301 @@
+"""Test-side access to the oracle (oracle/liboracle.so) and to the reference
+driver (oracle/_ref/glamer_ref).  Test infrastructure only: the product
+library never imports this module."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import tempfile
+from typing import Optional
+
+import numpy as np
+
+from slsimlib_b200 import synth
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+ORACLE_SO = os.path.join(ORACLE_DIR, "liboracle.so")
+REF_BIN = os.path.join(ORACLE_DIR, "_ref", "glamer_ref")
+
+_dp = C.POINTER(C.c_double)
+_vp = C.c_void_p
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(_vp)
+
+
+_lib = None
+
+
+def oracle_lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(ORACLE_SO):
+        subprocess.check_call(["make", "-s", "-C", ORACLE_DIR, "liboracle.so"])
+    L = C.CDLL(ORACLE_SO)
+    L.orc_coordist.restype = C.c_double
+    L.orc_coordist.argtypes = [C.c_double]
+    L.orc_angdist.restype = C.c_double
+    L.orc_angdist.argtypes = [C.c_double]
+    L.orc_tree_build.restype = _vp
+    L.orc_tree_build.argtypes = [_vp, C.c_size_t, C.c_float, C.c_float, C.c_double, C.c_int,
+                                 C.c_double, C.c_int, C.c_double, C.c_double, C.POINTER(C.c_int)]
+    L.orc_tree_free.argtypes = [_vp]
+    L.orc_tree_force2D_recur.argtypes = [_vp, _vp, _vp, _vp, _vp, _vp]
+    L.orc_direct_sum.argtypes = [_vp, C.c_size_t, C.c_double, _vp, _vp, _vp, _vp, _vp]
+    L.orc_tree_nbranches.restype = C.c_size_t
+    L.orc_tree_nbranches.argtypes = [_vp]
+    L.orc_tree_export.argtypes = [_vp, _vp]
+    L.orc_tree_membership.argtypes = [_vp, _vp]
+    L.orc_halo_nfw.restype = _vp
+    L.orc_halo_nfw.argtypes = [C.c_float, C.c_float, C.c_double, C.c_float, C.c_float, C.c_float]
+    L.orc_halo_nsie.restype = _vp
+    L.orc_halo_nsie.argtypes = [C.c_float, C.c_double, C.c_float, C.c_float, C.c_float, C.c_float]
+    L.orc_halo_particles.restype = _vp
+    L.orc_halo_particles.argtypes = [_vp, C.c_size_t, C.c_double, C.c_double, C.c_double]
+    L.orc_halo_set_theta.argtypes = [_vp, C.c_double, C.c_double]
+    L.orc_halo_free.argtypes = [_vp]
+    for f in ("orc_halo_mass", "orc_halo_rsize", "orc_halo_rmax"):
+        getattr(L, f).restype = C.c_float
+        getattr(L, f).argtypes = [_vp]
+    L.orc_halo_force.argtypes = [_vp, C.c_size_t, _vp, _vp, _vp, _vp, _vp]
+    L.orc_lens_create.restype = _vp
+    L.orc_lens_create.argtypes = [C.c_double]
+    L.orc_lens_free.argtypes = [_vp]
+    L.orc_lens_add_halo.argtypes = [_vp, _vp, C.c_int]
+    L.orc_lens_nplanes.restype = C.c_int
+    L.orc_lens_nplanes.argtypes = [_vp]
+    L.orc_lens_planes.argtypes = [_vp, _vp, _vp, _vp]
+    L.orc_lens_reset_source.restype = C.c_int
+    L.orc_lens_reset_source.argtypes = [_vp, C.c_double, C.c_int]
+    L.orc_lens_rayshoot.argtypes = [_vp, C.c_size_t, _vp, _vp, _vp, _vp, C.c_int]
+    L.orc_lens_plane_force.argtypes = [_vp, C.c_int, C.c_size_t, _vp, _vp, _vp, _vp, _vp]
+    L.orc_grid_positions.argtypes = [C.c_size_t, _vp, C.c_double, _vp]
+    _lib = L
+    return L
+
+
+# ----------------------------------------------------------------- trees
+class OracleTree:
+    def __init__(self, particles: np.ndarray, bucket=5, theta=0.1, inv_area=0.0,
+                 periodic=False, inv_screening=0.0, max_range=-1.0):
+        L = oracle_lib()
+        self.p = np.ascontiguousarray(particles)
+        err = C.c_int(0)
+        self.h = L.orc_tree_build(_ptr(self.p), len(self.p), -1.0, -1.0, inv_area, bucket, theta,
+                                  int(periodic), inv_screening, max_range, C.byref(err))
+        if not self.h:
+            raise ValueError("particles in same place.")
+
+    def force(self, rays: np.ndarray) -> np.ndarray:
+        """(n,7): alpha[2], kappa, gamma[3], phi from force2D_recur."""
+        L = oracle_lib()
+        rays = np.ascontiguousarray(rays, dtype=np.float64).reshape(-1, 2)
+        out = np.zeros((len(rays), 7))
+        a = np.zeros(2); k = np.zeros(1); g = np.zeros(3); ph = np.zeros(1)
+        for i in range(len(rays)):
+            r = np.ascontiguousarray(rays[i])
+            L.orc_tree_force2D_recur(self.h, _ptr(r), _ptr(a), _ptr(k), _ptr(g), _ptr(ph))
+            out[i, :2] = a; out[i, 2] = k[0]; out[i, 3:6] = g; out[i, 6] = ph[0]
+        return out
+
+    def export(self) -> np.ndarray:
+        L = oracle_lib()
+        n = L.orc_tree_nbranches(self.h)
+        out = np.zeros((n, 16))
+        L.orc_tree_export(self.h, _ptr(out))
+        return out
+
+    def membership(self) -> np.ndarray:
+        L = oracle_lib()
+        n = L.orc_tree_nbranches(self.h)
+        out = np.zeros((n, 2))
+        L.orc_tree_membership(self.h, _ptr(out))
+        return out
+
+    def __del__(self):
+        try:
+            oracle_lib().orc_tree_free(self.h)
+        except Exception:
+            pass
+
+
+def direct_sum(particles: np.ndarray, rays: np.ndarray, inv_area=0.0) -> np.ndarray:
+    L = oracle_lib()
+    p = np.ascontiguousarray(particles)
+    rays = np.ascontiguousarray(rays, dtype=np.float64).reshape(-1, 2)
+    out = np.zeros((len(rays), 7))
+    a = np.zeros(2); k = np.zeros(1); g = np.zeros(3); ph = np.zeros(1)
+    for i in range(len(rays)):
+        r = np.ascontiguousarray(rays[i])
+        L.orc_direct_sum(_ptr(p), len(p), inv_area, _ptr(r), _ptr(a), _ptr(k), _ptr(g), _ptr(ph))
+        out[i, :2] = a; out[i, 2] = k[0]; out[i, 3:6] = g; out[i, 6] = ph[0]
+    return out
+
+
+# ----------------------------------------------------------------- halos
+def _make_halo(h):
+    L = oracle_lib()
+    if isinstance(h, synth.ParticlePlane):
+        p = np.ascontiguousarray(h.particles)
+        ptr = L.orc_halo_particles(_ptr(p), len(p), h.z, h.inv_area, h.max_range)
+    elif isinstance(h, synth.NSIEHalo):
+        ptr = L.orc_halo_nsie(h.mass, h.z, h.sigma, h.rcore, h.fratio, h.pa)
+    elif isinstance(h, synth.NFWHalo):
+        ptr = L.orc_halo_nfw(h.mass, h.rsize, h.z, h.conc, 1.0, 0.0)
+    else:
+        raise TypeError(h)
+    L.orc_halo_set_theta(ptr, h.theta[0], h.theta[1])
+    return ptr
+
+
+def oracle_halo_force(h, xcm: np.ndarray) -> np.ndarray:
+    """(n,7) force_halo outputs for one halo at positions xcm (physical Mpc)."""
+    L = oracle_lib()
+    ptr = _make_halo(h)
+    xcm = np.ascontiguousarray(xcm, dtype=np.float64).reshape(-1, 2)
+    n = len(xcm)
+    a = np.zeros((n, 2)); k = np.zeros(n); g = np.zeros((n, 3)); ph = np.zeros(n)
+    L.orc_halo_force(ptr, n, _ptr(xcm), _ptr(a), _ptr(k), _ptr(g), _ptr(ph))
+    params = (L.orc_halo_mass(ptr), L.orc_halo_rsize(ptr), L.orc_halo_rmax(ptr))
+    L.orc_halo_free(ptr)
+    return np.concatenate([a, k[:, None], g, ph[:, None]], axis=1), params
+
+
+class OracleLens:
+    def __init__(self, spec: synth.LensSpec):
+        L = oracle_lib()
+        self.h = L.orc_lens_create(spec.zsource)
+        for halo in spec.halos:
+            L.orc_lens_add_halo(self.h, _make_halo(halo), 1)
+
+    def planes(self):
+        L = oracle_lib()
+        n = L.orc_lens_nplanes(self.h)
+        z = np.zeros(n + 1); Dl = np.zeros(n + 1); dDl = np.zeros(n + 1)
+        L.orc_lens_planes(self.h, _ptr(z), _ptr(Dl), _ptr(dDl))
+        return z, Dl, dDl
+
+    def reset_source(self, z, nearest=False):
+        return oracle_lib().orc_lens_reset_source(self.h, z, int(nearest))
+
+    def rayshoot(self, x: np.ndarray, zs: Optional[np.ndarray] = None, threads=0):
+        """y (n,2), A (n,4) from Lens::rayshooterInternal."""
+        L = oracle_lib()
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1, 2)
+        n = len(x)
+        y = np.zeros((n, 2)); A = np.zeros((n, 4))
+        zsp = None
+        if zs is not None:
+            zs = np.ascontiguousarray(zs, dtype=np.float64)
+            zsp = _ptr(zs)
+        L.orc_lens_rayshoot(self.h, n, _ptr(x), zsp, _ptr(y), _ptr(A), threads)
+        return y, A
+
+    def plane_force(self, j: int, xx: np.ndarray) -> np.ndarray:
+        L = oracle_lib()
+        xx = np.ascontiguousarray(xx, dtype=np.float64).reshape(-1, 2)
+        n = len(xx)
+        a = np.zeros((n, 2)); k = np.zeros(n); g = np.zeros((n, 3)); ph = np.zeros(n)
+        L.orc_lens_plane_force(self.h, j, n, _ptr(xx), _ptr(a), _ptr(k), _ptr(g), _ptr(ph))
+        return np.concatenate([a, k[:, None], g, ph[:, None]], axis=1)
+
+    def __del__(self):
+        try:
+            oracle_lib().orc_lens_free(self.h)
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------- reference driver
+def ref_available() -> bool:
+    return os.path.exists(REF_BIN)
+
+
+class RefDriver:
+    """Runs commands against the reference compiled in place (oracle/_ref)."""
+
+    def __init__(self):
+        self.tmp = tempfile.mkdtemp(prefix="glamer_ref_")
+        self.lines = []
+        self.k = 0
+
+    def _file(self, arr: Optional[np.ndarray] = None) -> str:
+        self.k += 1
+        f = os.path.join(self.tmp, f"a{self.k}.bin")
+        if arr is not None:
+            np.ascontiguousarray(arr).tofile(f)
+        return f
+
+    def run(self, lines, timeout=3600):
+        script = "\n".join(lines) + "\n"
+        r = subprocess.run([REF_BIN], input=script.encode(), stdout=subprocess.PIPE,
+                           stderr=subprocess.PIPE, timeout=timeout)
+        if r.returncode != 0:
+            raise RuntimeError(f"glamer_ref failed: {r.stderr.decode()[-2000:]}")
+
+    def tree_force(self, particles, rays, bucket=5, theta=0.1, inv_area=0.0, max_range=-1.0,
+                   periodic=False, inv_screening=0.0, export=False):
+        pf = self._file(particles)
+        rays = np.ascontiguousarray(rays, dtype=np.float64).reshape(-1, 2)
+        rf = self._file(rays)
+        of = self._file()
+        ef = self._file() if export else ""
+        self.run([f"tree {pf} {len(particles)} {bucket} {theta!r} {inv_area!r} {max_range!r} "
+                  f"{int(periodic)} {inv_screening!r} {rf} {len(rays)} {of} {ef}"])
+        out = np.fromfile(of).reshape(-1, 7)
+        if export:
+            return out, np.fromfile(ef).reshape(-1, 16)
+        return out
+
+    def halo_force(self, h, xcm):
+        xcm = np.ascontiguousarray(xcm, dtype=np.float64).reshape(-1, 2)
+        xf = self._file(xcm)
+        of = self._file()
+        if isinstance(h, synth.NFWHalo):
+            cmd = f"nfw {h.mass!r} {h.rsize!r} {h.z!r} {h.conc!r} 1 0 {xf} {len(xcm)} {of}"
+        else:
+            cmd = (f"nsie {h.mass!r} {h.z!r} {h.sigma!r} {h.rcore!r} {h.fratio!r} {h.pa!r} "
+                   f"{xf} {len(xcm)} {of}")
+        self.run([cmd])
+        o = np.fromfile(of)
+        return o[:-3].reshape(-1, 7), tuple(o[-3:])
+
+    def lens_lines(self, spec: synth.LensSpec):
+        lines = [f"lens {spec.zsource!r}"]
+        for h in spec.halos:
+            if isinstance(h, synth.ParticlePlane):
+                pf = self._file(h.particles)
+                lines.append(f"particles {pf} {len(h.particles)} {h.z!r} {h.inv_area!r} "
+                             f"{h.max_range!r} {h.theta[0]!r} {h.theta[1]!r}")
+            elif isinstance(h, synth.NSIEHalo):
+                lines.append(f"addnsie {h.mass!r} {h.z!r} {h.sigma!r} {h.rcore!r} {h.fratio!r} "
+                             f"{h.pa!r} {h.theta[0]!r} {h.theta[1]!r}")
+            elif isinstance(h, synth.NFWHalo):
+                lines.append(f"addnfw {h.mass!r} {h.rsize!r} {h.z!r} {h.conc!r} "
+                             f"{h.theta[0]!r} {h.theta[1]!r}")
+        return lines
+
+    def grid(self, spec, n1d, center=(0.0, 0.0), range_rad=30 * synth.ARCSEC):
+        of = self._file()
+        tf = self._file()
+        self.run(self.lens_lines(spec) + [f"grid {n1d} {center[0]!r} {center[1]!r} {range_rad!r} {of} {tf}"])
+        o = np.fromfile(of).reshape(-1, 6)
+        return o[:, :2], o[:, 2:], float(np.fromfile(tf)[0])
+
+    def rays(self, spec, x, zs=None):
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1, 2)
+        xf = self._file(x)
+        of = self._file()
+        tf = self._file()
+        if zs is None:
+            cmd = f"points {xf} {len(x)} {of} {tf}"
+        else:
+            zf = self._file(np.ascontiguousarray(zs, dtype=np.float64))
+            cmd = f"rays {xf} {len(x)} {zf} {of} {tf}"
+        self.run(self.lens_lines(spec) + [cmd])
+        o = np.fromfile(of).reshape(-1, 6)
+        return o[:, :2], o[:, 2:], float(np.fromfile(tf)[0])
