@@ -19,6 +19,7 @@
  *   addnfw MASS RSIZE Z CONC TX TY                   insertMainHalo(LensHaloNFW, true)
  *   addnsie MASS Z SIGMA RCORE FRATIO PA TX TY       insertMainHalo(LensHaloRealNSIE, true)
  *   haloforce I XFILE N OUT                          force_halo of the lens's i-th main halo
+ *   threads OUT                                      Utilities::GetNThreads()
  *   planes OUT                                       z, Dl, dDl of every plane (+ source)
  *   grid N CX CY RANGE OUT TIMEFILE                  GridMap ctor -> per ray y[2] A[4];
  *                                                    TIMEFILE gets the ctor wall seconds
@@ -198,6 +199,11 @@ int main() {
         std::copy(v, v + 7, &o[7 * k]);
       }
       write_arr(out, o);
+    } else if (cmd == "threads") {
+      /* the thread count Lens::rayshooterInternal uses (utilities.cpp:553) */
+      std::string out;
+      in >> out;
+      write_arr(out, std::vector<double>(1, (double)Utilities::GetNThreads()));
     } else if (cmd == "planes") {
       std::string out;
       in >> out;

@@ -1,1 +1,379 @@
-"""B200-native GLAMER ray-shooting path."""
+"""B200-native ray shooting for GLAMER / SLsimLib lenses.
+
+Python mirror of the reference's interface for the ray-shooting path, over the
+C ABI of ``libglamer_b200.so`` (include/glamer_b200.h).  Class and method
+names follow the reference:
+
+* ``TreeQuadParticles(particles, ...)`` / ``force2D_recur(rays)``
+  (include/quadTree.h:49-68, 932-987);
+* ``LensHaloParticles``, ``LensHaloNFW``, ``LensHaloRealNSIE`` with
+  ``force_halo(xcm)`` and ``setTheta`` (include/particle_halo.h,
+  include/lens_halos.h);
+* ``Lens(zsource)`` with ``insertMainHalo`` / ``moveinMainHalo``,
+  ``ResetSourcePlane`` and ``rayshooterInternal`` (include/lens.h);
+* ``GridMap(lens, N, center, range)`` (include/gridmap.h:35).
+
+There is no CPU path: without a CUDA device every call raises
+``GlamerError`` (status GLB_ERR_NO_DEVICE).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+from .synth import PARTICLE_DTYPE
+
+__all__ = [
+    "GlamerError", "load_library", "TreeQuadParticles", "LensHaloParticles", "LensHaloNFW",
+    "LensHaloRealNSIE", "Lens", "GridMap", "PREC_FP64", "PREC_SPLIT", "PARTICLE_DTYPE",
+]
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libglamer_b200.so")
+
+PREC_FP64 = 0
+PREC_SPLIT = 1
+
+GLB_ERR_ARG = -1
+GLB_ERR_CUDA = -2
+GLB_ERR_OOM = -3
+GLB_ERR_SAME_PLACE = -4
+GLB_ERR_DEPTH = -5
+GLB_ERR_UNSUPPORTED = -6
+GLB_ERR_NO_DEVICE = -7
+
+# every symbol include/glamer_b200.h declares
+EXPORTED = [
+    "glb_last_error", "glb_version", "glb_set_option",
+    "glb_tree_create", "glb_tree_destroy", "glb_tree_force2D_recur", "glb_tree_export", "glb_tree_build_ms",
+    "glb_halo_particles", "glb_halo_nfw", "glb_halo_nsie", "glb_halo_set_theta", "glb_halo_force",
+    "glb_halo_params", "glb_halo_destroy",
+    "glb_lens_create", "glb_lens_destroy", "glb_lens_insert_halo", "glb_lens_nplanes", "glb_lens_planes",
+    "glb_lens_reset_source", "glb_lens_rayshoot", "glb_lens_rayshoot_device", "glb_gridmap",
+    "glb_lens_last_timing", "glb_lens_count_interactions",
+]
+
+
+class GlamerError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+_vp = C.c_void_p
+_lib = None
+
+
+def load_library():
+    """Loads libglamer_b200.so (built in-tree by slsimlib_b200.build)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise GlamerError(GLB_ERR_NO_DEVICE,
+                          f"{LIB_PATH} is missing: run `python -m slsimlib_b200.build` first")
+    L = C.CDLL(LIB_PATH)
+    L.glb_last_error.restype = C.c_char_p
+    L.glb_version.restype = C.c_char_p
+    L.glb_set_option.argtypes = [C.c_int, C.c_longlong]
+    L.glb_tree_create.argtypes = [_vp, C.c_size_t, C.c_float, C.c_float, C.c_double, C.c_int, C.c_double,
+                                  C.c_int, C.c_double, C.c_double, C.POINTER(_vp)]
+    L.glb_tree_destroy.argtypes = [_vp]
+    L.glb_tree_force2D_recur.argtypes = [_vp, C.c_size_t, _vp, _vp, _vp, _vp, _vp]
+    L.glb_tree_export.argtypes = [_vp, C.POINTER(C.c_size_t), _vp]
+    L.glb_tree_build_ms.argtypes = [_vp, C.POINTER(C.c_double)]
+    L.glb_halo_particles.argtypes = [_vp, C.c_size_t, C.c_double, C.c_double, C.c_double, C.POINTER(_vp)]
+    L.glb_halo_nfw.argtypes = [C.c_float, C.c_float, C.c_double, C.c_float, C.c_float, C.c_float, C.POINTER(_vp)]
+    L.glb_halo_nsie.argtypes = [C.c_float, C.c_double, C.c_float, C.c_float, C.c_float, C.c_float,
+                                C.POINTER(_vp)]
+    L.glb_halo_set_theta.argtypes = [_vp, C.c_double, C.c_double]
+    L.glb_halo_force.argtypes = [_vp, C.c_size_t, _vp, _vp, _vp, _vp, _vp]
+    L.glb_halo_params.argtypes = [_vp, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)]
+    L.glb_halo_destroy.argtypes = [_vp]
+    L.glb_lens_create.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, C.POINTER(_vp)]
+    L.glb_lens_destroy.argtypes = [_vp]
+    L.glb_lens_insert_halo.argtypes = [_vp, _vp, C.c_int]
+    L.glb_lens_nplanes.argtypes = [_vp, C.POINTER(C.c_int)]
+    L.glb_lens_planes.argtypes = [_vp, _vp, _vp, _vp]
+    L.glb_lens_reset_source.argtypes = [_vp, C.c_double, C.c_int, C.POINTER(C.c_int)]
+    L.glb_lens_rayshoot.argtypes = [_vp, C.c_size_t, _vp, _vp, _vp, _vp, C.c_int]
+    L.glb_lens_rayshoot_device.argtypes = [_vp, C.c_size_t, _vp, _vp, _vp, _vp, C.c_int, _vp]
+    L.glb_gridmap.argtypes = [_vp, C.c_size_t, _vp, C.c_double, _vp, _vp, C.c_int]
+    L.glb_lens_last_timing.argtypes = [_vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.glb_lens_count_interactions.argtypes = [_vp, C.c_size_t, _vp, _vp, _vp]
+    _lib = L
+    return L
+
+
+def _check(rc: int):
+    if rc != 0:
+        raise GlamerError(rc, load_library().glb_last_error().decode())
+
+
+def _p(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(_vp)
+
+
+def _f64(a, shape=None) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    return a if shape is None else a.reshape(shape)
+
+
+def _particles(p) -> np.ndarray:
+    p = np.ascontiguousarray(p)
+    if p.dtype != PARTICLE_DTYPE:
+        raise TypeError("particles must be a ParticleType<float> record array (slsimlib_b200.PARTICLE_DTYPE)")
+    return p
+
+
+def _forces(n):
+    return (np.zeros((n, 2)), np.zeros(n), np.zeros((n, 3)), np.zeros(n))
+
+
+# ------------------------------------------------------------------- trees
+class TreeQuadParticles:
+    """TreeQuadParticles<ParticleType<float>> (include/quadTree.h:49-60)."""
+
+    def __init__(self, particles, mass_fixed=-1.0, size_fixed=-1.0, inv_area=0.0, bucket=5, theta_force=0.1,
+                 periodic_buffer=False, inv_screening_scale=0.0, maximum_range=-1.0, keep_export=False):
+        L = load_library()
+        p = _particles(particles)
+        h = _vp()
+        if keep_export:
+            _check(L.glb_set_option(1, 1))
+        try:
+            _check(L.glb_tree_create(_p(p), len(p), mass_fixed, size_fixed, inv_area, bucket, theta_force,
+                                     int(periodic_buffer), inv_screening_scale, maximum_range, C.byref(h)))
+        finally:
+            if keep_export:
+                L.glb_set_option(1, 0)
+        self._h = h
+
+    def force2D_recur(self, rays):
+        """alpha (n,2), kappa (n,), gamma (n,3), phi (n,) at rays (n,2) in physical Mpc."""
+        r = _f64(rays, (-1, 2))
+        a, k, g, ph = _forces(len(r))
+        _check(load_library().glb_tree_force2D_recur(self._h, len(r), _p(r), _p(a), _p(k), _p(g), _p(ph)))
+        return a, k, g, ph
+
+    def export(self) -> np.ndarray:
+        L = load_library()
+        nb = C.c_size_t(0)
+        _check(L.glb_tree_export(self._h, C.byref(nb), None))
+        out = np.zeros((nb.value, 16))
+        _check(L.glb_tree_export(self._h, C.byref(nb), _p(out)))
+        return out
+
+    def build_ms(self) -> float:
+        v = C.c_double(0)
+        _check(load_library().glb_tree_build_ms(self._h, C.byref(v)))
+        return v.value
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            load_library().glb_tree_destroy(self._h)
+            self._h = None
+
+
+# ------------------------------------------------------------------- halos
+class _Halo:
+    """Common part of the halo classes: a description that can create the
+    C-side halo (Lens.insertMainHalo copies, as the reference does)."""
+
+    theta = (0.0, 0.0)
+
+    def setTheta(self, tx, ty=None):
+        if ty is None:
+            tx, ty = tx
+        self.theta = (float(tx), float(ty))
+
+    def _create(self):
+        raise NotImplementedError
+
+    def _make(self):
+        h = self._create()
+        _check(load_library().glb_halo_set_theta(h, self.theta[0], self.theta[1]))
+        return h
+
+    def force_halo(self, xcm):
+        """LensHalo::force_halo at positions xcm (n,2) relative to the halo
+        centre, physical Mpc: alpha (n,2), kappa, gamma (n,3), phi."""
+        L = load_library()
+        x = _f64(xcm, (-1, 2))
+        h = self._make()
+        try:
+            a, k, g, ph = _forces(len(x))
+            _check(L.glb_halo_force(h, len(x), _p(x), _p(a), _p(k), _p(g), _p(ph)))
+            return a, k, g, ph
+        finally:
+            L.glb_halo_destroy(h)
+
+    def params(self):
+        L = load_library()
+        h = self._make()
+        try:
+            m, rs, rm = C.c_float(), C.c_float(), C.c_float()
+            _check(L.glb_halo_params(h, C.byref(m), C.byref(rs), C.byref(rm)))
+            return m.value, rs.value, rm.value
+        finally:
+            L.glb_halo_destroy(h)
+
+
+class LensHaloParticles(_Halo):
+    """LensHaloParticles(std::vector<ParticleType<float>>&, float redshift,
+    cosmo, Point_2d(0,0), recenter=false, inv_area, MinPSize=0, max_range)
+    (include/particle_halo.h:58-75)."""
+
+    def __init__(self, particles, redshift, inv_area=0.0, max_range=-1.0):
+        self.particles = _particles(particles)
+        self.z = float(redshift)
+        self.inv_area = float(inv_area)
+        self.max_range = float(max_range)
+
+    def _create(self):
+        h = _vp()
+        _check(load_library().glb_halo_particles(_p(self.particles), len(self.particles), self.z, self.inv_area,
+                                                 self.max_range, C.byref(h)))
+        return h
+
+
+class LensHaloNFW(_Halo):
+    """LensHaloNFW(float mass, float Rsize, z, float concentration, float fratio,
+    float pa, cosmo) (MultiPlane/lens_halos.cpp:389-431)."""
+
+    def __init__(self, mass, Rsize, zlens, concentration, fratio=1.0, pa=0.0):
+        self.args = (float(mass), float(Rsize), float(zlens), float(concentration), float(fratio), float(pa))
+
+    def _create(self):
+        h = _vp()
+        m, r, z, c, f, pa = self.args
+        _check(load_library().glb_halo_nfw(m, r, z, c, f, pa, C.byref(h)))
+        return h
+
+
+class LensHaloRealNSIE(_Halo):
+    """LensHaloRealNSIE(float mass, z, float sigma, float rcore, float fratio,
+    float pa, cosmo) (MultiPlane/lens_halos.cpp:1043-1078)."""
+
+    def __init__(self, mass, zlens, sigma, rcore, fratio, pa):
+        self.args = (float(mass), float(zlens), float(sigma), float(rcore), float(fratio), float(pa))
+
+    def _create(self):
+        h = _vp()
+        _check(load_library().glb_halo_nsie(*self.args, C.byref(h)))
+        return h
+
+
+# -------------------------------------------------------------------- lens
+class Lens:
+    """Lens(long *seed, z_source, COSMOLOGY) (MultiPlane/lens.cpp:59-77) for a
+    flat LambdaCDM cosmology."""
+
+    def __init__(self, zsource, omega_m=0.3, omega_l=0.7, hubble=0.7):
+        L = load_library()
+        h = _vp()
+        _check(L.glb_lens_create(float(zsource), omega_m, omega_l, hubble, C.byref(h)))
+        self._h = h
+
+    def insertMainHalo(self, halo: _Halo, addplanes: bool = True):
+        """Lens::insertMainHalo / moveinMainHalo (include/lens.h:149-185)."""
+        _check(load_library().glb_lens_insert_halo(self._h, halo._make(), int(addplanes)))
+
+    moveinMainHalo = insertMainHalo
+
+    def getNplanes(self) -> int:
+        n = C.c_int(0)
+        _check(load_library().glb_lens_nplanes(self._h, C.byref(n)))
+        return n.value
+
+    def planes(self):
+        n = self.getNplanes()
+        z, Dl, dDl = np.zeros(n + 1), np.zeros(n + 1), np.zeros(n + 1)
+        _check(load_library().glb_lens_planes(self._h, _p(z), _p(Dl), _p(dDl)))
+        return z, Dl, dDl
+
+    def ResetSourcePlane(self, z, nearest=False) -> int:
+        j = C.c_int(0)
+        _check(load_library().glb_lens_reset_source(self._h, float(z), int(nearest), C.byref(j)))
+        return j.value
+
+    def rayshooterInternal(self, x, source_zs=None, precision=PREC_FP64):
+        """x (n,2) image-plane angles (radians) -> y (n,2) source-plane angles,
+        A (n,4) Jacobian.  source_zs: one source redshift per ray (the
+        LinkedPoint / RAY overloads), or None for the lens's source plane."""
+        x = _f64(x, (-1, 2))
+        n = len(x)
+        zs = None
+        if source_zs is not None:
+            zs = _f64(source_zs)
+            if len(zs) != n:
+                raise ValueError("missing redshifts")  # internal_rayshooter_multi.cpp:130-133
+        y = np.zeros((n, 2))
+        A = np.zeros((n, 4))
+        _check(load_library().glb_lens_rayshoot(self._h, n, _p(x), _p(zs), _p(y), _p(A), precision))
+        return y, A
+
+    def rayshoot_device(self, n, x_ptr, zs_ptr, y_ptr, A_ptr, precision=PREC_FP64, stream=None):
+        """Device-buffer form (raw CUDA pointers)."""
+        _check(load_library().glb_lens_rayshoot_device(self._h, n, x_ptr, zs_ptr, y_ptr, A_ptr, precision,
+                                                       stream))
+
+    def count_interactions(self, x, source_zs=None) -> np.ndarray:
+        """Interaction counts (nodes tested, far cells, leaf point masses,
+        big-particle checks, B-splines) summed over rays and planes."""
+        x = _f64(x, (-1, 2))
+        zs = None if source_zs is None else _f64(source_zs)
+        out = np.zeros(5, dtype=np.uint64)
+        _check(load_library().glb_lens_count_interactions(self._h, len(x), _p(x), _p(zs), _p(out)))
+        return out
+
+    def last_timing(self):
+        k, t = C.c_double(0), C.c_double(0)
+        _check(load_library().glb_lens_last_timing(self._h, C.byref(k), C.byref(t)))
+        return k.value, t.value
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            load_library().glb_lens_destroy(self._h)
+            self._h = None
+
+
+class GridMap:
+    """GridMap(LensHndl, N1d, center, range) (TreeCode_link/gridmap.cpp:93-120):
+    an N1d x N1d grid, x fastest, shot through the lens on construction."""
+
+    def __init__(self, lens: Lens, N1d: int, center: Sequence[float], range_: float, precision=PREC_FP64):
+        self.N = int(N1d)
+        self.center = np.ascontiguousarray(center, dtype=np.float64)
+        self.range = float(range_)
+        n = self.N * self.N
+        self.y = np.zeros((n, 2))
+        self.A = np.zeros((n, 4))
+        _check(load_library().glb_gridmap(lens._h, self.N, _p(self.center), self.range, _p(self.y), _p(self.A),
+                                          precision))
+
+    def positions(self) -> np.ndarray:
+        from .synth import grid_positions
+        return grid_positions(self.N, tuple(self.center), self.range)
+
+    # LensingVariable outputs of GridMap::writePixelMap (include/gridmap.h:532-600)
+    def kappa(self):
+        return 1 - (self.A[:, 0] + self.A[:, 3]) / 2
+
+    def gamma1(self):
+        return (self.A[:, 0] - self.A[:, 3]) / 2
+
+    def gamma2(self):
+        return (self.A[:, 1] + self.A[:, 2]) / 2
+
+    def gamma3(self):
+        return (self.A[:, 2] - self.A[:, 1]) / 2
+
+    def invmag(self):
+        return self.A[:, 0] * self.A[:, 3] - self.A[:, 1] * self.A[:, 2]
+
+    def alpha(self):
+        return self.positions() - self.y

@@ -1,0 +1,89 @@
+// Host-side objects behind the C ABI (include/glamer_b200.h).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "glb_internal.h"
+
+struct glb_particle_rec {
+  float x[3];
+  float Mass;
+  float Size;
+  int type;
+};
+static_assert(sizeof(glb_particle_rec) == 24, "ParticleType<float> is 24 bytes");
+
+namespace glb {
+
+// Error status carried through the C ABI.
+struct Status {
+  int code = 0;
+  std::string msg;
+  static Status ok() { return Status(); }
+  static Status err(int c, const std::string &m) {
+    Status s;
+    s.code = c;
+    s.msg = m;
+    return s;
+  }
+  bool good() const { return code == 0; }
+};
+
+// Device memory owned by RAII.
+template <typename T>
+struct DBuf {
+  T *p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  DBuf(const DBuf &) = delete;
+  DBuf &operator=(const DBuf &) = delete;
+  ~DBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  cudaError_t alloc(size_t count) {
+    release();
+    n = count;
+    if (count == 0) return cudaSuccess;
+    return cudaMalloc((void **)&p, count * sizeof(T));
+  }
+};
+
+// TreeQuadParticles built on the device.
+struct Tree {
+  TreeDev dev{};
+  DBuf<GNode> nodes;
+  DBuf<GNodeF> nodesf;
+  DBuf<float4> parts;
+  DBuf<float4> prel;
+  DBuf<float4> bigs;
+  int nnodes = 0;
+  size_t nparticles = 0;
+  size_t nbranches = 0;            // including empty children (reference count)
+  std::vector<double> export_rows; // 16 doubles per branch when requested
+  float build_ms = 0;
+};
+
+struct TreeParams {
+  float mass_fixed = -1, size_fixed = -1;
+  double inv_area = 0;
+  int bucket = 5;
+  double theta = 0.1;
+  int periodic = 0;
+  double inv_screening = 0;
+  double max_range = -1;
+};
+
+// Builds a tree from host particle records (ParticleType<float>).
+Status build_tree(const glb_particle_rec *host_particles, size_t n, const TreeParams &prm,
+                  bool want_export, cudaStream_t stream, std::unique_ptr<Tree> &out);
+
+// Global options.
+extern int g_keep_tree_export;
+
+}  // namespace glb

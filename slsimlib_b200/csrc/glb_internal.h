@@ -1,0 +1,102 @@
+// Device-side data layout of the ray-shooting path.
+//
+// Tree nodes are stored in depth-first (preorder) order with empty children
+// removed, so a walk is a forward scan: opening a node moves to node + 1,
+// accepting or leaving it jumps to `skip` (first node after its subtree).
+// Leaf particles sit contiguously in key order; "big" particles of internal
+// nodes (those whose softening exceeds half the node width,
+// include/quadTree.h:403-431) are copied into a separate contiguous list.
+#pragma once
+#include <stddef.h>
+#include <stdint.h>
+
+#include "cosmology.h"
+
+namespace glb {
+
+constexpr double kPi = 3.14159265358979323846;  // include/standard.h:39 (M_PI)
+constexpr double kGrav = 4.7788e-20;              // include/standard.h:43
+constexpr double kLightspeed = 2.99792458e5;      // km/s
+constexpr int kMaxDepth = 32;                     // 2-bit Morton digits in a 64-bit key
+
+// One tree node (preorder, non-empty).  96 bytes.
+struct __align__(16) GNode {
+  double cx, cy;   // centre of |m|-weighted mass (quadTree.h:591-598)
+  double open2;    // max(r2crit_angle, 5.83 boxsize^2): open when rcm2cell < open2
+  double near2;    // 5.83 boxsize^2: big particles are tested when rcm2cell < near2
+  double mass;     // signed mass
+  double q0, q1, q2;  // quadrupole about the centre of mass (quadTree.h:602-612)
+  double width;    // x-extent of the box (leaf big-particle test, quadTree.h:386)
+  int skip;        // preorder index of the first node after this subtree
+  int leaf;        // 1 for a leaf
+  int pstart, pcount;  // leaf: range in the sorted particle array
+  int bstart, bcount;  // internal: range in the big-particle array
+};
+
+// FP32 companion of a node for the split-precision walk: positions are kept
+// in FP64 (cx, cy of GNode); everything else is rounded to FP32.
+struct __align__(16) GNodeF {
+  float open2, near2, mass, q0;
+  float q1, q2, width, pad;
+};
+
+struct TreeDev {
+  const GNode *nodes;
+  const GNodeF *nodesf;
+  const float4 *parts;  // sorted particles {x, y, mass, size}
+  const float4 *bigs;   // big-particle list of internal nodes
+  const float4 *prel;   // sorted particles relative to their leaf's centre of mass (FP32)
+  int nnodes;
+  int nparticles;
+  double inv_area;
+  double screen2;       // inv_screening_scale^2
+  int periodic;
+  double period_x, period_y;  // original (unsquared) bbox lengths
+  // mass and quadrupole of the last branch of the reference's moments walk,
+  // read by its far-field potential (quadTree.h:1103-1104)
+  double phi_mass, phi_q0, phi_q1, phi_q2;
+  double phiintconst;
+};
+
+enum HaloKind { HALO_PARTICLES = 0, HALO_NFW = 1, HALO_NSIE = 2 };
+
+struct NFWDev {
+  double mass, rscale, gmax, Rmax2;  // Rmax2: float(Rmax*Rmax) as the reference compares
+  double phi_const;                  // 0.25*h(Rsize/rscale)/gmax - log(Rsize) terms
+  double h_xmax;
+  double log_rsize;
+};
+
+struct NSIEDev {
+  double mass, Rsize, Rmax, Rsize2, Rmax2, units;
+  double f, bc, sqrt_f, fp;
+  double c1, s1;    // cos/sin(pa)      (rotation into the halo frame)
+  double c2, s2;    // cos/sin(-pa)     (deflection back)
+  double c3, s3;    // cos/sin(-2 pa)   (shear back)
+  double c0, s0;    // cos/sin(0)
+  double dRmaxRsize;  // float(Rmax - Rsize)
+};
+
+struct HaloDev {
+  int kind;
+  double px, py;  // posHalo * Dist (physical Mpc), LensHalo::getX
+  TreeDev tree;
+  NFWDev nfw;
+  NSIEDev nsie;
+};
+
+// One lens plane of the combined list, with the scalars of the recursion
+// (include/lens.h:1003-1066) precomputed on the host in the reference's
+// operation order.
+struct PlaneDev {
+  double Dphys;  // Dl[j] / (1 + z_j)
+  double Gfac;   // charge * Dl[j] / (1 + z_j)
+  double aa, bb; // dDl[j+1]/Dl[j+1], Dl[j]/Dl[j+1] (j < last)
+  int halo0, nhalo;
+};
+
+struct NFWTables {
+  const double *x, *f, *g, *g2, *h;
+};
+
+}  // namespace glb

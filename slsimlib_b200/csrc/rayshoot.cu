@@ -1,0 +1,1207 @@
+// Multi-plane ray shooting on the GPU and the C ABI (include/glamer_b200.h).
+//
+// Lens::rayshooterInternal (FullRange/internal_rayshooter_multi.cpp:53-235)
+// hands chunks of rays to std::threads that each run
+// Lens::compute_points_parallel (include/lens.h:913-1103): for every ray,
+// every plane: LensPlaneSingular::force (MultiPlane/planes.cpp:114-161) over
+// the plane's halos, then the position / Jacobian recursion.  Here every
+// plane is one kernel launch over all rays (rays sorted along a Morton curve
+// so that a warp holds neighbouring rays and walks the tree together); the
+// per-ray recursion state (theta, SumPrevAlphas, A, SumPrevAG: 12 doubles)
+// stays in HBM between planes.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/glamer_b200.h"
+#include "glb_host.h"
+#include "halos.cuh"
+#include "walk.cuh"
+#include "walk_split.cuh"
+
+using namespace glb;
+
+// ===================================================================== errors
+static thread_local std::string t_err;
+static int fail(int code, const std::string &m) {
+  t_err = m;
+  return code;
+}
+static int fail(const Status &s) { return fail(s.code, s.msg); }
+
+#define CKR(call)                                                                              \
+  do {                                                                                         \
+    cudaError_t e_ = (call);                                                                   \
+    if (e_ != cudaSuccess)                                                                     \
+      return fail(e_ == cudaErrorMemoryAllocation ? GLB_ERR_OOM : GLB_ERR_CUDA,                \
+                  std::string("CUDA: ") + cudaGetErrorString(e_) + " at " #call);              \
+  } while (0)
+
+static int need_device() {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0)
+    return fail(GLB_ERR_NO_DEVICE, "no CUDA device: the B200 ray-shooting library has no CPU path");
+  return 0;
+}
+
+// ================================================================ NFW tables
+namespace {
+struct HostNFWTables {
+  std::vector<double> x, f, g, g2, h;
+};
+std::once_flag g_nfw_host_once;
+HostNFWTables g_nfw_host;
+
+// LensHaloNFW::make_tables, MultiPlane/lens_halos.cpp:482-508.
+void make_host_tables() {
+  HostNFWTables &T = g_nfw_host;
+  T.x.resize(kNfwTable);
+  T.f.resize(kNfwTable);
+  T.g.resize(kNfwTable);
+  T.g2.resize(kNfwTable);
+  T.h.resize(kNfwTable);
+  double dx = kNfwMaxRm / (double)kNfwTable;
+  for (int i = 0; i < kNfwTable; i++) {
+    double x = i * dx;
+    T.x[i] = x;
+    T.f[i] = nfw_f(x);
+    T.g[i] = nfw_g(x);
+    T.g2[i] = nfw_g2(x);
+    T.h[i] = nfw_h(x);
+  }
+}
+
+// InterpolateFromTable (lens_halos.cpp:566-580) on the host, for set-up values.
+double nfw_interp_host(int which, double y) {
+  const HostNFWTables &T = g_nfw_host;
+  int j = (int)(y / kNfwMaxRm * kNfwTable);
+  if (j == 0) {
+    switch (which) {
+      case 0: return nfw_f(y);
+      case 1: return nfw_g(y);
+      case 2: return nfw_g2(y);
+      default: return nfw_h(y);
+    }
+  }
+  const std::vector<double> &t = which == 0 ? T.f : which == 1 ? T.g : which == 2 ? T.g2 : T.h;
+  return (t[j + 1] - t[j]) / (T.x[j + 1] - T.x[j]) * (y - T.x[j]) + t[j];
+}
+
+// Device copies, one set per device.
+struct DevNFWTables {
+  double *x = nullptr, *f = nullptr, *g = nullptr, *g2 = nullptr, *h = nullptr;
+};
+std::mutex g_dev_nfw_mu;
+DevNFWTables g_dev_nfw[64];
+
+int device_nfw_tables(NFWTables &out) {
+  std::call_once(g_nfw_host_once, make_host_tables);
+  int dev = 0;
+  CKR(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(g_dev_nfw_mu);
+  DevNFWTables &D = g_dev_nfw[dev & 63];
+  if (!D.x) {
+    double **dst[5] = {&D.x, &D.f, &D.g, &D.g2, &D.h};
+    const std::vector<double> *src[5] = {&g_nfw_host.x, &g_nfw_host.f, &g_nfw_host.g, &g_nfw_host.g2,
+                                         &g_nfw_host.h};
+    for (int i = 0; i < 5; ++i) {
+      CKR(cudaMalloc((void **)dst[i], kNfwTable * sizeof(double)));
+      CKR(cudaMemcpy(*dst[i], src[i]->data(), kNfwTable * sizeof(double), cudaMemcpyHostToDevice));
+    }
+  }
+  out.x = D.x;
+  out.f = D.f;
+  out.g = D.g;
+  out.g2 = D.g2;
+  out.h = D.h;
+  return 0;
+}
+}  // namespace
+
+// ===================================================================== halos
+struct glb_halo {
+  int kind = HALO_PARTICLES;
+  double theta[2] = {0, 0};  // posHalo (radians)
+  double zlens = 0;
+  double Dist = 0;  // angular-size distance used by LensHalo::getX
+  // LensHalo float members (include/lens_halos.h:279-356)
+  float mass = 0, Rsize = 0, Rmax = 0, rscale = 1;
+  NFWDev nfw{};
+  NSIEDev nsie{};
+  std::unique_ptr<Tree> tree;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+};
+
+// ====================================================================== lens
+struct PlaneHost {
+  double z, Dl;
+  std::vector<glb_halo *> halos;
+};
+
+struct glb_lens {
+  Cosmo cosmo{0.3, 0.7, 0.7};
+  double zsource = 0;
+  double charge = 0;
+  std::vector<std::unique_ptr<glb_halo>> owned;
+  std::vector<PlaneHost> main;  // sorted by Dl
+  std::vector<double> plane_z, Dl, dDl;  // combined, source pseudo-plane last
+  bool toggle_source_plane = false;
+  double zs_implant = 0;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  // device copies of the plane / halo descriptors
+  bool dirty = true;
+  DBuf<PlaneDev> d_planes;
+  DBuf<HaloDev> d_halos;
+  DBuf<double> d_planez, d_Dl;
+  // rayshoot workspace
+  DBuf<double> st;          // 12 n recursion state
+  DBuf<double> io;          // host-call staging: x 2n, zs n, y 2n, A 4n
+  DBuf<int> jmax_ray;
+  DBuf<double> src_ray;     // Dls/Ds, D/Ds per ray
+  DBuf<unsigned> keys, keys2, perm0, perm;
+  DBuf<char> sort_tmp;
+  DBuf<unsigned long long> bbox;
+  size_t ws_n = 0;
+  float last_kernel_ms = 0, last_total_ms = 0;
+};
+
+// ================================================================== kernels
+namespace {
+
+__device__ inline unsigned long long d2ord(double d) {
+  unsigned long long b = (unsigned long long)__double_as_longlong(d);
+  return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
+}
+__device__ inline double ord2d(unsigned long long u) {
+  unsigned long long b = (u & 0x8000000000000000ull) ? (u & 0x7fffffffffffffffull) : ~u;
+  return __longlong_as_double((long long)b);
+}
+
+__global__ void k_ray_bbox(const double *x, size_t n, unsigned long long *bb) {
+  unsigned long long mnx = ~0ull, mny = ~0ull, mxx = 0, mxy = 0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    unsigned long long ux = d2ord(x[2 * i]), uy = d2ord(x[2 * i + 1]);
+    mnx = min(mnx, ux);
+    mny = min(mny, uy);
+    mxx = max(mxx, ux);
+    mxy = max(mxy, uy);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    mnx = min(mnx, __shfl_xor_sync(kFull, mnx, o));
+    mny = min(mny, __shfl_xor_sync(kFull, mny, o));
+    mxx = max(mxx, __shfl_xor_sync(kFull, mxx, o));
+    mxy = max(mxy, __shfl_xor_sync(kFull, mxy, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(bb + 0, mnx);
+    atomicMin(bb + 1, mny);
+    atomicMax(bb + 2, mxx);
+    atomicMax(bb + 3, mxy);
+  }
+}
+
+__device__ inline unsigned spread16(unsigned v) {
+  v &= 0xffffu;
+  v = (v | (v << 8)) & 0x00ff00ffu;
+  v = (v | (v << 4)) & 0x0f0f0f0fu;
+  v = (v | (v << 2)) & 0x33333333u;
+  v = (v | (v << 1)) & 0x55555555u;
+  return v;
+}
+
+__global__ void k_ray_morton(const double *x, size_t n, const unsigned long long *bb, unsigned *keys,
+                             unsigned *idx) {
+  size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double x0 = ord2d(bb[0]), y0 = ord2d(bb[1]), x1 = ord2d(bb[2]), y1 = ord2d(bb[3]);
+  double sx = x1 > x0 ? 65535.0 / (x1 - x0) : 0.0, sy = y1 > y0 ? 65535.0 / (y1 - y0) : 0.0;
+  double fx = (x[2 * i] - x0) * sx, fy = (x[2 * i + 1] - y0) * sy;
+  unsigned qx = (unsigned)fmin(fmax(fx, 0.0), 65535.0), qy = (unsigned)fmin(fmax(fy, 0.0), 65535.0);
+  keys[i] = spread16(qx) | (spread16(qy) << 1);
+  idx[i] = (unsigned)i;
+}
+
+__global__ void k_identity(unsigned *p, size_t n) {
+  size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i < n) p[i] = (unsigned)i;
+}
+
+struct SrcArgs {
+  Cosmo cosmo;
+  const double *planez;  // np + 1
+  const double *Dl;      // np + 1
+  int np;
+};
+
+// Lens::FindSourcePlane (MultiPlane/lens.cpp:2659-2680) for one ray.
+__device__ inline void find_source_plane(const SrcArgs &s, double zs, int &jmax, double &dls_ds, double &d_ds) {
+  double Ds = coordist(s.cosmo, zs), Dls;
+  if (zs <= s.planez[0]) {
+    jmax = 0;
+    Dls = Ds;
+  } else {
+    jmax = s.np;
+    if (jmax <= 0) {
+      Dls = Ds;
+    } else {
+      while (s.planez[jmax - 1] > zs) --jmax;
+      Dls = coordist2(s.cosmo, s.planez[jmax - 1], zs);
+    }
+  }
+  dls_ds = Dls / Ds;
+  d_ds = jmax > 0 ? s.Dl[jmax - 1] / Ds : 0.0;
+}
+
+// State layout: st[c * n + k], c = 0..11:
+//   theta0 theta1 | SumPrevAlphas0 1 | A0..A3 | SumPrevAG0..3
+__global__ void k_init_state(const double *x, const double *zs, const unsigned *perm, size_t n, double *st,
+                             int *jmax_ray, double *src_ray, SrcArgs s) {
+  size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  unsigned i = perm[k];
+  double t0 = x[2 * i], t1 = x[2 * i + 1];
+  st[0 * n + k] = t0;
+  st[1 * n + k] = t1;
+  st[2 * n + k] = t0;
+  st[3 * n + k] = t1;
+  st[4 * n + k] = 1;
+  st[5 * n + k] = 0;
+  st[6 * n + k] = 0;
+  st[7 * n + k] = 1;
+  st[8 * n + k] = 1;
+  st[9 * n + k] = 0;
+  st[10 * n + k] = 0;
+  st[11 * n + k] = 1;
+  if (zs) {
+    int jm;
+    double a, b;
+    find_source_plane(s, zs[i], jm, a, b);
+    jmax_ray[k] = jm;
+    src_ray[2 * k] = a;
+    src_ray[2 * k + 1] = b;
+  }
+}
+
+__global__ void k_finish(const double *st, const unsigned *perm, size_t n, double *y, double *A) {
+  size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  unsigned i = perm[k];
+  y[2 * i] = st[0 * n + k];
+  y[2 * i + 1] = st[1 * n + k];
+  A[4 * i] = st[4 * n + k];
+  A[4 * i + 1] = st[5 * n + k];
+  A[4 * i + 2] = st[6 * n + k];
+  A[4 * i + 3] = st[7 * n + k];
+}
+
+__global__ void k_identity_rays(const double *x, size_t n, double *y, double *A) {
+  size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  y[2 * i] = x[2 * i];
+  y[2 * i + 1] = x[2 * i + 1];
+  A[4 * i] = 1;
+  A[4 * i + 1] = 0;
+  A[4 * i + 2] = 0;
+  A[4 * i + 3] = 1;
+}
+
+// xygridpoints + PositionFromIndex (TreeCode_link/gridmap.cpp:293-321,
+// TreeCode_link/utilities.cpp:149-158), x fastest.
+__global__ void k_grid(size_t N1d, double c0, double c1, double range, double *x) {
+  size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= N1d * N1d) return;
+  if (N1d == 1) {
+    x[0] = c0;
+    x[1] = c1;
+    return;
+  }
+  x[2 * i] = c0 + range * (1.0 * (double)(i % N1d) / (double)(N1d - 1) - 0.5);
+  x[2 * i + 1] = c1 + range * (1.0 * (double)(i / N1d) / (double)(N1d - 1) - 0.5);
+}
+
+template <int PREC, bool PHI, bool COUNT = false>
+__device__ __forceinline__ void particle_halo_acc(const TreeDev &T, double rx, double ry, bool valid, double *acc,
+                                                  WalkCount *wc = nullptr) {
+  if (T.periodic) {
+    // force2D_recur with a periodic buffer: nine shifted copies (quadTree.h:944-974)
+    for (int i = -1; i < 2; ++i)
+      for (int j = -1; j < 2; ++j) {
+        if (PREC == GLB_PREC_FP64)
+          walk_f64<PHI, COUNT>(T, rx + i * T.period_x, ry + j * T.period_y, valid, acc, wc);
+        else
+          walk_split(T, rx + i * T.period_x, ry + j * T.period_y, valid, acc);
+      }
+  } else {
+    if (PREC == GLB_PREC_FP64)
+      walk_f64<PHI, COUNT>(T, rx, ry, valid, acc, wc);
+    else
+      walk_split(T, rx, ry, valid, acc);
+  }
+}
+
+struct StepArgs {
+  const PlaneDev *planes;
+  const HaloDev *halos;
+  NFWTables tab;
+  double *st;
+  size_t n;
+  int j;
+  int jmax;             // uniform source plane
+  double dls_ds, d_ds;  // uniform source plane
+  const int *jmax_ray;  // per-ray source planes (or null)
+  const double *src_ray;
+  double charge;
+  unsigned long long *counts;  // V F P B S totals (counting launches only)
+};
+
+// One lens plane for every ray: LensPlaneSingular::force + the recursion of
+// include/lens.h:1003-1066.
+template <int PREC, bool COUNT = false>
+__global__ void __launch_bounds__(128) k_plane_step(StepArgs a) {
+  const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  const bool inrange = k < a.n;
+  const size_t n = a.n;
+  int jmax = a.jmax;
+  double dls = a.dls_ds, dds = a.d_ds;
+  if (a.jmax_ray && inrange) {
+    jmax = a.jmax_ray[k];
+    dls = a.src_ray[2 * k];
+    dds = a.src_ray[2 * k + 1];
+  }
+  const bool valid = inrange && a.j < jmax;
+  if (!__any_sync(kFull, valid)) return;
+  double *st = a.st;
+  double th0 = 0, th1 = 0;
+  if (valid) {
+    th0 = st[0 * n + k];
+    th1 = st[1 * n + k];
+  }
+  const PlaneDev P = a.planes[a.j];
+  const double xx0 = th0 * P.Dphys, xx1 = th1 * P.Dphys;
+  double al0 = 0, al1 = 0, kap = 0, g0 = 0, g1 = 0;
+  for (int h = 0; h < P.nhalo; ++h) {
+    const HaloDev *H = a.halos + P.halo0 + h;
+    const int kind = H->kind;
+    const double xc0 = xx0 - H->px, xc1 = xx1 - H->py;
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    if (kind == HALO_PARTICLES) {
+      if (COUNT) {
+        WalkCount wc;
+        particle_halo_acc<PREC, false, true>(H->tree, xc0, xc1, valid, acc, &wc);
+        unsigned long long v[5] = {wc.V, wc.F, wc.P, wc.B, wc.S};
+        for (int c = 0; c < 5; ++c) {
+          for (int o = 16; o > 0; o >>= 1) v[c] += __shfl_xor_sync(kFull, v[c], o);
+          if ((threadIdx.x & 31) == 0) atomicAdd(a.counts + c, v[c]);
+        }
+      } else {
+        particle_halo_acc<PREC, false>(H->tree, xc0, xc1, valid, acc);
+      }
+      // LensHaloParticles::force_halo negates alpha (particle_halo.h:432-433)
+      acc[0] = -acc[0];
+      acc[1] = -acc[1];
+    } else if (valid) {
+      if (kind == HALO_NFW)
+        nfw_force<false>(H->nfw, a.tab, xc0, xc1, acc);
+      else
+        nsie_force<false>(H->nsie, xc0, xc1, acc);
+    }
+    al0 -= acc[0];
+    al1 -= acc[1];
+    kap += acc[2];
+    g0 += acc[3];
+    g1 += acc[4];
+  }
+  if (!valid) return;
+  double G0 = kap + g0, G1 = g1, G2 = g1, G3 = kap - g0;
+  G0 *= P.Gfac;
+  G1 *= P.Gfac;
+  G2 *= P.Gfac;
+  G3 *= P.Gfac;
+  double sa0 = st[2 * n + k] - a.charge * al0;
+  double sa1 = st[3 * n + k] - a.charge * al1;
+  double aa, bb;
+  if (a.j < jmax - 1) {
+    aa = P.aa;
+    bb = P.bb;
+  } else {
+    aa = dls;
+    bb = dds;
+  }
+  th0 = bb * th0 + aa * sa0;
+  th1 = bb * th1 + aa * sa1;
+  const double A0 = st[4 * n + k], A1 = st[5 * n + k], A2 = st[6 * n + k], A3 = st[7 * n + k];
+  double s0 = st[8 * n + k], s1 = st[9 * n + k], s2 = st[10 * n + k], s3 = st[11 * n + k];
+  // SumPrevAG -= G * A (Matrix2x2 product, include/point.h:249-258)
+  s0 -= G0 * A0 + G1 * A2;
+  s1 -= G0 * A1 + G1 * A3;
+  s2 -= G2 * A0 + G3 * A2;
+  s3 -= G2 * A1 + G3 * A3;
+  st[0 * n + k] = th0;
+  st[1 * n + k] = th1;
+  st[2 * n + k] = sa0;
+  st[3 * n + k] = sa1;
+  st[4 * n + k] = A0 * bb + s0 * aa;
+  st[5 * n + k] = A1 * bb + s1 * aa;
+  st[6 * n + k] = A2 * bb + s2 * aa;
+  st[7 * n + k] = A3 * bb + s3 * aa;
+  st[8 * n + k] = s0;
+  st[9 * n + k] = s1;
+  st[10 * n + k] = s2;
+  st[11 * n + k] = s3;
+}
+
+// force2D_recur / force_halo at arbitrary positions (walk-level API, with phi).
+__global__ void __launch_bounds__(128) k_halo_force(HaloDev H, NFWTables tab, size_t n, const double *x,
+                                                    double *out) {
+  const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  const bool valid = k < n;
+  if (!__any_sync(kFull, valid)) return;
+  double x0 = 0, x1 = 0;
+  if (valid) {
+    x0 = x[2 * k];
+    x1 = x[2 * k + 1];
+  }
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  if (H.kind == HALO_PARTICLES) {
+    particle_halo_acc<GLB_PREC_FP64, true>(H.tree, x0, x1, valid, acc);
+  } else if (valid) {
+    if (H.kind == HALO_NFW)
+      nfw_force<true>(H.nfw, tab, x0, x1, acc);
+    else
+      nsie_force<true>(H.nsie, x0, x1, acc);
+  }
+  if (!valid) return;
+  for (int c = 0; c < 6; ++c) out[6 * k + c] = acc[c];
+}
+
+inline int nblk(size_t n, int t) { return (int)((n + t - 1) / t); }
+
+}  // namespace
+
+// ================================================================ host side
+namespace {
+
+HaloDev make_halo_dev(const glb_halo &h) {
+  HaloDev d;
+  memset(&d, 0, sizeof(d));
+  d.kind = h.kind;
+  d.px = h.theta[0] * h.Dist;  // LensHalo::getX (include/lens_halos.h:95-99)
+  d.py = h.theta[1] * h.Dist;
+  if (h.tree) d.tree = h.tree->dev;
+  d.nfw = h.nfw;
+  d.nsie = h.nsie;
+  return d;
+}
+
+int set_dev(int device) {
+  CKR(cudaSetDevice(device));
+  return 0;
+}
+
+// Lens::combinePlanes (MultiPlane/lens.cpp:2397-2515) without field planes.
+void combine_planes(glb_lens *l) {
+  size_t n = l->main.size();
+  l->plane_z.assign(n + 1, 0);
+  l->Dl.assign(n + 1, 0);
+  l->dDl.assign(n + 1, 0);
+  for (size_t i = 0; i < n; ++i) l->Dl[i] = l->main[i].Dl;
+  for (size_t i = 1; i < n; ++i)
+    if ((l->Dl[i] - l->Dl[i - 1]) < 1e-6) l->Dl[i] = l->Dl[i - 1] + 1e-6;  // MIN_PLANE_DIST
+  for (size_t i = 0; i < n; ++i) l->plane_z[i] = l->main[i].z;
+  if (n > 0 && l->zsource <= l->plane_z[n - 1]) l->zsource = l->plane_z[n - 1] + 0.1;
+  l->plane_z[n] = l->zsource;
+  l->Dl[n] = coordist2(l->cosmo, 0, l->zsource);
+  l->dDl[0] = l->Dl[0];
+  for (size_t i = 1; i <= n; ++i) l->dDl[i] = l->Dl[i] - l->Dl[i - 1];
+  l->dirty = true;
+}
+
+int upload_lens(glb_lens *l) {
+  if (!l->dirty) return 0;
+  size_t np = l->main.size();
+  std::vector<PlaneDev> P(np);
+  std::vector<HaloDev> H;
+  for (size_t j = 0; j < np; ++j) {
+    PlaneDev &p = P[j];
+    p.Dphys = l->Dl[j] / (1 + l->plane_z[j]);
+    p.Gfac = l->charge * l->Dl[j] / (1 + l->plane_z[j]);
+    p.aa = l->dDl[j + 1] / l->Dl[j + 1];
+    p.bb = l->Dl[j] / l->Dl[j + 1];
+    p.halo0 = (int)H.size();
+    p.nhalo = (int)l->main[j].halos.size();
+    for (glb_halo *h : l->main[j].halos) H.push_back(make_halo_dev(*h));
+  }
+  CKR(l->d_planes.alloc(std::max<size_t>(np, 1)));
+  CKR(l->d_halos.alloc(std::max<size_t>(H.size(), 1)));
+  CKR(l->d_planez.alloc(np + 1));
+  CKR(l->d_Dl.alloc(np + 1));
+  if (np) CKR(cudaMemcpyAsync(l->d_planes.p, P.data(), np * sizeof(PlaneDev), cudaMemcpyHostToDevice, l->stream));
+  if (!H.empty())
+    CKR(cudaMemcpyAsync(l->d_halos.p, H.data(), H.size() * sizeof(HaloDev), cudaMemcpyHostToDevice, l->stream));
+  CKR(cudaMemcpyAsync(l->d_planez.p, l->plane_z.data(), (np + 1) * sizeof(double), cudaMemcpyHostToDevice,
+                      l->stream));
+  CKR(cudaMemcpyAsync(l->d_Dl.p, l->Dl.data(), (np + 1) * sizeof(double), cudaMemcpyHostToDevice, l->stream));
+  CKR(cudaStreamSynchronize(l->stream));
+  l->dirty = false;
+  return 0;
+}
+
+int ensure_ws(glb_lens *l, size_t n, bool per_ray) {
+  if (n > 0xffffffffull) return fail(GLB_ERR_ARG, "too many rays in one call (max 2^32-1)");
+  if (l->ws_n < n || (per_ray && l->jmax_ray.n < n)) {
+    size_t m = std::max(n, l->ws_n);
+    CKR(l->st.alloc(12 * m));
+    CKR(l->keys.alloc(m));
+    CKR(l->keys2.alloc(m));
+    CKR(l->perm0.alloc(m));
+    CKR(l->perm.alloc(m));
+    CKR(l->jmax_ray.alloc(m));
+    CKR(l->src_ray.alloc(2 * m));
+    size_t tb = 0;
+    CKR(cub::DeviceRadixSort::SortPairs(nullptr, tb, l->keys.p, l->keys2.p, l->perm0.p, l->perm.p, (int)m, 0, 32,
+                                        l->stream));
+    CKR(l->sort_tmp.alloc(tb));
+    CKR(l->bbox.alloc(4));
+    l->ws_n = m;
+  }
+  return 0;
+}
+
+// The whole ray-shooting pass on device buffers, enqueued on stream s.
+int rayshoot_device(glb_lens *l, size_t n, const double *x, const double *zs, double *y, double *A,
+                    int precision, cudaStream_t s, unsigned long long *d_counts = nullptr) {
+  if (n == 0) return 0;
+  size_t np = l->main.size();
+  if (np == 0) {  // no lens plane (internal_rayshooter_multi.cpp:62-76)
+    k_identity_rays<<<nblk(n, 256), 256, 0, s>>>(x, n, y, A);
+    CKR(cudaGetLastError());
+    return 0;
+  }
+  if (int rc = upload_lens(l)) return rc;
+  if (int rc = ensure_ws(l, n, zs != nullptr)) return rc;
+  CKR(cudaEventRecord(l->ev[0], s));
+  // spatial ordering of the rays along a Morton curve
+  if (n >= 64) {
+    unsigned long long init[4] = {~0ull, ~0ull, 0ull, 0ull};
+    CKR(cudaMemcpyAsync(l->bbox.p, init, sizeof(init), cudaMemcpyHostToDevice, s));
+    k_ray_bbox<<<std::min(nblk(n, 256), 1184), 256, 0, s>>>(x, n, l->bbox.p);
+    k_ray_morton<<<nblk(n, 256), 256, 0, s>>>(x, n, l->bbox.p, l->keys.p, l->perm0.p);
+    size_t tb = l->sort_tmp.n;
+    CKR(cub::DeviceRadixSort::SortPairs(l->sort_tmp.p, tb, l->keys.p, l->keys2.p, l->perm0.p, l->perm.p, (int)n, 0,
+                                        32, s));
+  } else {
+    k_identity<<<nblk(n, 256), 256, 0, s>>>(l->perm.p, n);
+  }
+  SrcArgs sa{l->cosmo, l->d_planez.p, l->d_Dl.p, (int)np};
+  k_init_state<<<nblk(n, 256), 256, 0, s>>>(x, zs, l->perm.p, n, l->st.p, l->jmax_ray.p, l->src_ray.p, sa);
+
+  StepArgs a;
+  a.planes = l->d_planes.p;
+  a.halos = l->d_halos.p;
+  if (int rc = device_nfw_tables(a.tab)) return rc;
+  a.st = l->st.p;
+  a.n = n;
+  a.charge = l->charge;
+  a.counts = d_counts;
+  a.jmax_ray = zs ? l->jmax_ray.p : nullptr;
+  a.src_ray = zs ? l->src_ray.p : nullptr;
+  int jmax_launch = (int)np;
+  a.jmax = (int)np;
+  a.dls_ds = 0;
+  a.d_ds = 0;
+  if (!zs) {
+    // Point* overload: compute_points_parallel's !multiZs branch (lens.h:944-955)
+    double source_z = l->toggle_source_plane ? l->zs_implant : l->plane_z.back();
+    if (source_z == l->plane_z.back()) {
+      a.dls_ds = l->dDl.back() / l->Dl.back();
+      a.d_ds = l->Dl[np - 1] / l->Dl.back();
+    } else {
+      double Ds = coordist(l->cosmo, source_z), Dls;
+      int jm;
+      if (source_z <= l->plane_z[0]) {
+        jm = 0;
+        Dls = Ds;
+      } else {
+        jm = (int)np;
+        while (l->plane_z[jm - 1] > source_z) --jm;
+        Dls = coordist2(l->cosmo, l->plane_z[jm - 1], source_z);
+      }
+      a.jmax = jm;
+      a.dls_ds = Dls / Ds;
+      if (jm > 0) a.d_ds = l->Dl[jm - 1] / Ds;
+      jmax_launch = jm;
+    }
+  }
+  CKR(cudaEventRecord(l->ev[1], s));
+  for (int j = 0; j < jmax_launch; ++j) {
+    a.j = j;
+    if (d_counts)
+      k_plane_step<GLB_PREC_FP64, true><<<nblk(n, 128), 128, 0, s>>>(a);
+    else if (precision == GLB_PREC_SPLIT)
+      k_plane_step<GLB_PREC_SPLIT><<<nblk(n, 128), 128, 0, s>>>(a);
+    else
+      k_plane_step<GLB_PREC_FP64><<<nblk(n, 128), 128, 0, s>>>(a);
+  }
+  CKR(cudaEventRecord(l->ev[2], s));
+  k_finish<<<nblk(n, 256), 256, 0, s>>>(l->st.p, l->perm.p, n, y, A);
+  CKR(cudaEventRecord(l->ev[3], s));
+  CKR(cudaGetLastError());
+  return 0;
+}
+
+}  // namespace
+
+// ===================================================================== C ABI
+extern "C" {
+
+const char *glb_last_error(void) { return t_err.c_str(); }
+const char *glb_version(void) { return "glamer_b200 0.1 (sm_100a)"; }
+
+int glb_set_option(int option, long long value) {
+  if (option == GLB_OPT_KEEP_TREE_EXPORT) {
+    g_keep_tree_export = value ? 1 : 0;
+    return 0;
+  }
+  return fail(GLB_ERR_ARG, "unknown option");
+}
+
+// ------------------------------------------------------------------ trees
+struct glb_tree {
+  std::unique_ptr<Tree> tree;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+};
+
+int glb_tree_create(const glb_particle *particles, size_t n, float mass_fixed, float size_fixed, double inv_area,
+                    int bucket, double theta_force, int periodic_buffer, double inv_screening_scale,
+                    double maximum_range, glb_tree **out) {
+  if (!out || (n > 0 && !particles)) return fail(GLB_ERR_ARG, "null argument");
+  if (bucket < 1) return fail(GLB_ERR_ARG, "bucket must be >= 1");
+  if (int rc = need_device()) return rc;
+  auto t = std::make_unique<glb_tree>();
+  CKR(cudaGetDevice(&t->device));
+  CKR(cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking));
+  TreeParams prm;
+  prm.mass_fixed = mass_fixed;
+  prm.size_fixed = size_fixed;
+  prm.inv_area = inv_area;
+  prm.bucket = bucket;
+  prm.theta = theta_force;
+  prm.periodic = periodic_buffer;
+  prm.inv_screening = inv_screening_scale;
+  prm.max_range = maximum_range;
+  Status s = build_tree(reinterpret_cast<const glb_particle_rec *>(particles), n, prm, g_keep_tree_export != 0,
+                        t->stream, t->tree);
+  if (!s.good()) {
+    cudaStreamDestroy(t->stream);
+    return fail(s);
+  }
+  *out = t.release();
+  return 0;
+}
+
+int glb_tree_destroy(glb_tree *t) {
+  if (!t) return 0;
+  cudaSetDevice(t->device);
+  t->tree.reset();
+  if (t->stream) cudaStreamDestroy(t->stream);
+  delete t;
+  return 0;
+}
+
+static int force_generic(const HaloDev &H, int device, cudaStream_t s, size_t n, const double *xcm, double *alpha,
+                         double *kappa, double *gamma, double *phi) {
+  if (n == 0) return 0;
+  if (!xcm) return fail(GLB_ERR_ARG, "null positions");
+  if (int rc = set_dev(device)) return rc;
+  NFWTables tab{};
+  if (H.kind == HALO_NFW)
+    if (int rc = device_nfw_tables(tab)) return rc;
+  DBuf<double> dx, dout;
+  CKR(dx.alloc(2 * n));
+  CKR(dout.alloc(6 * n));
+  CKR(cudaMemcpyAsync(dx.p, xcm, 2 * n * sizeof(double), cudaMemcpyHostToDevice, s));
+  k_halo_force<<<nblk(n, 128), 128, 0, s>>>(H, tab, n, dx.p, dout.p);
+  CKR(cudaGetLastError());
+  std::vector<double> o(6 * n);
+  CKR(cudaMemcpyAsync(o.data(), dout.p, 6 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CKR(cudaStreamSynchronize(s));
+  for (size_t i = 0; i < n; ++i) {
+    if (alpha) {
+      alpha[2 * i] = o[6 * i];
+      alpha[2 * i + 1] = o[6 * i + 1];
+    }
+    if (kappa) kappa[i] = o[6 * i + 2];
+    if (gamma) {
+      gamma[3 * i] = o[6 * i + 3];
+      gamma[3 * i + 1] = o[6 * i + 4];
+      gamma[3 * i + 2] = 0.0;
+    }
+    if (phi) phi[i] = o[6 * i + 5];
+  }
+  return 0;
+}
+
+int glb_tree_force2D_recur(glb_tree *t, size_t n, const double *rays, double *alpha, double *kappa, double *gamma,
+                           double *phi) {
+  if (!t) return fail(GLB_ERR_ARG, "null tree");
+  HaloDev H;
+  memset(&H, 0, sizeof(H));
+  H.kind = HALO_PARTICLES;
+  H.tree = t->tree->dev;
+  if (t->tree->nparticles == 0) {
+    for (size_t i = 0; i < n; ++i) {
+      if (alpha) alpha[2 * i] = alpha[2 * i + 1] = 0;
+      if (kappa) kappa[i] = 0;
+      if (gamma) gamma[3 * i] = gamma[3 * i + 1] = gamma[3 * i + 2] = 0;
+      if (phi) phi[i] = 0;
+    }
+    return 0;
+  }
+  return force_generic(H, t->device, t->stream, n, rays, alpha, kappa, gamma, phi);
+}
+
+int glb_tree_export(glb_tree *t, size_t *nbranches, double *out) {
+  if (!t || !nbranches) return fail(GLB_ERR_ARG, "null argument");
+  *nbranches = t->tree->nbranches;
+  if (!out) return 0;
+  if (t->tree->export_rows.size() != 16 * t->tree->nbranches)
+    return fail(GLB_ERR_ARG, "tree built without GLB_OPT_KEEP_TREE_EXPORT");
+  memcpy(out, t->tree->export_rows.data(), t->tree->export_rows.size() * sizeof(double));
+  return 0;
+}
+
+int glb_tree_build_ms(glb_tree *t, double *ms) {
+  if (!t || !ms) return fail(GLB_ERR_ARG, "null argument");
+  *ms = t->tree->build_ms;
+  return 0;
+}
+
+// ------------------------------------------------------------------ halos
+static int new_halo(std::unique_ptr<glb_halo> &h) {
+  if (int rc = need_device()) return rc;
+  h = std::make_unique<glb_halo>();
+  CKR(cudaGetDevice(&h->device));
+  CKR(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  return 0;
+}
+
+int glb_halo_particles(const glb_particle *particles, size_t n, double z, double inv_area, double max_range,
+                       glb_halo **out) {
+  if (!out || (n > 0 && !particles)) return fail(GLB_ERR_ARG, "null argument");
+  std::unique_ptr<glb_halo> h;
+  if (int rc = new_halo(h)) return rc;
+  h->kind = HALO_PARTICLES;
+  h->zlens = (double)(float)z;  // the vector constructor takes a float redshift
+  // the cosmology is bound when the halo enters a lens (Dist is reset there)
+  double m = 0;
+  for (size_t i = 0; i < n; ++i) m += particles[i].Mass;  // set_up, particle_halo.h:366-378
+  h->mass = (float)m;
+  h->Rsize = h->Rmax = (float)1.0e100;
+  TreeParams prm;
+  prm.inv_area = inv_area;
+  prm.bucket = 20;        // particle_halo.h:416
+  prm.theta = 0.1;
+  prm.periodic = 0;
+  prm.inv_screening = max_range;  // the ninth argument there is inv_screening_scale
+  prm.max_range = -1;
+  Status s = build_tree(reinterpret_cast<const glb_particle_rec *>(particles), n, prm, g_keep_tree_export != 0,
+                        h->stream, h->tree);
+  if (!s.good()) return fail(s);
+  *out = h.release();
+  return 0;
+}
+
+int glb_halo_nfw(float mass, float Rsize, double z, float concentration, float fratio, float pa, glb_halo **out) {
+  if (!out) return fail(GLB_ERR_ARG, "null argument");
+  if (fratio != 1.0f)
+    return fail(GLB_ERR_UNSUPPORTED, "elliptical NFW (fratio != 1) is outside this library's scope");
+  if (!(concentration > 0) || !(Rsize > 0)) return fail(GLB_ERR_ARG, "Rsize and concentration must be positive");
+  std::unique_ptr<glb_halo> h;
+  if (int rc = new_halo(h)) return rc;
+  std::call_once(g_nfw_host_once, make_host_tables);
+  h->kind = HALO_NFW;
+  h->zlens = z;
+  h->Rsize = Rsize;
+  h->mass = mass;
+  h->rscale = h->Rsize / concentration;  // float / float (lens_halos.cpp:411)
+  double xmax = (double)(h->Rsize / h->rscale);
+  if (xmax >= kNfwMaxRm * (kNfwTable - 1) / kNfwTable)
+    return fail(GLB_ERR_ARG, "concentration beyond the reference's NFW table");
+  double gmax = nfw_interp_host(1, xmax);
+  h->Rmax = h->Rsize;  // fratio == 1 (lens_halos.cpp:425-428)
+  NFWDev &d = h->nfw;
+  d.mass = h->mass;
+  d.rscale = h->rscale;
+  d.gmax = gmax;
+  d.Rmax2 = (double)(h->Rmax * h->Rmax);
+  d.h_xmax = nfw_interp_host(3, (double)(h->Rsize / h->rscale));
+  d.log_rsize = (double)logf(h->Rsize);  // log of a float member: the float overload
+  (void)pa;
+  *out = h.release();
+  return 0;
+}
+
+// LensHalo::MassBy1DIntegation (lens_halos.cpp:2469-2473): R/2 times the
+// angular integral of the inward radial deflection on the circle R; the
+// integrand is smooth and periodic, so a 4096-point trapezoid rule is used.
+static double nsie_mass_1d(const NSIEDev &d, double R) {
+  const int NQ = 4096;
+  double sum = 0;
+  for (int i = 0; i < NQ; ++i) {
+    double th = 2 * kPi * i / NQ;
+    double out[6] = {0, 0, 0, 0, 0, 0};
+    nsie_force<false>(d, R * cos(th), R * sin(th), out);
+    sum += -out[0] * cos(th) - out[1] * sin(th);
+  }
+  return R * (sum * 2 * kPi / NQ) / 2;
+}
+
+int glb_halo_nsie(float mass, double z, float sigma, float rcore, float fratio, float pa, glb_halo **out) {
+  if (!out) return fail(GLB_ERR_ARG, "null argument");
+  if (fratio > 1.0f || fratio < 0.01f) return fail(GLB_ERR_ARG, "invalid fratio");  // lens_halos.cpp:1072
+  if (!(sigma > 0)) return fail(GLB_ERR_ARG, "sigma must be positive");
+  std::unique_ptr<glb_halo> h;
+  if (int rc = new_halo(h)) return rc;
+  h->kind = HALO_NSIE;
+  h->rscale = 1.0f;
+  h->mass = mass;
+  h->zlens = z;
+  float pa_m = (float)(kPi / 2 - pa);  // lens_halos.cpp:1058
+  // rmax_calc (lens_halos.cpp:1154-1171)
+  double rs;
+  if (fratio == 1.0f || rcore > 0.0f) {
+    float sf = sqrtf(fratio);
+    double a = (double)h->mass * kGrav * kLightspeed * kLightspeed * (double)sf / kPi / (double)sigma /
+                   (double)sigma + (double)rcore;
+    rs = sqrt(pow(a, 2) - (double)(rcore * rcore));
+  } else {
+    // elliptic-integral normalisation: (2/pi) int_0^{pi/2} dt / sqrt(1 + (q^2-1) sin^2 t)
+    // = 1 / AGM(1, q), interpolated linearly on the reference's 200-point q table
+    auto F = [](double q) {
+      double a = 1.0, b = q;
+      for (int i = 0; i < 40; ++i) {
+        double an = 0.5 * (a + b), bn = sqrt(a * b);
+        a = an;
+        b = bn;
+      }
+      return 1.0 / a;
+    };
+    const int N = 200;
+    std::vector<double> qt(N), Ft(N);
+    qt[0] = 0.01;
+    Ft[0] = F(0.01);
+    for (int i = 1; i < N - 1; ++i) {
+      qt[i] = i * 1.0 / (N - 1);
+      Ft[i] = F(qt[i]);
+    }
+    qt[N - 1] = 1.0;
+    Ft[N - 1] = 1.0;
+    double q = fratio;
+    int i = 0;
+    while (i < N - 2 && qt[i + 1] <= q) ++i;
+    double ell = (Ft[i] + (Ft[i + 1] - Ft[i]) * (q - qt[i]) / (qt[i + 1] - qt[i])) * sqrt((double)fratio);
+    rs = (double)h->mass * kGrav * kLightspeed * kLightspeed / kPi / (double)sigma / (double)sigma / ell;
+  }
+  h->Rsize = (float)rs;
+  h->Rmax = 1.2f * h->Rsize;
+  float units = (float)(pow((double)sigma / kLightspeed, 2) / kGrav);
+  NSIEDev &d = h->nsie;
+  d.f = (double)fratio;
+  d.bc = (double)rcore;
+  d.sqrt_f = sqrt(d.f);
+  d.fp = sqrt(1 - d.f * d.f);
+  double p = (double)pa_m;
+  d.c1 = cos(p);
+  d.s1 = sin(p);
+  d.c2 = cos(-p);
+  d.s2 = sin(-p);
+  d.c3 = cos(-2 * p);
+  d.s3 = sin(-2 * p);
+  d.c0 = 1.0;
+  d.s0 = 0.0;
+  d.units = (double)units;
+  d.Rsize = (double)h->Rsize;
+  d.Rmax = (double)h->Rmax;
+  d.Rsize2 = (double)(h->Rsize * h->Rsize);
+  d.Rmax2 = (double)(h->Rmax * h->Rmax);
+  d.dRmaxRsize = (double)(h->Rmax - h->Rsize);
+  d.mass = (double)h->mass;
+  // A cored halo's mass is reset by 1D integration (lens_halos.cpp:1073-1075)
+  // with `units` already assigned.
+  if (rcore > 0.0f) {
+    h->mass = (float)nsie_mass_1d(d, (double)h->Rsize);
+    d.mass = (double)h->mass;
+  }
+  *out = h.release();
+  return 0;
+}
+
+int glb_halo_set_theta(glb_halo *h, double tx, double ty) {
+  if (!h) return fail(GLB_ERR_ARG, "null halo");
+  h->theta[0] = tx;
+  h->theta[1] = ty;
+  return 0;
+}
+
+int glb_halo_force(glb_halo *h, size_t n, const double *xcm, double *alpha, double *kappa, double *gamma,
+                   double *phi) {
+  if (!h) return fail(GLB_ERR_ARG, "null halo");
+  HaloDev H = make_halo_dev(*h);
+  if (h->kind == HALO_PARTICLES && h->tree->nparticles == 0) {
+    for (size_t i = 0; i < n; ++i) {
+      if (alpha) alpha[2 * i] = alpha[2 * i + 1] = 0;
+      if (kappa) kappa[i] = 0;
+      if (gamma) gamma[3 * i] = gamma[3 * i + 1] = gamma[3 * i + 2] = 0;
+      if (phi) phi[i] = 0;
+    }
+    return 0;
+  }
+  int rc = force_generic(H, h->device, h->stream, n, xcm, alpha, kappa, gamma, phi);
+  if (rc) return rc;
+  if (h->kind == HALO_PARTICLES && alpha)  // LensHaloParticles::force_halo negates alpha
+    for (size_t i = 0; i < 2 * n; ++i) alpha[i] = -alpha[i];
+  return 0;
+}
+
+int glb_halo_params(glb_halo *h, float *mass, float *rsize, float *rmax) {
+  if (!h) return fail(GLB_ERR_ARG, "null halo");
+  if (mass) *mass = h->mass;
+  if (rsize) *rsize = h->Rsize;
+  if (rmax) *rmax = h->Rmax;
+  return 0;
+}
+
+int glb_halo_destroy(glb_halo *h) {
+  if (!h) return 0;
+  cudaSetDevice(h->device);
+  h->tree.reset();
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return 0;
+}
+
+// ------------------------------------------------------------------- lens
+int glb_lens_create(double zsource, double omega_m, double omega_l, double hubble, glb_lens **out) {
+  if (!out) return fail(GLB_ERR_ARG, "null argument");
+  if (omega_m + omega_l != 1.0)
+    return fail(GLB_ERR_ARG, "Lens can only handle flat universes at present");  // lens.cpp:63-67
+  if (int rc = need_device()) return rc;
+  auto l = std::make_unique<glb_lens>();
+  l->cosmo = Cosmo{omega_m, omega_l, hubble};
+  l->zsource = zsource;
+  l->charge = 4 * kPi * kGrav;  // lens.cpp:93
+  CKR(cudaGetDevice(&l->device));
+  CKR(cudaStreamCreateWithFlags(&l->stream, cudaStreamNonBlocking));
+  for (int i = 0; i < 4; ++i) CKR(cudaEventCreate(&l->ev[i]));
+  combine_planes(l.get());
+  *out = l.release();
+  return 0;
+}
+
+int glb_lens_destroy(glb_lens *l) {
+  if (!l) return 0;
+  cudaSetDevice(l->device);
+  if (l->stream) cudaStreamSynchronize(l->stream);
+  for (auto &h : l->owned) {
+    h->tree.reset();
+    if (h->stream) cudaStreamDestroy(h->stream);
+  }
+  for (int i = 0; i < 4; ++i)
+    if (l->ev[i]) cudaEventDestroy(l->ev[i]);
+  cudaStream_t s = l->stream;
+  delete l;
+  if (s) cudaStreamDestroy(s);
+  return 0;
+}
+
+// Lens::addMainHaloToPlane (lens.cpp:772-815) / addMainHaloToNearestPlane
+// (lens.cpp:821-838), then combinePlanes.
+int glb_lens_insert_halo(glb_lens *l, glb_halo *h, int addplanes) {
+  if (!l || !h) return fail(GLB_ERR_ARG, "null argument");
+  const Cosmo &c = l->cosmo;
+  l->owned.emplace_back(h);
+  h->Dist = angdist(c, h->zlens);  // LensHalo(z, cosmo): Dist = angDist(z)
+  double hz = h->zlens, hD = coordist2(c, 0, hz);
+  auto &M = l->main;
+  auto setz = [&](glb_halo *x, double z) {
+    x->zlens = z;
+    x->Dist = angdist(c, z);
+  };
+  if (addplanes) {
+    size_t i = 0;
+    while (i < M.size() && !(hD < M[i].Dl)) ++i;  // upper_bound
+    if (i > 0 && (hD - M[i - 1].Dl) < 1e-6) {
+      M[i - 1].halos.push_back(h);
+      setz(h, M[i - 1].z);
+    } else if (i == M.size()) {
+      M.push_back(PlaneHost{hz, hD, {h}});
+    } else if ((M[i].Dl - hD) < 1e-6) {
+      M[i].halos.push_back(h);
+      setz(h, M[i].z);
+    } else {
+      M.insert(M.begin() + i, PlaneHost{hz, hD, {h}});
+      setz(h, hz);
+    }
+  } else {
+    if (M.empty()) {
+      M.push_back(PlaneHost{hz, hD, {h}});
+    } else {
+      size_t best = 0;
+      for (size_t i = 1; i < M.size(); ++i)
+        if (std::fabs(M[i].Dl - hD) < std::fabs(M[best].Dl - hD)) best = i;
+      M[best].halos.push_back(h);
+      setz(h, M[best].z);
+    }
+  }
+  combine_planes(l);
+  return 0;
+}
+
+int glb_lens_nplanes(glb_lens *l, int *nplanes) {
+  if (!l || !nplanes) return fail(GLB_ERR_ARG, "null argument");
+  *nplanes = (int)l->main.size();
+  return 0;
+}
+
+int glb_lens_planes(glb_lens *l, double *z, double *Dl, double *dDl) {
+  if (!l) return fail(GLB_ERR_ARG, "null lens");
+  for (size_t i = 0; i < l->plane_z.size(); ++i) {
+    if (z) z[i] = l->plane_z[i];
+    if (Dl) Dl[i] = l->Dl[i];
+    if (dDl) dDl[i] = l->dDl[i];
+  }
+  return 0;
+}
+
+int glb_lens_reset_source(glb_lens *l, double z, int nearest, int *plane_index) {
+  if (!l) return fail(GLB_ERR_ARG, "null lens");
+  l->toggle_source_plane = true;
+  long j = 0;
+  if (z <= 0.0) {
+    if (plane_index) *plane_index = 0;
+    return 0;
+  }
+  double Ds = coordist2(l->cosmo, 0, z);
+  size_t np = l->main.size();
+  if (l->Dl.size() > 1) {
+    // NR locate on Dl[0..np-1] (1-based bisection)
+    unsigned long n = (unsigned long)np, ju = n + 1, jl = 0, jm;
+    const double *xx = l->Dl.data() - 1;
+    while (ju - jl > 1) {
+      jm = (ju + jl) >> 1;
+      if (Ds >= xx[jm]) jl = jm; else ju = jm;
+    }
+    if (Ds == xx[1]) j = 1;
+    else if (Ds == xx[n]) j = (long)n - 1;
+    else j = (long)jl;
+  }
+  if (j > 0) {
+    if (l->Dl[j - 1] == Ds) --j;
+    else if (nearest) {
+      double z1 = invcoordist(l->cosmo, l->Dl[j] - 0.5 * l->dDl[j]);
+      if (z < z1) --j;
+    }
+  }
+  if (nearest && (j < (long)np)) l->zs_implant = l->plane_z[j];
+  else l->zs_implant = z;
+  if (plane_index) *plane_index = (int)j;
+  return 0;
+}
+
+int glb_lens_rayshoot_device(glb_lens *l, size_t n, const double *x_dev, const double *zs_dev, double *y_dev,
+                             double *A_dev, int precision, void *stream) {
+  if (!l) return fail(GLB_ERR_ARG, "null lens");
+  if (n > 0 && (!x_dev || !y_dev || !A_dev)) return fail(GLB_ERR_ARG, "null buffer");
+  if (precision != GLB_PREC_FP64 && precision != GLB_PREC_SPLIT) return fail(GLB_ERR_ARG, "unknown precision");
+  if (int rc = set_dev(l->device)) return rc;
+  cudaStream_t s = stream ? (cudaStream_t)stream : l->stream;
+  return rayshoot_device(l, n, x_dev, zs_dev, y_dev, A_dev, precision, s);
+}
+
+static int rayshoot_host(glb_lens *l, size_t n, const double *x, const double *zs, double *y, double *A,
+                         int precision, bool x_on_device) {
+  if (n == 0) return 0;
+  size_t need = (x_on_device ? 0 : 2 * n) + (zs ? n : 0) + 6 * n;
+  if (l->io.n < need) CKR(l->io.alloc(need));
+  double *dx = x_on_device ? const_cast<double *>(x) : l->io.p;
+  double *dzs = zs ? l->io.p + (x_on_device ? 0 : 2 * n) : nullptr;
+  double *dy = l->io.p + (x_on_device ? 0 : 2 * n) + (zs ? n : 0);
+  double *dA = dy + 2 * n;
+  if (!x_on_device) CKR(cudaMemcpyAsync(dx, x, 2 * n * sizeof(double), cudaMemcpyHostToDevice, l->stream));
+  if (zs) CKR(cudaMemcpyAsync(dzs, zs, n * sizeof(double), cudaMemcpyHostToDevice, l->stream));
+  if (int rc = rayshoot_device(l, n, dx, dzs, dy, dA, precision, l->stream)) return rc;
+  CKR(cudaMemcpyAsync(y, dy, 2 * n * sizeof(double), cudaMemcpyDeviceToHost, l->stream));
+  CKR(cudaMemcpyAsync(A, dA, 4 * n * sizeof(double), cudaMemcpyDeviceToHost, l->stream));
+  CKR(cudaStreamSynchronize(l->stream));
+  if (l->main.size() > 0) {
+    cudaEventElapsedTime(&l->last_kernel_ms, l->ev[1], l->ev[2]);
+    cudaEventElapsedTime(&l->last_total_ms, l->ev[0], l->ev[3]);
+  }
+  return 0;
+}
+
+int glb_lens_rayshoot(glb_lens *l, size_t n, const double *x, const double *zs, double *y, double *A,
+                      int precision) {
+  if (!l) return fail(GLB_ERR_ARG, "null lens");
+  if (n > 0 && (!x || !y || !A)) return fail(GLB_ERR_ARG, "null buffer");
+  if (precision != GLB_PREC_FP64 && precision != GLB_PREC_SPLIT) return fail(GLB_ERR_ARG, "unknown precision");
+  if (int rc = set_dev(l->device)) return rc;
+  return rayshoot_host(l, n, x, zs, y, A, precision, false);
+}
+
+int glb_gridmap(glb_lens *l, size_t n1d, const double *center, double range, double *y, double *A, int precision) {
+  if (!l || !center || !y || !A) return fail(GLB_ERR_ARG, "null argument");
+  if (n1d < 1) return fail(GLB_ERR_ARG, "GridMap size is < 1!");  // gridmap.cpp:102
+  if (range <= 0) return fail(GLB_ERR_ARG, "GridMap range is <= 0!");
+  if (precision != GLB_PREC_FP64 && precision != GLB_PREC_SPLIT) return fail(GLB_ERR_ARG, "unknown precision");
+  if (int rc = set_dev(l->device)) return rc;
+  size_t n = n1d * n1d;
+  DBuf<double> dx;
+  CKR(dx.alloc(2 * n));
+  k_grid<<<nblk(n, 256), 256, 0, l->stream>>>(n1d, center[0], center[1], range, dx.p);
+  CKR(cudaGetLastError());
+  int rc = rayshoot_host(l, n, dx.p, nullptr, y, A, precision, true);
+  CKR(cudaStreamSynchronize(l->stream));
+  return rc;
+}
+
+int glb_lens_count_interactions(glb_lens *l, size_t n, const double *x, const double *zs,
+                                unsigned long long *counts) {
+  if (!l || !counts || (n > 0 && !x)) return fail(GLB_ERR_ARG, "null argument");
+  if (int rc = set_dev(l->device)) return rc;
+  DBuf<double> dx, dzs, dy, dA;
+  DBuf<unsigned long long> dc;
+  CKR(dx.alloc(2 * n));
+  CKR(dy.alloc(2 * n));
+  CKR(dA.alloc(4 * n));
+  CKR(dc.alloc(5));
+  CKR(cudaMemsetAsync(dc.p, 0, 5 * sizeof(unsigned long long), l->stream));
+  CKR(cudaMemcpyAsync(dx.p, x, 2 * n * sizeof(double), cudaMemcpyHostToDevice, l->stream));
+  if (zs) {
+    CKR(dzs.alloc(n));
+    CKR(cudaMemcpyAsync(dzs.p, zs, n * sizeof(double), cudaMemcpyHostToDevice, l->stream));
+  }
+  if (int rc = rayshoot_device(l, n, dx.p, zs ? dzs.p : nullptr, dy.p, dA.p, GLB_PREC_FP64, l->stream, dc.p))
+    return rc;
+  CKR(cudaMemcpyAsync(counts, dc.p, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, l->stream));
+  CKR(cudaStreamSynchronize(l->stream));
+  return 0;
+}
+
+int glb_lens_last_timing(glb_lens *l, double *kernel_ms, double *total_ms) {
+  if (!l) return fail(GLB_ERR_ARG, "null lens");
+  if (kernel_ms) *kernel_ms = l->last_kernel_ms;
+  if (total_ms) *total_ms = l->last_total_ms;
+  return 0;
+}
+
+}  // extern "C"

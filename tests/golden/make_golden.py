@@ -1,0 +1,100 @@
+"""Generates tests/golden/*.npz from the reference itself.
+
+The reference ships no test vectors, so the golden outputs come from the
+reference's own sources compiled in place (oracle/_ref/glamer_ref, built by
+oracle/Makefile from the SLsimLib tree).  Each fixture stores its inputs and
+the reference's outputs, so tests need neither the reference tree nor the
+generator at run time.
+
+    make -C oracle && python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from slsimlib_b200 import synth  # noqa: E402
+from tests import harness as H  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+
+def tree_fixture():
+    rng = np.random.default_rng(11)
+    p = synth.nfw_particles(rng, 3000, 1e14, 5.0, 0.3, 1e-3)
+    # a few particles with large softening to populate internal big-particle lists
+    p["Size"][:40] = np.float32(0.05)
+    rays = np.concatenate([rng.uniform(-0.05, 0.05, size=(48, 2)), rng.uniform(-0.6, 0.6, size=(16, 2))])
+    R = H.RefDriver()
+    out, exp = R.tree_force(p, rays, bucket=20, theta=0.1, inv_screening=1.0, export=True)
+    np.savez_compressed(os.path.join(OUT, "tree_small.npz"), particles=p, rays=rays, force=out, export=exp,
+                        bucket=20, theta=0.1, inv_screening=1.0)
+
+
+def halo_fixture():
+    rng = np.random.default_rng(12)
+    x = rng.uniform(-1.0, 1.0, size=(64, 2)) * np.logspace(-4, 0.2, 64)[:, None]
+    R = H.RefDriver()
+    halos = {
+        "nfw": synth.NFWHalo(1e14, 0.864, 0.3, 5.0),
+        "nsie_cored": synth.NSIEHalo(1e13, 0.5, 250.0, 3.05e-4, 0.7, 0.0),
+        "nsie_sis": synth.NSIEHalo(1e13, 0.5, 250.0, 0.0, 1.0, 0.0),
+        "nsie_rot": synth.NSIEHalo(1e12, 0.5, 200.0, 1e-4, 0.5, 0.3),
+    }
+    data = {"x": x}
+    for k, h in halos.items():
+        f, prm = R.halo_force(h, x)
+        data[k] = f
+        data[k + "_params"] = np.array(prm)
+    np.savez_compressed(os.path.join(OUT, "halos.npz"), **data)
+
+
+def lens_fixture():
+    spec = synth.light_cone(seed=13, n_total=6000, n_planes=3, halos_per_plane=3)
+    spec.halos.append(synth.NFWHalo(3e13, 0.4, 0.7, 6.0, theta=(2e-5, -1e-5)))
+    R = H.RefDriver()
+    rng_range = 60 * synth.ARCSEC
+    y, A, _ = R.grid(spec, 16, range_rad=rng_range)
+    rng = np.random.default_rng(14)
+    x = rng.uniform(-30, 30, size=(64, 2)) * synth.ARCSEC
+    zs = rng.uniform(0.2, 3.0, size=64)
+    y2, A2, _ = R.rays(spec, x, zs)
+    arrays = {"grid_y": y, "grid_A": A, "grid_n": 16, "grid_range": rng_range, "rays_x": x, "rays_zs": zs,
+              "rays_y": y2, "rays_A": A2, "zsource": spec.zsource}
+    for i, h in enumerate(spec.halos):
+        if isinstance(h, synth.ParticlePlane):
+            arrays[f"plane{i}_particles"] = h.particles
+            arrays[f"plane{i}_z"] = h.z
+    nsie = [h for h in spec.halos if isinstance(h, synth.NSIEHalo)][0]
+    arrays["nsie"] = np.array([nsie.mass, nsie.z, nsie.sigma, nsie.rcore, nsie.fratio, nsie.pa])
+    nfw = [h for h in spec.halos if isinstance(h, synth.NFWHalo)][0]
+    arrays["nfw"] = np.array([nfw.mass, nfw.rsize, nfw.z, nfw.conc, nfw.theta[0], nfw.theta[1]])
+    np.savez_compressed(os.path.join(OUT, "lens_small.npz"), **arrays)
+
+
+def lens_spec_from_fixture(d) -> synth.LensSpec:
+    """Rebuilds the LensSpec of lens_small.npz (insertion order as generated)."""
+    halos = []
+    i = 0
+    while f"plane{i}_particles" in d:
+        halos.append(synth.ParticlePlane(d[f"plane{i}_particles"], float(d[f"plane{i}_z"])))
+        i += 1
+    m, z, s, rc, f, pa = d["nsie"]
+    halos.append(synth.NSIEHalo(m, z, s, rc, f, pa))
+    m, r, z, c, tx, ty = d["nfw"]
+    halos.append(synth.NFWHalo(m, r, z, c, theta=(tx, ty)))
+    return synth.LensSpec(zsource=float(d["zsource"]), halos=halos)
+
+
+if __name__ == "__main__":
+    if not H.ref_available():
+        sys.exit("oracle/_ref/glamer_ref missing: run `make -C oracle` where the reference tree exists")
+    tree_fixture()
+    halo_fixture()
+    lens_fixture()
+    print("golden fixtures written to", OUT)

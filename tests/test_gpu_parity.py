@@ -1,0 +1,228 @@
+"""Parity of the sm_100a library with the reference (golden fixtures) and the
+oracle (live, seeded inputs), through the C ABI.
+
+FP64 tolerance: the GPU performs the reference's operations with fused
+multiply-adds and a different (depth-first, bottom-up) summation order, so
+results agree to ~1e-13 relative; the tests allow 1e-9 relative to
+max(|ref|, 1e-6 x median |ref| of the column)."""
+import numpy as np
+import pytest
+
+import slsimlib_b200 as glb
+from slsimlib_b200 import synth
+from tests import harness as H
+from tests.conftest import rel_err
+from tests.golden.make_golden import lens_spec_from_fixture
+
+pytestmark = pytest.mark.gpu
+
+RTOL64 = 1e-9
+
+
+def pack(a, k, g, ph):
+    return np.concatenate([a, k[:, None], g, ph[:, None]], axis=1)
+
+
+def make_lens(spec: synth.LensSpec) -> glb.Lens:
+    L = glb.Lens(spec.zsource)
+    for h in spec.halos:
+        if isinstance(h, synth.ParticlePlane):
+            hh = glb.LensHaloParticles(h.particles, h.z, h.inv_area, h.max_range)
+        elif isinstance(h, synth.NSIEHalo):
+            hh = glb.LensHaloRealNSIE(h.mass, h.z, h.sigma, h.rcore, h.fratio, h.pa)
+        else:
+            hh = glb.LensHaloNFW(h.mass, h.rsize, h.z, h.conc)
+        hh.setTheta(*h.theta)
+        L.insertMainHalo(hh, True)
+    return L
+
+
+# ------------------------------------------------------------------ trees
+def test_tree_build_matches_reference_branch_by_branch(golden):
+    d = golden("tree_small.npz")
+    t = glb.TreeQuadParticles(d["particles"], bucket=int(d["bucket"]), theta_force=float(d["theta"]),
+                              inv_screening_scale=float(d["inv_screening"]), keep_export=True)
+    e, r = t.export(), d["export"]
+    assert e.shape == r.shape
+    # geometry, membership counts, big-particle counts and leaf flags: exact
+    for c in (0, 1, 2, 3, 4, 5, 6, 14, 15):
+        np.testing.assert_array_equal(e[:, c], r[:, c], err_msg=f"column {c}")
+    # mass and centre of mass: summation order only
+    np.testing.assert_allclose(e[:, 7], r[:, 7], rtol=1e-12)
+    w = r[:, 3] - r[:, 1]
+    for c in (8, 9):
+        assert np.all(np.abs(e[:, c] - r[:, c]) <= 1e-12 * (np.abs(r[:, c]) + w))
+    scale = np.abs(r[:, 7]) * w * w + 1e-300
+    for c in (10, 11, 12):
+        assert np.all(np.abs(e[:, c] - r[:, c]) <= 1e-9 * scale), c
+    np.testing.assert_allclose(e[:, 13], r[:, 13], rtol=1e-10)
+
+
+def test_tree_force_matches_reference(golden):
+    d = golden("tree_small.npz")
+    t = glb.TreeQuadParticles(d["particles"], bucket=int(d["bucket"]), theta_force=float(d["theta"]),
+                              inv_screening_scale=float(d["inv_screening"]))
+    f = pack(*t.force2D_recur(d["rays"]))
+    assert np.max(rel_err(f, d["force"])) < RTOL64
+
+
+@pytest.mark.parametrize("inv_area,screen,periodic,bucket,theta", [
+    (0.0, 0.0, False, 20, 0.1),
+    (0.5, 0.0, False, 5, 0.3),
+    (0.0, 2.0, False, 1, 0.05),
+    (0.1, 0.0, True, 8, 0.2),
+])
+def test_tree_force_matches_oracle(inv_area, screen, periodic, bucket, theta):
+    rng = np.random.default_rng(5)
+    p = synth.nfw_particles(rng, 20000, 1e14, 5.0, 0.3, 1e-3)
+    p["Size"][:200] = np.float32(0.03)  # big particles on internal branches
+    rays = np.concatenate([rng.uniform(-0.05, 0.05, (200, 2)), rng.uniform(-1, 1, (56, 2))])
+    ref = H.OracleTree(p, bucket=bucket, theta=theta, inv_area=inv_area, periodic=periodic,
+                       inv_screening=screen).force(rays)
+    t = glb.TreeQuadParticles(p, inv_area=inv_area, bucket=bucket, theta_force=theta,
+                              periodic_buffer=periodic, inv_screening_scale=screen)
+    f = pack(*t.force2D_recur(rays))
+    assert np.max(rel_err(f, ref)) < RTOL64
+
+
+def test_tree_same_place_error():
+    p = np.zeros(30, dtype=synth.PARTICLE_DTYPE)
+    p["Mass"] = 1
+    with pytest.raises(glb.GlamerError) as e:
+        glb.TreeQuadParticles(p)
+    assert e.value.code == glb.GLB_ERR_SAME_PLACE
+
+
+def test_tree_tiny_and_empty_inputs():
+    rng = np.random.default_rng(9)
+    for n in (1, 2, 3, 25):
+        p = np.zeros(n, dtype=synth.PARTICLE_DTYPE)
+        p["x"][:, :2] = rng.uniform(-1, 1, (n, 2))
+        p["Mass"] = 2.0
+        p["Size"] = 0.1
+        rays = rng.uniform(-1, 1, (7, 2))
+        ref = H.OracleTree(p, bucket=5).force(rays)
+        f = pack(*glb.TreeQuadParticles(p, bucket=5).force2D_recur(rays))
+        assert np.max(rel_err(f, ref)) < RTOL64, n
+    t = glb.TreeQuadParticles(np.zeros(0, dtype=synth.PARTICLE_DTYPE))
+    a, k, g, ph = t.force2D_recur(rng.uniform(-1, 1, (4, 2)))
+    assert not a.any() and not k.any()
+    a, k, g, ph = glb.TreeQuadParticles(p).force2D_recur(np.zeros((0, 2)))
+    assert a.shape == (0, 2)
+
+
+# ------------------------------------------------------------------ halos
+def test_analytic_halos_match_reference(golden):
+    d = golden("halos.npz")
+    halos = {
+        "nfw": glb.LensHaloNFW(1e14, 0.864, 0.3, 5.0),
+        "nsie_cored": glb.LensHaloRealNSIE(1e13, 0.5, 250.0, 3.05e-4, 0.7, 0.0),
+        "nsie_sis": glb.LensHaloRealNSIE(1e13, 0.5, 250.0, 0.0, 1.0, 0.0),
+        "nsie_rot": glb.LensHaloRealNSIE(1e12, 0.5, 200.0, 1e-4, 0.5, 0.3),
+    }
+    for k, h in halos.items():
+        f = pack(*h.force_halo(d["x"]))
+        assert np.max(rel_err(f, d[k])) < 1e-9, k
+        np.testing.assert_allclose(h.params(), d[k + "_params"], rtol=1e-6, err_msg=k)
+
+
+def test_particle_halo_force_matches_oracle():
+    rng = np.random.default_rng(6)
+    p = synth.nfw_particles(rng, 5000, 1e13, 6.0, 0.5, 5e-4)
+    x = rng.uniform(-0.2, 0.2, (128, 2))
+    ref, _ = H.oracle_halo_force(synth.ParticlePlane(p, 0.5), x)
+    f = pack(*glb.LensHaloParticles(p, 0.5).force_halo(x))
+    assert np.max(rel_err(f, ref)) < RTOL64
+
+
+# ------------------------------------------------------------------- lens
+def test_gridmap_and_rays_match_reference(golden):
+    d = golden("lens_small.npz")
+    spec = lens_spec_from_fixture(d)
+    L = make_lens(spec)
+    z, Dl, dDl = L.planes()
+    zo, Dlo, dDlo = H.OracleLens(spec).planes()
+    np.testing.assert_allclose(z, zo, rtol=0)
+    np.testing.assert_allclose(Dl, Dlo, rtol=1e-12)
+    gm = glb.GridMap(L, int(d["grid_n"]), (0.0, 0.0), float(d["grid_range"]))
+    assert np.max(rel_err(gm.y, d["grid_y"])) < RTOL64
+    assert np.max(np.abs(gm.A - d["grid_A"])) < 1e-9
+    y, A = L.rayshooterInternal(d["rays_x"], d["rays_zs"])
+    assert np.max(rel_err(y, d["rays_y"])) < RTOL64
+    assert np.max(np.abs(A - d["rays_A"])) < 1e-9
+
+
+def test_light_cone_matches_oracle_and_reset_source():
+    spec = synth.light_cone(seed=31, n_total=60000, n_planes=5, halos_per_plane=6)
+    L = make_lens(spec)
+    O = H.OracleLens(spec)
+    x = synth.grid_positions(48, range_rad=60 * synth.ARCSEC)
+    y, A = L.rayshooterInternal(x)
+    yo, Ao = O.rayshoot(x)
+    assert np.max(rel_err(y, yo)) < RTOL64
+    assert np.max(np.abs(A - Ao)) < 1e-9
+    # a lower source plane (Lens::ResetSourcePlane)
+    assert L.ResetSourcePlane(0.6, False) == O.reset_source(0.6, False)
+    y, A = L.rayshooterInternal(x)
+    yo, Ao = O.rayshoot(x)
+    assert np.max(rel_err(y, yo)) < RTOL64
+    assert np.max(np.abs(A - Ao)) < 1e-9
+
+
+def test_lens_edge_cases():
+    # no lens plane: identity (internal_rayshooter_multi.cpp:62-76)
+    L = glb.Lens(2.0)
+    x = np.random.default_rng(1).uniform(-1e-4, 1e-4, (5, 2))
+    y, A = L.rayshooterInternal(x)
+    np.testing.assert_array_equal(y, x)
+    np.testing.assert_array_equal(A, np.tile([1.0, 0, 0, 1.0], (5, 1)))
+    spec = synth.single_plane_nfw(seed=2, n=4096)
+    L = make_lens(spec)
+    y, A = L.rayshooterInternal(np.zeros((0, 2)))
+    assert y.shape == (0, 2)
+    with pytest.raises(ValueError):
+        L.rayshooterInternal(x, source_zs=[1.0, 2.0])
+    # a single ray, and sources in front of / behind the plane
+    O = H.OracleLens(spec)
+    x1 = np.array([[1e-5, -2e-5]])
+    for zs in (None, np.array([0.1]), np.array([3.0])):
+        y, A = L.rayshooterInternal(x1, zs)
+        yo, Ao = O.rayshoot(x1, zs)
+        assert np.max(rel_err(y, yo)) < RTOL64
+        assert np.max(np.abs(A - Ao)) < 1e-9
+
+
+# ------------------------------------------------------- split precision
+def error_percentiles(y, A, yref, Aref, x):
+    """median and 99.9th percentile of |d alpha|/|alpha| and of the kappa,
+    gamma and invmag errors (invmag away from critical curves, |invmag|>0.05)."""
+    a, ar = x - y, x - yref
+    na = np.hypot(ar[:, 0], ar[:, 1])
+    keep = na > 1e-6 * np.median(na)
+    ea = np.hypot(*(a - ar).T)[keep] / na[keep]
+
+    def derived(M):
+        k = 1 - (M[:, 0] + M[:, 3]) / 2
+        g1 = (M[:, 0] - M[:, 3]) / 2
+        g2 = (M[:, 1] + M[:, 2]) / 2
+        inv = M[:, 0] * M[:, 3] - M[:, 1] * M[:, 2]
+        return k, np.hypot(g1, g2), inv
+    k, g, inv = derived(A)
+    kr, gr, invr = derived(Aref)
+    ek = np.abs(k - kr) / np.abs(kr)
+    eg = np.abs(g - gr) / np.abs(gr)
+    m = np.abs(invr) > 0.05
+    ei = np.abs(inv - invr)[m] / np.abs(invr[m])
+    return {n: (float(np.median(e)), float(np.percentile(e, 99.9))) for n, e in
+            (("alpha", ea), ("kappa", ek), ("gamma", eg), ("invmag", ei))}
+
+
+def test_split_precision_within_tolerance():
+    spec = synth.light_cone(seed=41, n_total=200000, n_planes=4, halos_per_plane=8)
+    L = make_lens(spec)
+    x = synth.grid_positions(96, range_rad=60 * synth.ARCSEC)
+    y64, A64 = L.rayshooterInternal(x, precision=glb.PREC_FP64)
+    y32, A32 = L.rayshooterInternal(x, precision=glb.PREC_SPLIT)
+    st = error_percentiles(y32, A32, y64, A64, x)
+    for name, (med, p999) in st.items():
+        assert med <= 1e-6 and p999 <= 1e-5, (name, med, p999)

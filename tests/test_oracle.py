@@ -1,0 +1,109 @@
+"""The oracle (C restatement) against the reference's own outputs.
+
+Golden fixtures come from the reference compiled in place
+(tests/golden/make_golden.py); when oracle/_ref/glamer_ref is present the
+oracle is also compared live on fresh seeded inputs.  CPU only."""
+import numpy as np
+import pytest
+
+from slsimlib_b200 import synth
+from tests import harness as H
+from tests.golden.make_golden import lens_spec_from_fixture
+
+EXACT = 1e-13  # the restatement performs the reference's operations in order
+
+
+def test_tree_matches_golden(golden):
+    d = golden("tree_small.npz")
+    t = H.OracleTree(d["particles"], bucket=int(d["bucket"]), theta=float(d["theta"]),
+                     inv_screening=float(d["inv_screening"]))
+    np.testing.assert_allclose(t.export(), d["export"], rtol=EXACT, atol=0)
+    np.testing.assert_allclose(t.force(d["rays"]), d["force"], rtol=EXACT, atol=0)
+
+
+def test_halos_match_golden(golden):
+    d = golden("halos.npz")
+    halos = {
+        "nfw": synth.NFWHalo(1e14, 0.864, 0.3, 5.0),
+        "nsie_cored": synth.NSIEHalo(1e13, 0.5, 250.0, 3.05e-4, 0.7, 0.0),
+        "nsie_sis": synth.NSIEHalo(1e13, 0.5, 250.0, 0.0, 1.0, 0.0),
+        "nsie_rot": synth.NSIEHalo(1e12, 0.5, 200.0, 1e-4, 0.5, 0.3),
+    }
+    for k, h in halos.items():
+        f, prm = H.oracle_halo_force(h, d["x"])
+        np.testing.assert_allclose(f, d[k], rtol=1e-12, atol=0, err_msg=k)
+        np.testing.assert_allclose(prm, d[k + "_params"], rtol=1e-6, err_msg=k)
+
+
+def test_lens_matches_golden(golden):
+    d = golden("lens_small.npz")
+    spec = lens_spec_from_fixture(d)
+    O = H.OracleLens(spec)
+    x = synth.grid_positions(int(d["grid_n"]), range_rad=float(d["grid_range"]))
+    y, A = O.rayshoot(x)
+    np.testing.assert_allclose(y, d["grid_y"], rtol=1e-12, atol=0)
+    np.testing.assert_allclose(A, d["grid_A"], rtol=1e-10, atol=1e-12)
+    y2, A2 = O.rayshoot(d["rays_x"], d["rays_zs"])
+    np.testing.assert_allclose(y2, d["rays_y"], rtol=1e-12, atol=0)
+    np.testing.assert_allclose(A2, d["rays_A"], rtol=1e-10, atol=1e-12)
+
+
+def test_tree_big_particles_and_edge_shapes():
+    # ragged inputs: a handful of particles, a line-like cloud, sizes spanning the tree
+    rng = np.random.default_rng(3)
+    for n in (1, 2, 21, 500):
+        p = np.zeros(n, dtype=synth.PARTICLE_DTYPE)
+        p["x"][:, 0] = rng.uniform(-1, 1, n)
+        p["x"][:, 1] = rng.uniform(-1, 1, n) * 1e-3
+        p["Mass"] = 1.0
+        p["Size"] = rng.uniform(1e-4, 0.5, n).astype(np.float32)
+        if n == 1:
+            t = H.OracleTree(p, bucket=5)
+            f = t.force(np.array([[0.3, 0.2]]))
+            assert np.all(np.isfinite(f))
+            continue
+        t = H.OracleTree(p, bucket=5)
+        e = t.export()
+        assert e[0, 5] == n
+        # every particle is in exactly one leaf
+        assert e[e[:, 14] == 1, 5].sum() == n
+
+
+def test_same_place_raises():
+    p = np.zeros(4, dtype=synth.PARTICLE_DTYPE)
+    p["Mass"] = 1
+    with pytest.raises(ValueError):
+        H.OracleTree(p)
+
+
+def test_direct_sum_is_close_to_tree():
+    d = np.load(__import__("os").path.join(H.ROOT, "tests", "golden", "tree_small.npz"))
+    p = d["particles"]
+    rays = d["rays"][:16]
+    t = H.OracleTree(p, bucket=20, theta=0.1)
+    ft = t.force(rays)
+    fd = H.direct_sum(p, rays)
+    a_t = np.hypot(ft[:, 0], ft[:, 1])
+    a_d = np.hypot(fd[:, 0], fd[:, 1])
+    # quadTree.h:37-38: theta = 0.1 gives better than 1% on alpha
+    assert np.max(np.abs(a_t - a_d) / a_d) < 1e-2
+
+
+@pytest.mark.skipif(not H.ref_available(), reason="reference build (oracle/_ref) not present")
+def test_oracle_matches_reference_live():
+    spec = synth.light_cone(seed=21, n_total=8000, n_planes=2, halos_per_plane=2)
+    R = H.RefDriver()
+    y_r, A_r, _ = R.grid(spec, 12, range_rad=60 * synth.ARCSEC)
+    O = H.OracleLens(spec)
+    y_o, A_o = O.rayshoot(synth.grid_positions(12, range_rad=60 * synth.ARCSEC))
+    np.testing.assert_allclose(y_o, y_r, rtol=1e-12, atol=0)
+    np.testing.assert_allclose(A_o, A_r, rtol=1e-10, atol=1e-12)
+
+
+def test_cosmology_shim_matches_product_restatement():
+    # the oracle's adaptive-Simpson distances against the library's (and the
+    # synthetic generator's) Gauss-Legendre ones
+    L = H.oracle_lib()
+    c = synth.Cosmology()
+    for z in (0.1, 0.3, 0.5, 1.0, 2.5, 5.0):
+        assert abs(L.orc_coordist(z) - c.coordist(z)) < 1e-9 * c.coordist(z)
