@@ -209,7 +209,8 @@ def main():
     x = torch.from_numpy(x_host).to(dev)
     y = torch.empty((n, 2), dtype=torch.float64, device=dev)
     A = torch.empty((n, 4), dtype=torch.float64, device=dev)
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream(device=dev)  # a real stream handle (the library maps NULL to its own)
+    torch.cuda.set_stream(stream)
 
     def shoot(prec):
         lens.rayshoot_device(n, x.data_ptr(), None, y.data_ptr(), A.data_ptr(), prec, stream.cuda_stream)

@@ -1199,6 +1199,12 @@ int glb_lens_count_interactions(glb_lens *l, size_t n, const double *x, const do
 
 int glb_lens_last_timing(glb_lens *l, double *kernel_ms, double *total_ms) {
   if (!l) return fail(GLB_ERR_ARG, "null lens");
+  if (int rc = set_dev(l->device)) return rc;
+  if (l->main.size() > 0 && cudaEventQuery(l->ev[0]) != cudaErrorNotReady) {
+    CKR(cudaEventSynchronize(l->ev[3]));
+    cudaEventElapsedTime(&l->last_kernel_ms, l->ev[1], l->ev[2]);
+    cudaEventElapsedTime(&l->last_total_ms, l->ev[0], l->ev[3]);
+  }
   if (kernel_ms) *kernel_ms = l->last_kernel_ms;
   if (total_ms) *total_ms = l->last_total_ms;
   return 0;

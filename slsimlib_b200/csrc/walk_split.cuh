@@ -11,8 +11,10 @@
 //     terms are flushed into FP64 totals, which bounds the accumulation error
 //     by the per-term rounding instead of letting it grow with the ~1e4 terms
 //     of a walk;
-//   * softened (B-spline) corrections of big particles, which sit at the
-//     closest range, are evaluated entirely in FP64.
+//   * particles within two softening lengths of the ray, whose point-mass
+//     term is cancelled by a B-spline correction, and the B-spline
+//     corrections themselves are evaluated entirely in FP64 (the close-range
+//     offsets), so no cancellation happens in FP32.
 #pragma once
 #include "walk.cuh"
 
@@ -87,29 +89,37 @@ __device__ __forceinline__ void walk_split(const TreeDev &T, double rx, double r
         const float4 P = __ldg(T.prel + p);
         if (open) {
           const float x0 = P.x + dxn, x1 = P.y + dyn;
-          float rcm2 = x0 * x0 + x1 * x1;
-          const float scr = screen ? __expf(-rcm2 * s2f) : 1.0f;
-          rcm2 = fmaxf(rcm2, 1e-20f);
-          const float m = P.z;
-          const float ir2 = __fdividef(1.0f, rcm2);
-          const float prefac = m * scr * ir2 * inv_pi;
-          const float ta = iaf * m - prefac;
-          fa.a0 += ta * x0;
-          fa.a1 += ta * x1;
-          const float tmp = -2.0f * prefac * ir2;
-          fa.g0 += 0.5f * (x0 * x0 - x1 * x1) * tmp;
-          fa.g1 += x0 * x1 * tmp;
-          fa.k -= m * iaf;
-          if (nearc) {
-            // leaf big particle: exact FP64 test and FP64 B-spline (quadTree.h:1050-1077)
+          const float rcm2f = x0 * x0 + x1 * x1;
+          if (rcm2f < 4.0001f * P.w * P.w) {
+            // within two softening lengths: the point mass and any B-spline
+            // correction cancel, so both are done in FP64 exactly as walk_f64
             const float4 Q = __ldg(T.parts + p);
+            const double y0 = (double)Q.x - rx, y1 = (double)Q.y - ry;
+            double rr = y0 * y0 + y1 * y1;
+            const double scr = screen ? exp(-rr * T.screen2) : 1.0;
+            if (rr < 1e-20) rr = 1e-20;
+            const double m = (double)Q.z, ir2 = 1.0 / rr, prefac = m * scr * ir2 * (1.0 / kPi);
+            acc[0] += (T.inv_area * m - prefac) * y0;
+            acc[1] += (T.inv_area * m - prefac) * y1;
+            const double tmp = -2.0 * prefac * ir2;
+            acc[3] += 0.5 * (y0 * y0 - y1 * y1) * tmp;
+            acc[4] += y0 * y1 * tmp;
+            acc[2] -= m * T.inv_area;
             const double size = (double)Q.w;
-            if (size < nd->width) {
-              const double y0 = (double)Q.x - rx, y1 = (double)Q.y - ry;
-              double rr = y0 * y0 + y1 * y1;
-              if (rr < 1e-20) rr = 1e-20;
-              if (rr < 4 * size * size) bspline_f64<false>(y0, y1, sqrt(rr), (double)Q.z, size, 0.0, acc);
-            }
+            if (nearc && size < nd->width && rr < 4 * size * size)
+              bspline_f64<false>(y0, y1, sqrt(rr), m, size, 0.0, acc);
+          } else {
+            const float scr = screen ? __expf(-rcm2f * s2f) : 1.0f;
+            const float m = P.z;
+            const float ir2 = __fdividef(1.0f, rcm2f);
+            const float prefac = m * scr * ir2 * inv_pi;
+            const float ta = iaf * m - prefac;
+            fa.a0 += ta * x0;
+            fa.a1 += ta * x1;
+            // shear terms scaled by 1/r^2 first so that nothing overflows FP32
+            fa.g0 -= prefac * ((x0 * x0 - x1 * x1) * ir2);
+            fa.g1 -= prefac * (2.0f * x0 * x1 * ir2);
+            fa.k -= m * iaf;
           }
         }
         if (((p - p0) & 31) == 31 && open) fa.flush(acc);
