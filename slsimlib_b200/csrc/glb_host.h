@@ -58,7 +58,7 @@ struct DBuf {
 struct Tree {
   TreeDev dev{};
   DBuf<GNode> nodes;
-  DBuf<GNodeF> nodesf;
+  DBuf<GNodeS> snodes;
   DBuf<float4> parts;
   DBuf<float4> prel;
   DBuf<float4> bigs;

@@ -33,16 +33,20 @@ struct __align__(16) GNode {
   int bstart, bcount;  // internal: range in the big-particle array
 };
 
-// FP32 companion of a node for the split-precision walk: positions are kept
-// in FP64 (cx, cy of GNode); everything else is rounded to FP32.
-struct __align__(16) GNodeF {
+// FP32 node of the split-precision walk (64 bytes).  The centre of mass is a
+// double-float pair (hi + lo, both FP32), so that a ray offset computed as
+// (cxh - rxh) + (cxl - rxl) carries FP32 relative precision however far the
+// node sits from the origin.
+struct __align__(16) GNodeS {
+  float cxh, cyh, cxl, cyl;
   float open2, near2, mass, q0;
   float q1, q2, width, pad;
+  int skip, leaf, start, count;  // leaf: particle range; internal: big-particle range
 };
 
 struct TreeDev {
   const GNode *nodes;
-  const GNodeF *nodesf;
+  const GNodeS *snodes;
   const float4 *parts;  // sorted particles {x, y, mass, size}
   const float4 *bigs;   // big-particle list of internal nodes
   const float4 *prel;   // sorted particles relative to their leaf's centre of mass (FP32)

@@ -10,20 +10,20 @@ namespace glb {
 
 // ------------------------------------------------------------- NFW
 // LensHaloNFW profile functions, AnalyticNSIE/nfw_lens.cpp:82-132.
-__host__ __device__ inline double nfw_g(double x) {
+__host__ __device__ __forceinline__ double nfw_g(double x) {
   if (x < 1e-5) x = 1e-5;
   double ans = log(x / 2);
   if (x == 1.0) return ans + 1.0;
   if (x > 1.0) return ans + 2 * atan(sqrt((x - 1) / (x + 1))) / sqrt(x * x - 1);
   return ans + 2 * atanh(sqrt((1 - x) / (x + 1))) / sqrt(1 - x * x);
 }
-__host__ __device__ inline double nfw_f(double x) {
+__host__ __device__ __forceinline__ double nfw_f(double x) {
   if (x == 0) x = 1e-5;
   if (x == 1.0) return 1.0 / 3.0;
   if (x > 1.0) return (1 - 2 * atan(sqrt((x - 1) / (x + 1))) / sqrt(x * x - 1)) / (x * x - 1);
   return (1 - 2 * atanh(sqrt((1 - x) / (x + 1))) / sqrt(1 - x * x)) / (x * x - 1);
 }
-__host__ __device__ inline double nfw_g2(double x) {
+__host__ __device__ __forceinline__ double nfw_g2(double x) {
   if (x == 0) x = 1e-5;
   if (x == 1) return 10 / 3. + 4 * log(0.5);
   double y = x * x - 1;
@@ -31,7 +31,7 @@ __host__ __device__ inline double nfw_g2(double x) {
   if (x < 1.0) return ans + 4 * (2 / x / x + 1 / y) * atanh(sqrt((1 - x) / (x + 1))) / sqrt(-y);
   return ans + 4 * (2 / x / x + 1 / y) * atan(sqrt((x - 1) / (x + 1))) / sqrt(y);
 }
-__host__ __device__ inline double nfw_h(double x) {
+__host__ __device__ __forceinline__ double nfw_h(double x) {
   if (x == 0) x = 1e-5;
   if (x <= 1.0) {
     double a = atanh(sqrt(1. - x * x)), l = log(x / 2.);
@@ -46,7 +46,7 @@ constexpr double kNfwMaxRm = 100.0;  // LensHaloNFW::maxrm (lens_halos.cpp:353)
 
 // LensHaloNFW::InterpolateFromTable (lens_halos.cpp:566-580): linear between
 // table nodes, the analytic function in bin 0.  which: 0 f, 1 g, 2 g2, 3 h.
-__device__ inline double nfw_interp(const NFWTables &T, int which, double y) {
+__device__ __forceinline__ double nfw_interp(const NFWTables &T, int which, double y) {
   int j = (int)(y / kNfwMaxRm * kNfwTable);
   if (j <= 0) {
     switch (which) {
@@ -66,7 +66,7 @@ __device__ inline double nfw_interp(const NFWTables &T, int which, double y) {
 // Point mass of the full halo mass beyond Rmax: LensHalo::force_point,
 // lens_halos.cpp:1578-1598 (subtract_point = false).
 template <bool PHI>
-__host__ __device__ inline void point_mass(double mass, double x0, double x1, double rcm2, double *out) {
+__host__ __device__ __forceinline__ void point_mass(double mass, double x0, double x1, double rcm2, double *out) {
   double prefac = mass / rcm2 / kPi;
   out[0] += -1.0 * prefac * x0;
   out[1] += -1.0 * prefac * x1;
@@ -79,7 +79,7 @@ __host__ __device__ inline void point_mass(double mass, double x0, double x1, do
 // LensHalo::force_halo -> force_point / force_halo_sym with LensHaloNFW's
 // alpha_h, kappa_h, gamma_h, phi_h (include/lens_halos.h:842-856).
 template <bool PHI>
-__device__ inline void nfw_force(const NFWDev &d, const NFWTables &T, double x0, double x1,
+__device__ __forceinline__ void nfw_force(const NFWDev &d, const NFWTables &T, double x0, double x1,
                                  double *out) {
   double rcm2 = x0 * x0 + x1 * x1;
   if (!(rcm2 < d.Rmax2)) {
@@ -106,12 +106,12 @@ __device__ inline void nfw_force(const NFWDev &d, const NFWTables &T, double x0,
 struct cplx {
   double re, im;
 };
-__host__ __device__ inline cplx c_mul(cplx a, cplx b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
-__host__ __device__ inline cplx c_scale(cplx a, double s) { return {a.re * s, a.im * s}; }
-__host__ __device__ inline cplx c_add(cplx a, cplx b) { return {a.re + b.re, a.im + b.im}; }
-__host__ __device__ inline cplx c_sub(cplx a, cplx b) { return {a.re - b.re, a.im - b.im}; }
+__host__ __device__ __forceinline__ cplx c_mul(cplx a, cplx b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+__host__ __device__ __forceinline__ cplx c_scale(cplx a, double s) { return {a.re * s, a.im * s}; }
+__host__ __device__ __forceinline__ cplx c_add(cplx a, cplx b) { return {a.re + b.re, a.im + b.im}; }
+__host__ __device__ __forceinline__ cplx c_sub(cplx a, cplx b) { return {a.re - b.re, a.im - b.im}; }
 // real / complex
-__host__ __device__ inline cplx c_rdiv(double a, cplx b) {
+__host__ __device__ __forceinline__ cplx c_rdiv(double a, cplx b) {
   // scaled to avoid overflow in |b|^2 (Smith's formulation)
   if (fabs(b.re) >= fabs(b.im)) {
     double r = b.im / b.re, den = b.re + b.im * r;
@@ -122,7 +122,7 @@ __host__ __device__ inline cplx c_rdiv(double a, cplx b) {
 }
 // principal square root (branch cut on the negative real axis; the sign of a
 // zero imaginary part selects the side, as in C99 csqrt)
-__host__ __device__ inline cplx c_sqrt(cplx z) {
+__host__ __device__ __forceinline__ cplx c_sqrt(cplx z) {
   if (z.re == 0.0 && z.im == 0.0) return {0.0, z.im};
   double t = sqrt(0.5 * (fabs(z.re) + hypot(z.re, z.im)));
   if (z.re >= 0.0) return {t, z.im / (2.0 * t)};
@@ -131,7 +131,7 @@ __host__ __device__ inline cplx c_sqrt(cplx z) {
 // asinh(z) = log(z + sqrt(z^2 + 1)) for Re z >= 0; odd symmetry otherwise.
 // For |z| < 0.5 the logarithm is taken as log1p(z + z^2 / (1 + sqrt(z^2+1)))
 // so that small arguments keep full relative precision.
-__host__ __device__ inline cplx c_asinh(cplx z) {
+__host__ __device__ __forceinline__ cplx c_asinh(cplx z) {
   bool neg = z.re < 0.0 || (z.re == 0.0 && signbit(z.re));
   if (neg) z = {-z.re, -z.im};
   cplx zz = {z.re * z.re - z.im * z.im, 2.0 * z.re * z.im};
@@ -154,7 +154,7 @@ __host__ __device__ inline cplx c_asinh(cplx z) {
 }
 
 // alphaNSIE (AnalyticNSIE/nsie.cpp:14-83); rotation angles precomputed.
-__host__ __device__ inline void alpha_nsie(const NSIEDev &d, double xt0, double xt1, double *alpha) {
+__host__ __device__ __forceinline__ void alpha_nsie(const NSIEDev &d, double xt0, double xt1, double *alpha) {
   double r = sqrt(xt0 * xt0 + xt1 * xt1);
   if (r < 1.0e-20 || r > 1.0e20) {
     alpha[0] = alpha[1] = 0.0;
@@ -194,20 +194,20 @@ __host__ __device__ inline void alpha_nsie(const NSIEDev &d, double xt0, double 
 }
 
 // kappaNSIE (nsie.cpp:89-106) on already-rotated or raw coordinates.
-__host__ __device__ inline double kappa_nsie_rot(double f, double bc, double x0, double x1) {
+__host__ __device__ __forceinline__ double kappa_nsie_rot(double f, double bc, double x0, double x1) {
   double b2 = x0 * x0 + f * f * x1 * x1;
   if ((b2 < 1.0e-20) && (bc < 1.0e-20)) return 1.0e10;
   if (b2 > 1.0e20) return 0.0;
   return 0.5 * sqrt(f / (b2 + bc * bc));
 }
 
-__host__ __device__ inline double kappa_nsie(const NSIEDev &d, double xt0, double xt1) {
+__host__ __device__ __forceinline__ double kappa_nsie(const NSIEDev &d, double xt0, double xt1) {
   double x0 = xt0 * d.c1 - xt1 * d.s1, x1 = xt1 * d.c1 + xt0 * d.s1;
   return kappa_nsie_rot(d.f, d.bc, x0, x1);
 }
 
 // gammaNSIE (nsie.cpp:112-145)
-__host__ __device__ inline void gamma_nsie(const NSIEDev &d, double xt0, double xt1, double *gam) {
+__host__ __device__ __forceinline__ void gamma_nsie(const NSIEDev &d, double xt0, double xt1, double *gam) {
   double r = sqrt(xt0 * xt0 + xt1 * xt1);
   if (r < 1.0e-20 || r > 1.0e20) {
     gam[0] = gam[1] = 0.0;
@@ -230,7 +230,7 @@ __host__ __device__ inline void gamma_nsie(const NSIEDev &d, double xt0, double 
 
 // LensHaloRealNSIE::force_halo, MultiPlane/lens_halos.cpp:1938-2014.
 template <bool PHI>
-__host__ __device__ inline void nsie_force(const NSIEDev &d, double x0, double x1, double *out) {
+__host__ __device__ __forceinline__ void nsie_force(const NSIEDev &d, double x0, double x1, double *out) {
   double rcm2 = x0 * x0 + x1 * x1;
   if (!(rcm2 < d.Rmax2)) {
     point_mass<PHI>(d.mass, x0, x1, rcm2, out);

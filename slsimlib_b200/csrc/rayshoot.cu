@@ -347,6 +347,16 @@ __device__ __forceinline__ void particle_halo_acc(const TreeDev &T, double rx, d
   }
 }
 
+// Analytic halo of a plane at one position; kept out of line so that the rare
+// NFW / NSIE arithmetic does not add to the register budget of the tree walk.
+__device__ __noinline__ void analytic_halo(const HaloDev *H, const NFWTables *tab, double x0, double x1,
+                                           double *acc) {
+  if (H->kind == HALO_NFW)
+    nfw_force<false>(H->nfw, *tab, x0, x1, acc);
+  else
+    nsie_force<false>(H->nsie, x0, x1, acc);
+}
+
 struct StepArgs {
   const PlaneDev *planes;
   const HaloDev *halos;
@@ -408,10 +418,7 @@ __global__ void __launch_bounds__(128) k_plane_step(StepArgs a) {
       acc[0] = -acc[0];
       acc[1] = -acc[1];
     } else if (valid) {
-      if (kind == HALO_NFW)
-        nfw_force<false>(H->nfw, a.tab, xc0, xc1, acc);
-      else
-        nsie_force<false>(H->nsie, xc0, xc1, acc);
+      analytic_halo(H, &a.tab, xc0, xc1, acc);
     }
     al0 -= acc[0];
     al1 -= acc[1];

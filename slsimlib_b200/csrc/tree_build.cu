@@ -380,7 +380,7 @@ __global__ void k_pre2slot(const Slot *s, int nslots, int *pre2slot) {
   if (s[i].pre >= 0) pre2slot[s[i].pre] = i;
 }
 
-__global__ void k_emit_nodes(const Slot *s, int nslots, double theta, GNode *nodes, GNodeF *nodesf) {
+__global__ void k_emit_nodes(const Slot *s, int nslots, double theta, GNode *nodes, GNodeS *snodes) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nslots) return;
   const Slot &b = s[i];
@@ -405,7 +405,11 @@ __global__ void k_emit_nodes(const Slot *s, int nslots, double theta, GNode *nod
   g.bstart = b.child < 0 ? 0 : b.bstart;
   g.bcount = b.child < 0 ? 0 : b.nbig;
   nodes[b.pre] = g;
-  GNodeF f;
+  GNodeS f;
+  f.cxh = (float)g.cx;
+  f.cyh = (float)g.cy;
+  f.cxl = (float)(g.cx - (double)f.cxh);
+  f.cyl = (float)(g.cy - (double)f.cyh);
   f.open2 = (float)g.open2;
   f.near2 = (float)g.near2;
   f.mass = (float)g.mass;
@@ -414,7 +418,11 @@ __global__ void k_emit_nodes(const Slot *s, int nslots, double theta, GNode *nod
   f.q2 = (float)g.q2;
   f.width = (float)g.width;
   f.pad = 0;
-  nodesf[b.pre] = f;
+  f.skip = g.skip;
+  f.leaf = g.leaf;
+  f.start = g.leaf ? g.pstart : g.bstart;
+  f.count = g.leaf ? g.pcount : g.bcount;
+  snodes[b.pre] = f;
 }
 
 __global__ void k_gather_parts(const glb_particle_rec *p, const unsigned *sidx, int n, int multimass,
@@ -643,8 +651,8 @@ Status build_tree(const glb_particle_rec *hp, size_t n, const TreeParams &prm, b
 
   // ---- node array
   CK(T->nodes.alloc(nnodes));
-  CK(T->nodesf.alloc(nnodes));
-  k_emit_nodes<<<nblk(nslots, 256), 256, 0, st>>>(slots.p, nslots, prm.theta, T->nodes.p, T->nodesf.p);
+  CK(T->snodes.alloc(nnodes));
+  k_emit_nodes<<<nblk(nslots, 256), 256, 0, st>>>(slots.p, nslots, prm.theta, T->nodes.p, T->snodes.p);
   DBuf<double> phin;
   CK(phin.alloc(4));
   k_phi_node<<<1, 1, 0, st>>>(slots.p, phin.p);
@@ -670,7 +678,7 @@ Status build_tree(const glb_particle_rec *hp, size_t n, const TreeParams &prm, b
   T->dev.phi_q1 = hphi[2];
   T->dev.phi_q2 = hphi[3];
   T->dev.nodes = T->nodes.p;
-  T->dev.nodesf = T->nodesf.p;
+  T->dev.snodes = T->snodes.p;
   T->dev.parts = T->parts.p;
   T->dev.bigs = T->bigs.p;
   T->dev.prel = T->prel.p;

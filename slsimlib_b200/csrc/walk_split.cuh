@@ -1,20 +1,23 @@
-// Split-precision form of the warp-cooperative walk (same traversal and the
-// same per-ray opening decisions as walk_f64 in walk.cuh):
-//   * ray-minus-node-centre offsets and the opening tests stay in FP64, so
-//     every ray interacts with exactly the cells and particles of the FP64
-//     form;
-//   * far-field and leaf-particle terms are evaluated in FP32 from offsets
-//     that are exact to FP32 rounding: a leaf particle's offset is
-//     (particle - leaf centre of mass, stored in FP32 at build time) +
-//     (leaf centre of mass - ray, from FP64);
-//   * the sums are compensated by blocking: FP32 partial sums of at most 32
-//     terms are flushed into FP64 totals, which bounds the accumulation error
-//     by the per-term rounding instead of letting it grow with the ~1e4 terms
-//     of a walk;
-//   * particles within two softening lengths of the ray, whose point-mass
-//     term is cancelled by a B-spline correction, and the B-spline
-//     corrections themselves are evaluated entirely in FP64 (the close-range
-//     offsets), so no cancellation happens in FP32.
+// Split-precision form of the warp-cooperative walk: the same traversal and
+// the same per-ray opening decisions as walk_f64 (walk.cuh), with the
+// arithmetic moved to FP32 wherever that keeps FP32 relative precision.
+//   * Ray-minus-node offsets are formed from double-float pairs (node centre
+//     hi + lo, ray hi + lo), so each offset has FP32 relative error however
+//     far the cell is from the origin.
+//   * Opening tests are taken in FP32 when the FP32 distance is clearly on
+//     one side of the threshold (further than 4e-6 relative, ~8x the FP32
+//     error bound); otherwise the test is repeated in FP64 on the exact
+//     node, so every ray interacts with exactly the cells of the FP64 form.
+//   * Far-field and leaf-particle terms are evaluated in FP32; a leaf
+//     particle's offset is (particle - leaf centre of mass, stored in FP32 at
+//     build time) + (leaf centre of mass - ray).
+//   * Particles within two softening lengths of the ray, whose point-mass term
+//     is cancelled by a B-spline correction, and the B-spline corrections
+//     themselves, are evaluated entirely in FP64.
+//   * Sums are compensated by blocking: FP32 partial sums of at most 32 terms
+//     are flushed into FP64 totals, which bounds the accumulation error by the
+//     per-term rounding instead of letting it grow with the ~1e4 terms of a
+//     walk.
 #pragma once
 #include "walk.cuh"
 
@@ -23,7 +26,7 @@ namespace glb {
 struct F32Acc {
   float a0, a1, k, g0, g1;
   int cnt;
-  __device__ inline void zero() {
+  __device__ __forceinline__ void zero() {
     a0 = a1 = k = g0 = g1 = 0.f;
     cnt = 0;
   }
@@ -37,41 +40,55 @@ struct F32Acc {
   }
 };
 
+constexpr float kAmbiguous = 4e-6f;  // relative band around a threshold decided in FP64
+
 __device__ __forceinline__ void walk_split(const TreeDev &T, double rx, double ry, bool valid, double *acc) {
   const float inv_pi = (float)(1.0 / kPi);
   const bool screen = T.screen2 != 0.0;
   const float s2f = (float)T.screen2;
   const float iaf = (float)T.inv_area;
+  const float rxh = (float)rx, ryh = (float)ry;
+  const float rxl = (float)(rx - (double)rxh), ryl = (float)(ry - (double)ryh);
   F32Acc fa;
   fa.zero();
   int resume = valid ? 0 : 0x7fffffff;
   int node = 0;
   const int nn = T.nnodes;
   while (node < nn) {
-    const GNode *nd = T.nodes + node;
-    const double cx = nd->cx, cy = nd->cy, open2 = nd->open2;
-    const int skip = max(nd->skip, node + 1);  // forward progress even on a malformed array
+    const float4 *sp = reinterpret_cast<const float4 *>(T.snodes + node);
+    const float4 c0 = __ldg(sp), c1 = __ldg(sp + 1);
+    const int4 c3 = __ldg(reinterpret_cast<const int4 *>(sp + 3));
+    const int skip = max(c3.x, node + 1);  // forward progress even on a malformed array
     const bool act = node >= resume;
-    const double dx = cx - rx, dy = cy - ry;
-    const double r2 = dx * dx + dy * dy;
-    const bool open = act && (r2 < open2);
+    const float dxf = (c0.x - rxh) + (c0.z - rxl), dyf = (c0.y - ryh) + (c0.w - ryl);
+    const float r2f = dxf * dxf + dyf * dyf;
+    bool open = false;
+    if (act) {
+      const float d = r2f - c1.x;
+      if (fabsf(d) > kAmbiguous * c1.x) {
+        open = d < 0.f;
+      } else {
+        const GNode *nd = T.nodes + node;
+        const double dx = nd->cx - rx, dy = nd->cy - ry;
+        open = (dx * dx + dy * dy) < nd->open2;
+      }
+    }
     if (act && !open) {
-      const GNodeF nf = T.nodesf[node];
-      const float dxf = (float)dx, dyf = (float)dy, r2f = (float)r2;
+      // far field: monopole + quadrupole (quadTree.h:1090-1123)
+      const float4 c2 = __ldg(sp + 2);
       const float scr = screen ? __expf(-r2f * s2f) : 1.0f;
       const float ir2 = __fdividef(1.0f, r2f);
       const float ir4 = ir2 * ir2;
-      const float mass = nf.mass, q0 = nf.q0, q1 = nf.q1, q2 = nf.q2;
+      const float mass = c1.z, q0 = c1.w, q1 = c2.x, q2 = c2.y;
       const float ms = mass * inv_pi * scr;
-      float t = mass * iaf - ms * ir2;
+      const float t = mass * iaf - ms * ir2;
       const float qd = (q0 * dxf * dxf + q1 * dyf * dyf + 2.f * q2 * dxf * dyf);
       const float qs = inv_pi * scr * ir4;
       const float t4 = 4.f * qd * qs * ir2;
       fa.a0 += (t + t4) * dxf - (q0 * dxf + q2 * dyf) * qs;
       fa.a1 += (t + t4) * dyf - (q1 * dyf + q2 * dxf) * qs;
-      t = -2.0f * ms * ir4;
-      fa.g0 += 0.5f * (dxf * dxf - dyf * dyf) * t;
-      fa.g1 += dxf * dyf * t;
+      fa.g0 -= ms * ir2 * ((dxf * dxf - dyf * dyf) * ir2);
+      fa.g1 -= ms * ir2 * (2.0f * dxf * dyf * ir2);
       fa.k -= iaf * mass;
       if (++fa.cnt >= 32) fa.flush(acc);
       resume = skip;
@@ -80,15 +97,24 @@ __device__ __forceinline__ void walk_split(const TreeDev &T, double rx, double r
       node = skip;
       continue;
     }
-    const bool nearc = open && (r2 < nd->near2);
-    if (nd->leaf) {
-      const int p0 = nd->pstart, p1 = p0 + nd->pcount;
-      const float dxn = (float)dx, dyn = (float)dy;
+    bool nearc = false;
+    if (open) {
+      const float e = r2f - c1.y;
+      if (fabsf(e) > kAmbiguous * c1.y) {
+        nearc = e < 0.f;
+      } else {
+        const GNode *nd = T.nodes + node;
+        const double dx = nd->cx - rx, dy = nd->cy - ry;
+        nearc = (dx * dx + dy * dy) < nd->near2;
+      }
+    }
+    if (c3.y) {  // leaf
+      const int p0 = c3.z, p1 = p0 + c3.w;
       if (open && fa.cnt) fa.flush(acc);
       for (int p = p0; p < p1; ++p) {
         const float4 P = __ldg(T.prel + p);
         if (open) {
-          const float x0 = P.x + dxn, x1 = P.y + dyn;
+          const float x0 = P.x + dxf, x1 = P.y + dyf;
           const float rcm2f = x0 * x0 + x1 * x1;
           if (rcm2f < 4.0001f * P.w * P.w) {
             // within two softening lengths: the point mass and any B-spline
@@ -106,7 +132,7 @@ __device__ __forceinline__ void walk_split(const TreeDev &T, double rx, double r
             acc[4] += y0 * y1 * tmp;
             acc[2] -= m * T.inv_area;
             const double size = (double)Q.w;
-            if (nearc && size < nd->width && rr < 4 * size * size)
+            if (nearc && size < T.nodes[node].width && rr < 4 * size * size)
               bspline_f64<false>(y0, y1, sqrt(rr), m, size, 0.0, acc);
           } else {
             const float scr = screen ? __expf(-rcm2f * s2f) : 1.0f;
@@ -128,7 +154,7 @@ __device__ __forceinline__ void walk_split(const TreeDev &T, double rx, double r
       node = skip;
     } else {
       if (__any_sync(kFull, nearc)) {
-        const int b0 = nd->bstart, b1 = b0 + nd->bcount;
+        const int b0 = c3.z, b1 = b0 + c3.w;
         for (int b = b0; b < b1; ++b) {
           const float4 P = __ldg(T.bigs + b);
           if (nearc) {

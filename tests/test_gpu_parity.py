@@ -23,13 +23,26 @@ def pack(a, k, g, ph):
     return np.concatenate([a, k[:, None], g, ph[:, None]], axis=1)
 
 
+def vec_err(a, b, floor_frac=1e-6):
+    """|a-b| / max(|b|, floor_frac * median |b|) for 2-vectors (alpha, gamma)."""
+    nb = np.hypot(b[:, 0], b[:, 1])
+    floor = max(floor_frac * np.median(nb), 1e-300)
+    return np.hypot(*(a - b).T) / np.maximum(nb, floor)
+
+
+def scal_err(a, b, floor_frac):
+    floor = max(floor_frac * np.max(np.abs(b)), 1e-300)
+    return np.abs(a - b) / np.maximum(np.abs(b), floor)
+
+
 def force_err(f, ref):
-    """Largest relative error over alpha, kappa, gamma (columns 0-5) and over
-    the potential (column 6), whose sums of logarithms pass through zero, so
-    its floor is 1e-3 of the column's median magnitude."""
-    e = rel_err(f[:, :6], ref[:, :6])
-    ep = rel_err(f[:, 6:], ref[:, 6:], floor_frac=1e-3)
-    return max(np.max(e), np.max(ep)), np.concatenate([e.max(axis=0), ep.max(axis=0)])
+    """Largest relative error of alpha (vector), kappa, gamma (vector) and the
+    potential.  kappa and phi pass through zero (the potential is a sum of
+    logarithms), so their floors are 1e-6 and 1e-3 of the column's largest
+    magnitude."""
+    cols = np.array([vec_err(f[:, 0:2], ref[:, 0:2]).max(), scal_err(f[:, 2], ref[:, 2], 1e-6).max(),
+                     vec_err(f[:, 3:5], ref[:, 3:5]).max(), scal_err(f[:, 6], ref[:, 6], 1e-3).max()])
+    return cols.max(), cols
 
 
 def make_lens(spec: synth.LensSpec) -> glb.Lens:
