@@ -147,6 +147,24 @@ int glb_lens_rayshoot_device(glb_lens *l, size_t n, const double *x_dev, const d
 int glb_gridmap(glb_lens *l, size_t n1d, const double *center, double range, double *y, double *A,
                 int precision);
 
+/* No counterpart in the reference.  glb_lens_rayshoot_device for callers that
+ * cannot allocate device memory while they shoot rays: cudaMalloc / cudaFree
+ * synchronise the whole device and can fail under a memory cap, which grid
+ * refinement loops shooting a few thousand rays at a time, applications that
+ * reserve all their memory up front, or processes sharing a GPU under a quota
+ * cannot accept.  This entry point allocates nothing: its scratch is one
+ * fixed device array of about 13.5 MB inside the library, held by every GPU
+ * that loads the library until the process exits.  Limits: n <= 65536 rays
+ * per call, at most 64 lens planes and 256 halos (larger calls return
+ * GLB_ERR_ARG).  The first call on a device does a one-time set-up (looks up
+ * the array's device address and copies the NFW tables) and should come
+ * before any stream capture.  All calls share the one array, so calls that
+ * overlap on the GPU (different streams or threads) race; serialise them.
+ * Buffers are device pointers; the call returns once the work is enqueued on
+ * `stream` (NULL: the lens's own stream). */
+int glb_lens_rayshoot_noalloc(glb_lens *l, size_t n, const double *x_dev, const double *zs_dev,
+                              double *y_dev, double *A_dev, int precision, void *stream);
+
 /* Measurement aid with no counterpart in the reference: shoots n rays (host
  * buffers) in FP64 and returns the interaction counts summed over rays and
  * planes: counts[0..4] = nodes tested, far-field cells, leaf point masses,

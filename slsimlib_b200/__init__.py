@@ -53,7 +53,7 @@ EXPORTED = [
     "glb_halo_params", "glb_halo_destroy",
     "glb_lens_create", "glb_lens_destroy", "glb_lens_insert_halo", "glb_lens_nplanes", "glb_lens_planes",
     "glb_lens_reset_source", "glb_lens_rayshoot", "glb_lens_rayshoot_device", "glb_gridmap",
-    "glb_lens_last_timing", "glb_lens_count_interactions",
+    "glb_lens_last_timing", "glb_lens_count_interactions", "glb_lens_rayshoot_noalloc",
 ]
 
 
@@ -104,6 +104,7 @@ def load_library():
     L.glb_gridmap.argtypes = [_vp, C.c_size_t, _vp, C.c_double, _vp, _vp, C.c_int]
     L.glb_lens_last_timing.argtypes = [_vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.glb_lens_count_interactions.argtypes = [_vp, C.c_size_t, _vp, _vp, _vp]
+    L.glb_lens_rayshoot_noalloc.argtypes = [_vp, C.c_size_t, _vp, _vp, _vp, _vp, C.c_int, _vp]
     _lib = L
     return L
 

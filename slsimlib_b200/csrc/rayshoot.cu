@@ -1218,3 +1218,181 @@ int glb_lens_last_timing(glb_lens *l, double *kernel_ms, double *total_ms) {
 }
 
 }  // extern "C"
+
+// ======================================================= allocation-free entry
+// glb_lens_rayshoot_noalloc: the same multi-plane pass as
+// glb_lens_rayshoot_device for callers that must not allocate device memory
+// while they shoot rays -- a cudaMalloc / cudaFree pair synchronises the whole
+// device and may fail under a memory cap, which latency-bound callers (grid
+// refinement rounds that shoot a few thousand rays at a time, an application
+// that reserved its memory up front, or a process sharing the GPU under a
+// hard quota) cannot accept.  All scratch memory lives in one file-scope
+// device array of fixed size, held by every GPU that loads the library until
+// the process exits.
+namespace {
+
+constexpr size_t kNoAllocMaxRays = 65536;  // rays per call
+constexpr int kNoAllocMaxPlanes = 64;
+constexpr int kNoAllocMaxHalos = 256;
+constexpr size_t kNoAllocSortBytes = 4u << 20;  // radix-sort temporary storage
+
+constexpr size_t align256(size_t b) { return (b + 255) / 256 * 256; }
+constexpr size_t kOffState = 0;
+constexpr size_t kOffJmax = kOffState + align256(12 * kNoAllocMaxRays * sizeof(double));
+constexpr size_t kOffSrc = kOffJmax + align256(kNoAllocMaxRays * sizeof(int));
+constexpr size_t kOffKeys = kOffSrc + align256(2 * kNoAllocMaxRays * sizeof(double));
+constexpr size_t kOffKeys2 = kOffKeys + align256(kNoAllocMaxRays * sizeof(unsigned));
+constexpr size_t kOffPerm0 = kOffKeys2 + align256(kNoAllocMaxRays * sizeof(unsigned));
+constexpr size_t kOffPerm = kOffPerm0 + align256(kNoAllocMaxRays * sizeof(unsigned));
+constexpr size_t kOffBbox = kOffPerm + align256(kNoAllocMaxRays * sizeof(unsigned));
+constexpr size_t kOffPlanes = kOffBbox + align256(4 * sizeof(unsigned long long));
+constexpr size_t kOffHalos = kOffPlanes + align256(kNoAllocMaxPlanes * sizeof(PlaneDev));
+constexpr size_t kOffPlaneZ = kOffHalos + align256(kNoAllocMaxHalos * sizeof(HaloDev));
+constexpr size_t kOffDl = kOffPlaneZ + align256((kNoAllocMaxPlanes + 1) * sizeof(double));
+constexpr size_t kOffNfw = kOffDl + align256((kNoAllocMaxPlanes + 1) * sizeof(double));
+constexpr size_t kOffSort = kOffNfw + align256(5 * kNfwTable * sizeof(double));
+constexpr size_t kNoAllocBytes = kOffSort + kNoAllocSortBytes;  // about 13.5 MB
+
+__device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+std::mutex g_noalloc_mu;
+unsigned char *g_noalloc_ptr[64] = {};
+
+// Once per device, with that device current: the device address of the
+// scratch array (its host-side name is only a stand-in) and the NFW tables.
+int noalloc_setup(int dev, unsigned char **out) {
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (dev < 0 || dev >= 64) return fail(GLB_ERR_ARG, "device index out of range for the no-alloc scratch");
+  if (!g_noalloc_ptr[dev]) {
+    unsigned char *p = nullptr;
+    CKR(cudaGetSymbolAddress((void **)&p, g_noalloc_scratch));
+    std::call_once(g_nfw_host_once, make_host_tables);
+    const std::vector<double> *src[5] = {&g_nfw_host.x, &g_nfw_host.f, &g_nfw_host.g, &g_nfw_host.g2,
+                                         &g_nfw_host.h};
+    for (int i = 0; i < 5; ++i)
+      CKR(cudaMemcpy(p + kOffNfw + (size_t)i * kNfwTable * sizeof(double), src[i]->data(),
+                     kNfwTable * sizeof(double), cudaMemcpyHostToDevice));
+    size_t tb = 0;
+    CKR(cub::DeviceRadixSort::SortPairs(nullptr, tb, (unsigned *)nullptr, (unsigned *)nullptr,
+                                        (unsigned *)nullptr, (unsigned *)nullptr, (int)kNoAllocMaxRays, 0, 32));
+    if (tb > kNoAllocSortBytes) return fail(GLB_ERR_ARG, "no-alloc scratch: radix-sort temporary storage too small");
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return 0;
+}
+
+}  // namespace
+
+extern "C" int glb_lens_rayshoot_noalloc(glb_lens *l, size_t n, const double *x_dev, const double *zs_dev,
+                                         double *y_dev, double *A_dev, int precision, void *stream) {
+  if (!l) return fail(GLB_ERR_ARG, "null lens");
+  if (n > kNoAllocMaxRays)
+    return fail(GLB_ERR_ARG, "glb_lens_rayshoot_noalloc: at most 65536 rays per call");
+  if (n > 0 && (!x_dev || !y_dev || !A_dev)) return fail(GLB_ERR_ARG, "null buffer");
+  if (precision != GLB_PREC_FP64 && precision != GLB_PREC_SPLIT) return fail(GLB_ERR_ARG, "unknown precision");
+  size_t np = l->main.size(), nh = 0;
+  for (const PlaneHost &p : l->main) nh += p.halos.size();
+  if (np > (size_t)kNoAllocMaxPlanes || nh > (size_t)kNoAllocMaxHalos)
+    return fail(GLB_ERR_ARG, "glb_lens_rayshoot_noalloc: at most 64 planes and 256 halos");
+  if (int rc = set_dev(l->device)) return rc;
+  unsigned char *S = nullptr;
+  if (int rc = noalloc_setup(l->device, &S)) return rc;
+  cudaStream_t s = stream ? (cudaStream_t)stream : l->stream;
+  if (n == 0) return 0;
+  if (np == 0) {
+    k_identity_rays<<<nblk(n, 256), 256, 0, s>>>(x_dev, n, y_dev, A_dev);
+    CKR(cudaGetLastError());
+    return 0;
+  }
+  // plane and halo descriptors of this lens (host stack arrays, no heap),
+  // copied into the scratch; pageable copies are staged before they return
+  PlaneDev P[kNoAllocMaxPlanes];
+  HaloDev H[kNoAllocMaxHalos];
+  int nhd = 0;
+  for (size_t j = 0; j < np; ++j) {
+    PlaneDev &p = P[j];
+    p.Dphys = l->Dl[j] / (1 + l->plane_z[j]);
+    p.Gfac = l->charge * l->Dl[j] / (1 + l->plane_z[j]);
+    p.aa = l->dDl[j + 1] / l->Dl[j + 1];
+    p.bb = l->Dl[j] / l->Dl[j + 1];
+    p.halo0 = nhd;
+    p.nhalo = (int)l->main[j].halos.size();
+    for (glb_halo *h : l->main[j].halos) H[nhd++] = make_halo_dev(*h);
+  }
+  PlaneDev *d_planes = (PlaneDev *)(S + kOffPlanes);
+  HaloDev *d_halos = (HaloDev *)(S + kOffHalos);
+  double *d_planez = (double *)(S + kOffPlaneZ), *d_Dl = (double *)(S + kOffDl);
+  CKR(cudaMemcpyAsync(d_planes, P, np * sizeof(PlaneDev), cudaMemcpyHostToDevice, s));
+  if (nhd) CKR(cudaMemcpyAsync(d_halos, H, nhd * sizeof(HaloDev), cudaMemcpyHostToDevice, s));
+  CKR(cudaMemcpyAsync(d_planez, l->plane_z.data(), (np + 1) * sizeof(double), cudaMemcpyHostToDevice, s));
+  CKR(cudaMemcpyAsync(d_Dl, l->Dl.data(), (np + 1) * sizeof(double), cudaMemcpyHostToDevice, s));
+
+  double *st = (double *)(S + kOffState);
+  int *jmax_ray = (int *)(S + kOffJmax);
+  double *src_ray = (double *)(S + kOffSrc);
+  unsigned *keys = (unsigned *)(S + kOffKeys), *keys2 = (unsigned *)(S + kOffKeys2);
+  unsigned *perm0 = (unsigned *)(S + kOffPerm0), *perm = (unsigned *)(S + kOffPerm);
+  unsigned long long *bbox = (unsigned long long *)(S + kOffBbox);
+  if (n >= 64) {
+    // the bounding box starts from sentinels on every call
+    static const unsigned long long init[4] = {~0ull, ~0ull, 0ull, 0ull};
+    CKR(cudaMemcpyAsync(bbox, init, sizeof(init), cudaMemcpyHostToDevice, s));
+    k_ray_bbox<<<std::min(nblk(n, 256), 1184), 256, 0, s>>>(x_dev, n, bbox);
+    k_ray_morton<<<nblk(n, 256), 256, 0, s>>>(x_dev, n, bbox, keys, perm0);
+    size_t tb = kNoAllocSortBytes;
+    CKR(cub::DeviceRadixSort::SortPairs(S + kOffSort, tb, keys, keys2, perm0, perm, (int)n, 0, 32, s));
+  } else {
+    k_identity<<<nblk(n, 256), 256, 0, s>>>(perm, n);
+  }
+  SrcArgs sa{l->cosmo, d_planez, d_Dl, (int)np};
+  k_init_state<<<nblk(n, 256), 256, 0, s>>>(x_dev, zs_dev, perm, n, st, jmax_ray, src_ray, sa);
+
+  StepArgs a;
+  a.planes = d_planes;
+  a.halos = d_halos;
+  const double *T = (const double *)(S + kOffNfw);
+  a.tab = NFWTables{T, T + kNfwTable, T + 2 * kNfwTable, T + 3 * kNfwTable, T + 4 * kNfwTable};
+  a.st = st;
+  a.n = n;
+  a.charge = l->charge;
+  a.counts = nullptr;
+  a.jmax_ray = zs_dev ? jmax_ray : nullptr;
+  a.src_ray = zs_dev ? src_ray : nullptr;
+  int jmax_launch = (int)np;
+  a.jmax = (int)np;
+  a.dls_ds = 0;
+  a.d_ds = 0;
+  if (!zs_dev) {
+    double source_z = l->toggle_source_plane ? l->zs_implant : l->plane_z.back();
+    if (source_z == l->plane_z.back()) {
+      a.dls_ds = l->dDl.back() / l->Dl.back();
+      a.d_ds = l->Dl[np - 1] / l->Dl.back();
+    } else {
+      double Ds = coordist(l->cosmo, source_z), Dls;
+      int jm;
+      if (source_z <= l->plane_z[0]) {
+        jm = 0;
+        Dls = Ds;
+      } else {
+        jm = (int)np;
+        while (l->plane_z[jm - 1] > source_z) --jm;
+        Dls = coordist2(l->cosmo, l->plane_z[jm - 1], source_z);
+      }
+      a.jmax = jm;
+      a.dls_ds = Dls / Ds;
+      if (jm > 0) a.d_ds = l->Dl[jm - 1] / Ds;
+      jmax_launch = jm;
+    }
+  }
+  for (int j = 0; j < jmax_launch; ++j) {
+    a.j = j;
+    if (precision == GLB_PREC_SPLIT)
+      k_plane_step<GLB_PREC_SPLIT><<<nblk(n, 128), 128, 0, s>>>(a);
+    else
+      k_plane_step<GLB_PREC_FP64><<<nblk(n, 128), 128, 0, s>>>(a);
+  }
+  k_finish<<<nblk(n, 256), 256, 0, s>>>(st, perm, n, y_dev, A_dev);
+  CKR(cudaGetLastError());
+  return 0;
+}
