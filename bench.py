@@ -281,7 +281,7 @@ def main():
         clocks = clk.summary()
         value = world * n * args.steps / (ms / 1e3)
         nplanes = lens.getNplanes()
-        V, F, P, B, S = [int(c) for c in counts]
+        V, F, P, B, S, Wn, Wp = [int(c) for c in counts]
         alg_flops = (FLOPS["V"] * V + FLOPS["F"] * F + FLOPS["P"] * P + FLOPS["B"] * B + FLOPS["S"] * S
                      + FLOPS["rec"] * n * nplanes)
         sm = clocks.get("sm_mhz") or 1965.0
@@ -307,7 +307,8 @@ def main():
                          "kernel": "k_plane_step<split>", "kernel_ms_per_step": k_ms,
                          "peak_note": "FP32 CUDA-core FMA rate at the sampled SM clock (148 SMs x 128 lanes x 2)",
                          "alg_flops_per_step": alg_flops,
-                         "counts": {"V": V, "F": F, "P": P, "B": B, "S": S}},
+                         "counts": {"V": V, "F": F, "P": P, "B": B, "S": S},
+                         "lane_efficiency": {"nodes": V / max(Wn, 1), "leaf_particles": P / max(Wp, 1)}},
             "gpu_launches": args.steps * (4 + nplanes),
             "clocks": clocks,
         }

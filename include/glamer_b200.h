@@ -169,7 +169,9 @@ int glb_lens_rayshoot_noalloc(glb_lens *l, size_t n, const double *x_dev, const 
  * buffers) in FP64 and returns the interaction counts summed over rays and
  * planes: counts[0..4] = nodes tested, far-field cells, leaf point masses,
  * big-particle distance checks, B-spline corrections (the event counts of the
- * algorithmic-flop roofline). */
+ * algorithmic-flop roofline); counts[5..6] = node-loop and leaf-particle-loop
+ * iterations summed over lanes (32 per warp iteration), whose ratio to
+ * counts[0] and counts[2] is the lane efficiency of the warp-cooperative walk. */
 int glb_lens_count_interactions(glb_lens *l, size_t n, const double *x, const double *zs,
                                 unsigned long long *counts);
 

@@ -324,10 +324,11 @@ class Lens:
 
     def count_interactions(self, x, source_zs=None) -> np.ndarray:
         """Interaction counts (nodes tested, far cells, leaf point masses,
-        big-particle checks, B-splines) summed over rays and planes."""
+        big-particle checks, B-splines) summed over rays and planes, then the
+        node-loop and leaf-particle-loop iterations summed over lanes."""
         x = _f64(x, (-1, 2))
         zs = None if source_zs is None else _f64(source_zs)
-        out = np.zeros(5, dtype=np.uint64)
+        out = np.zeros(7, dtype=np.uint64)
         _check(load_library().glb_lens_count_interactions(self._h, len(x), _p(x), _p(zs), _p(out)))
         return out
 

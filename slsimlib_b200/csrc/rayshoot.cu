@@ -369,7 +369,7 @@ struct StepArgs {
   const int *jmax_ray;  // per-ray source planes (or null)
   const double *src_ray;
   double charge;
-  unsigned long long *counts;  // V F P B S totals (counting launches only)
+  unsigned long long *counts;  // V F P B S Wn Wp totals (counting launches only)
 };
 
 // One lens plane for every ray: LensPlaneSingular::force + the recursion of
@@ -406,8 +406,8 @@ __global__ void __launch_bounds__(128) k_plane_step(StepArgs a) {
       if (COUNT) {
         WalkCount wc;
         particle_halo_acc<PREC, false, true>(H->tree, xc0, xc1, valid, acc, &wc);
-        unsigned long long v[5] = {wc.V, wc.F, wc.P, wc.B, wc.S};
-        for (int c = 0; c < 5; ++c) {
+        unsigned long long v[7] = {wc.V, wc.F, wc.P, wc.B, wc.S, wc.Wn, wc.Wp};
+        for (int c = 0; c < 7; ++c) {
           for (int o = 16; o > 0; o >>= 1) v[c] += __shfl_xor_sync(kFull, v[c], o);
           if ((threadIdx.x & 31) == 0) atomicAdd(a.counts + c, v[c]);
         }
@@ -1190,8 +1190,8 @@ int glb_lens_count_interactions(glb_lens *l, size_t n, const double *x, const do
   CKR(dx.alloc(2 * n));
   CKR(dy.alloc(2 * n));
   CKR(dA.alloc(4 * n));
-  CKR(dc.alloc(5));
-  CKR(cudaMemsetAsync(dc.p, 0, 5 * sizeof(unsigned long long), l->stream));
+  CKR(dc.alloc(7));
+  CKR(cudaMemsetAsync(dc.p, 0, 7 * sizeof(unsigned long long), l->stream));
   CKR(cudaMemcpyAsync(dx.p, x, 2 * n * sizeof(double), cudaMemcpyHostToDevice, l->stream));
   if (zs) {
     CKR(dzs.alloc(n));
@@ -1199,7 +1199,7 @@ int glb_lens_count_interactions(glb_lens *l, size_t n, const double *x, const do
   }
   if (int rc = rayshoot_device(l, n, dx.p, zs ? dzs.p : nullptr, dy.p, dA.p, GLB_PREC_FP64, l->stream, dc.p))
     return rc;
-  CKR(cudaMemcpyAsync(counts, dc.p, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, l->stream));
+  CKR(cudaMemcpyAsync(counts, dc.p, 7 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, l->stream));
   CKR(cudaStreamSynchronize(l->stream));
   return 0;
 }

@@ -19,8 +19,10 @@ constexpr unsigned kFull = 0xffffffffu;
 // Interaction counts of one ray's walk, for the algorithmic-flop roofline:
 // V nodes tested, F far-field cells, P leaf point masses, B big-particle
 // distance checks, S B-spline corrections applied.
+// Wn / Wp count the warp's node-loop and leaf-particle-loop iterations (the
+// union over its 32 rays), for the lane-efficiency of the warp-cooperative walk.
 struct WalkCount {
-  unsigned long long V = 0, F = 0, P = 0, B = 0, S = 0;
+  unsigned long long V = 0, F = 0, P = 0, B = 0, S = 0, Wn = 0, Wp = 0;
 };
 
 // b_spline_profile, include/quadTree.h:147-190 (point mass subtracted).
@@ -74,6 +76,7 @@ __device__ __forceinline__ void walk_f64(const TreeDev &T, double rx, double ry,
     const double dx = cx - rx, dy = cy - ry;
     const double r2 = dx * dx + dy * dy;
     const bool open = act && (r2 < open2);
+    if (COUNT) wc->Wn++;
     if (COUNT && act) wc->V++;
     if (act && !open) {
       if (COUNT) wc->F++;
@@ -110,6 +113,7 @@ __device__ __forceinline__ void walk_f64(const TreeDev &T, double rx, double ry,
       const double width = nd->width;
       for (int p = p0; p < p1; ++p) {
         const float4 P = __ldg(T.parts + p);
+        if (COUNT) wc->Wp++;
         if (open) {
           // leaf particle as a point mass (quadTree.h:1017-1046)
           const double x0 = (double)P.x - rx, x1 = (double)P.y - ry;
