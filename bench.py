@@ -287,7 +287,7 @@ def main():
         sm = clocks.get("sm_mhz") or 1965.0
         peak = fp32_peak_tflops(sm)
         achieved = alg_flops / (k_ms / 1e3) / 1e12
-        cpu = None if args.no_cpu else cpu_reference(spec, n1d, 2048 if args.small else 8192)
+        cpu = None if args.no_cpu else cpu_reference(spec, n1d, 4096 if args.small else 65536)
         line = {
             "metric": METRIC, "value": value, "unit": "rays/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",

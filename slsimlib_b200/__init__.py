@@ -174,7 +174,7 @@ class TreeQuadParticles:
         return v.value
 
     def __del__(self):
-        if getattr(self, "_h", None):
+        if getattr(self, "_h", None) and _lib is not None:
             load_library().glb_tree_destroy(self._h)
             self._h = None
 
@@ -338,7 +338,7 @@ class Lens:
         return k.value, t.value
 
     def __del__(self):
-        if getattr(self, "_h", None):
+        if getattr(self, "_h", None) and _lib is not None:
             load_library().glb_lens_destroy(self._h)
             self._h = None
 

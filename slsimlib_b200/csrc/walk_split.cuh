@@ -42,6 +42,43 @@ struct F32Acc {
 
 constexpr float kAmbiguous = 4e-6f;  // relative band around a threshold decided in FP64
 
+// Exact FP64 threshold test for the rare rays in the ambiguity band.
+__device__ __noinline__ bool node_test_f64(const GNode *nd, double rx, double ry, int which) {
+  const double dx = nd->cx - rx, dy = nd->cy - ry;
+  return (dx * dx + dy * dy) < (which ? nd->near2 : nd->open2);
+}
+
+struct Near64 {
+  double a0, a1, k, g0, g1;
+};
+
+// A leaf particle within two softening lengths of the ray: the point mass and
+// its B-spline correction in FP64, exactly as walk_f64 evaluates them.
+__device__ __noinline__ Near64 near_particle_f64(float4 Q, double rx, double ry, double screen2, double inv_area,
+                                                  bool nearc, double width) {
+  Near64 o;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  const double y0 = (double)Q.x - rx, y1 = (double)Q.y - ry;
+  double rr = y0 * y0 + y1 * y1;
+  const double scr = screen2 != 0.0 ? exp(-rr * screen2) : 1.0;
+  if (rr < 1e-20) rr = 1e-20;
+  const double m = (double)Q.z, ir2 = 1.0 / rr, prefac = m * scr * ir2 * (1.0 / kPi);
+  acc[0] = (inv_area * m - prefac) * y0;
+  acc[1] = (inv_area * m - prefac) * y1;
+  const double tmp = -2.0 * prefac * ir2;
+  acc[3] = 0.5 * (y0 * y0 - y1 * y1) * tmp;
+  acc[4] = y0 * y1 * tmp;
+  acc[2] = -m * inv_area;
+  const double size = (double)Q.w;
+  if (nearc && size < width && rr < 4 * size * size) bspline_f64<false>(y0, y1, sqrt(rr), m, size, 0.0, acc);
+  o.a0 = acc[0];
+  o.a1 = acc[1];
+  o.k = acc[2];
+  o.g0 = acc[3];
+  o.g1 = acc[4];
+  return o;
+}
+
 __device__ __forceinline__ void walk_split(const TreeDev &T, double rx, double ry, bool valid, double *acc) {
   const float inv_pi = (float)(1.0 / kPi);
   const bool screen = T.screen2 != 0.0;
@@ -65,13 +102,8 @@ __device__ __forceinline__ void walk_split(const TreeDev &T, double rx, double r
     bool open = false;
     if (act) {
       const float d = r2f - c1.x;
-      if (fabsf(d) > kAmbiguous * c1.x) {
-        open = d < 0.f;
-      } else {
-        const GNode *nd = T.nodes + node;
-        const double dx = nd->cx - rx, dy = nd->cy - ry;
-        open = (dx * dx + dy * dy) < nd->open2;
-      }
+      open = d < 0.f;
+      if (fabsf(d) <= kAmbiguous * c1.x) open = node_test_f64(T.nodes + node, rx, ry, 0);
     }
     if (act && !open) {
       // far field: monopole + quadrupole (quadTree.h:1090-1123)
@@ -100,57 +132,46 @@ __device__ __forceinline__ void walk_split(const TreeDev &T, double rx, double r
     bool nearc = false;
     if (open) {
       const float e = r2f - c1.y;
-      if (fabsf(e) > kAmbiguous * c1.y) {
-        nearc = e < 0.f;
-      } else {
-        const GNode *nd = T.nodes + node;
-        const double dx = nd->cx - rx, dy = nd->cy - ry;
-        nearc = (dx * dx + dy * dy) < nd->near2;
-      }
+      nearc = e < 0.f;
+      if (fabsf(e) <= kAmbiguous * c1.y) nearc = node_test_f64(T.nodes + node, rx, ry, 1);
     }
     if (c3.y) {  // leaf
       const int p0 = c3.z, p1 = p0 + c3.w;
       if (open && fa.cnt) fa.flush(acc);
-      for (int p = p0; p < p1; ++p) {
-        const float4 P = __ldg(T.prel + p);
-        if (open) {
-          const float x0 = P.x + dxf, x1 = P.y + dyf;
-          const float rcm2f = x0 * x0 + x1 * x1;
-          if (rcm2f < 4.0001f * P.w * P.w) {
-            // within two softening lengths: the point mass and any B-spline
-            // correction cancel, so both are done in FP64 exactly as walk_f64
-            const float4 Q = __ldg(T.parts + p);
-            const double y0 = (double)Q.x - rx, y1 = (double)Q.y - ry;
-            double rr = y0 * y0 + y1 * y1;
-            const double scr = screen ? exp(-rr * T.screen2) : 1.0;
-            if (rr < 1e-20) rr = 1e-20;
-            const double m = (double)Q.z, ir2 = 1.0 / rr, prefac = m * scr * ir2 * (1.0 / kPi);
-            acc[0] += (T.inv_area * m - prefac) * y0;
-            acc[1] += (T.inv_area * m - prefac) * y1;
-            const double tmp = -2.0 * prefac * ir2;
-            acc[3] += 0.5 * (y0 * y0 - y1 * y1) * tmp;
-            acc[4] += y0 * y1 * tmp;
-            acc[2] -= m * T.inv_area;
-            const double size = (double)Q.w;
-            if (nearc && size < T.nodes[node].width && rr < 4 * size * size)
-              bspline_f64<false>(y0, y1, sqrt(rr), m, size, 0.0, acc);
-          } else {
-            const float scr = screen ? __expf(-rcm2f * s2f) : 1.0f;
-            const float m = P.z;
-            const float ir2 = __fdividef(1.0f, rcm2f);
-            const float prefac = m * scr * ir2 * inv_pi;
-            const float ta = iaf * m - prefac;
-            fa.a0 += ta * x0;
-            fa.a1 += ta * x1;
-            // shear terms scaled by 1/r^2 first so that nothing overflows FP32
-            fa.g0 -= prefac * ((x0 * x0 - x1 * x1) * ir2);
-            fa.g1 -= prefac * (2.0f * x0 * x1 * ir2);
-            fa.k -= m * iaf;
+      // particles in chunks of 32 so that the FP32 partial sums stay short
+      for (int q0 = p0; q0 < p1; q0 += 32) {
+        const int q1 = min(q0 + 32, p1);
+        for (int p = q0; p < q1; ++p) {
+          const float4 P = __ldg(T.prel + p);
+          if (open) {
+            const float x0 = P.x + dxf, x1 = P.y + dyf;
+            const float rcm2f = x0 * x0 + x1 * x1;
+            if (rcm2f < fmaxf(4.0001f * P.w * P.w, 1e-12f)) {  // near or (unsoftened) coincident
+              const Near64 o = near_particle_f64(__ldg(T.parts + p), rx, ry, T.screen2, T.inv_area, nearc,
+                                                 T.nodes[node].width);
+              acc[0] += o.a0;
+              acc[1] += o.a1;
+              acc[2] += o.k;
+              acc[3] += o.g0;
+              acc[4] += o.g1;
+            } else {
+              const float scr = screen ? __expf(-rcm2f * s2f) : 1.0f;
+              const float m = P.z;
+              const float ir2 = __fdividef(1.0f, rcm2f);
+              const float prefac = m * scr * ir2 * inv_pi;
+              const float ta = iaf * m - prefac;
+              fa.a0 += ta * x0;
+              fa.a1 += ta * x1;
+              // shear terms scaled by 1/r^2 first so that nothing overflows FP32
+              const float pi2 = prefac * ir2;
+              fa.g0 -= pi2 * (x0 * x0 - x1 * x1);
+              fa.g1 -= pi2 * (2.0f * x0 * x1);
+              fa.k -= m * iaf;
+            }
           }
         }
-        if (((p - p0) & 31) == 31 && open) fa.flush(acc);
+        if (open) fa.flush(acc);
       }
-      if (open) fa.flush(acc);
       node = skip;
     } else {
       if (__any_sync(kFull, nearc)) {
