@@ -41,7 +41,8 @@ enum {
   GLB_ERR_SAME_PLACE = -4,   /* "particles in same place." (quadTree.h:327-329) */
   GLB_ERR_DEPTH = -5,        /* more than 32 tree levels needed */
   GLB_ERR_UNSUPPORTED = -6,  /* a reference feature outside this library's scope */
-  GLB_ERR_NO_DEVICE = -7
+  GLB_ERR_NO_DEVICE = -7,
+  GLB_ERR_TIMEOUT = -8       /* glb_server_wait ran out of time */
 };
 
 /* Precision of the tree walk. */
@@ -174,6 +175,59 @@ int glb_lens_rayshoot_noalloc(glb_lens *l, size_t n, const double *x_dev, const 
  * counts[0] and counts[2] is the lane efficiency of the warp-cooperative walk. */
 int glb_lens_count_interactions(glb_lens *l, size_t n, const double *x, const double *zs,
                                 unsigned long long *counts);
+
+/* --------------------------------------------------- batched lenses */
+
+/* No counterpart in the reference (which shoots one GridMap at a time under a
+ * global mutex, TreeCode_link/gridmap.cpp:15,116-119): the GridMaps of many
+ * lenses (nlens lenses, grid sides n1d[i], centres centers[2i..2i+1], ranges
+ * ranges[i]) shot by one persistent kernel launch.  Each warp takes 8 x 4-ray
+ * grid tiles from a shared counter and carries them through all planes of
+ * their lens.  The lenses stay owned by the caller and must outlive the batch. */
+typedef struct glb_batch glb_batch;
+int glb_batch_create_grids(glb_lens *const *lenses, int nlens, const size_t *n1d, const double *centers,
+                           const double *ranges, int precision, glb_batch **out);
+/* Runs the batch; use_graph != 0 records the launch into a CUDA graph on the
+ * first call and replays it afterwards.  Returns when the results are ready. */
+int glb_batch_run(glb_batch *b, int use_graph);
+/* Times block sizes 64, 128 and 256 (persistent grid each) and keeps the
+ * fastest. */
+int glb_batch_autotune(glb_batch *b, int *best_block, double *best_ms);
+int glb_batch_set_block(glb_batch *b, int block);
+int glb_batch_info(glb_batch *b, size_t *total_rays, double *last_ms, int *block);
+/* y (2 n1d^2) and A (4 n1d^2) of lens i, GridMap order, host memory. */
+int glb_batch_result(glb_batch *b, int i, double *y, double *A);
+int glb_batch_destroy(glb_batch *b);
+
+/* --------------------------------------------------- served requests */
+
+/* No counterpart in the reference (its small-batch callers -- grid refinement
+ * in image and critical-curve finding -- call rayshooterInternal one at a
+ * time under a global mutex).  A resident request loop over `nmodels` lenses
+ * kept on the device: requests (model, rays, source redshift) are queued by
+ * glb_server_submit and admitted in arrival order into batches of at most
+ * max_rays_per_batch rays (bounded by free device memory); a batch launches
+ * as soon as one of `nslots` slots is free, so requests that arrive while
+ * others run are batched and overlap on the GPU.  A request's results do not
+ * depend on what it is batched with.  The lenses must outlive the server. */
+typedef struct glb_server glb_server;
+int glb_server_create(glb_lens *const *models, int nmodels, size_t max_rays_per_batch, int precision, int nslots,
+                      glb_server **out);
+/* Queues n rays x (2n, radians, host) for lens `model` with source redshift
+ * zs (zs < 0: the lens's own source plane).  x, y (2n) and A (4n) must stay
+ * valid until glb_server_wait returns for the ticket. */
+int glb_server_submit(glb_server *s, int model, size_t n, const double *x, double zs, double *y, double *A,
+                      long long *ticket);
+/* Waits for a ticket (timeout_s <= 0: no limit); times (optional, 3 doubles)
+ * gets the submit, start and completion times in seconds of a steady clock. */
+int glb_server_wait(glb_server *s, long long ticket, double timeout_s, double *times);
+int glb_server_poll(glb_server *s, long long ticket, int *done);
+/* stats[0..5]: rays done, requests done, batches, busy seconds (first launch
+ * to last completion), rays per batch budget, requests pending. */
+int glb_server_stats(glb_server *s, double *stats);
+/* Stops the loop; batches already on the GPU finish, queued requests are
+ * dropped. */
+int glb_server_destroy(glb_server *s);
 
 /* Timing of the last rayshoot on this lens: device milliseconds of the
  * per-plane kernels and of the whole call (CUDA events). */

@@ -28,7 +28,7 @@ from .synth import PARTICLE_DTYPE
 
 __all__ = [
     "GlamerError", "load_library", "TreeQuadParticles", "LensHaloParticles", "LensHaloNFW",
-    "LensHaloRealNSIE", "Lens", "GridMap", "PREC_FP64", "PREC_SPLIT", "PARTICLE_DTYPE",
+    "LensHaloRealNSIE", "Lens", "GridMap", "GridBatch", "Server", "PREC_FP64", "PREC_SPLIT", "PARTICLE_DTYPE",
 ]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -44,6 +44,7 @@ GLB_ERR_SAME_PLACE = -4
 GLB_ERR_DEPTH = -5
 GLB_ERR_UNSUPPORTED = -6
 GLB_ERR_NO_DEVICE = -7
+GLB_ERR_TIMEOUT = -8
 
 # every symbol include/glamer_b200.h declares
 EXPORTED = [
@@ -54,6 +55,10 @@ EXPORTED = [
     "glb_lens_create", "glb_lens_destroy", "glb_lens_insert_halo", "glb_lens_nplanes", "glb_lens_planes",
     "glb_lens_reset_source", "glb_lens_rayshoot", "glb_lens_rayshoot_device", "glb_gridmap",
     "glb_lens_last_timing", "glb_lens_count_interactions", "glb_lens_rayshoot_noalloc",
+    "glb_batch_create_grids", "glb_batch_run", "glb_batch_autotune", "glb_batch_set_block", "glb_batch_info",
+    "glb_batch_result", "glb_batch_destroy",
+    "glb_server_create", "glb_server_submit", "glb_server_wait", "glb_server_poll", "glb_server_stats",
+    "glb_server_destroy",
 ]
 
 
@@ -105,6 +110,20 @@ def load_library():
     L.glb_lens_last_timing.argtypes = [_vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.glb_lens_count_interactions.argtypes = [_vp, C.c_size_t, _vp, _vp, _vp]
     L.glb_lens_rayshoot_noalloc.argtypes = [_vp, C.c_size_t, _vp, _vp, _vp, _vp, C.c_int, _vp]
+    L.glb_batch_create_grids.argtypes = [_vp, C.c_int, _vp, _vp, _vp, C.c_int, C.POINTER(_vp)]
+    L.glb_batch_run.argtypes = [_vp, C.c_int]
+    L.glb_batch_autotune.argtypes = [_vp, C.POINTER(C.c_int), C.POINTER(C.c_double)]
+    L.glb_batch_set_block.argtypes = [_vp, C.c_int]
+    L.glb_batch_info.argtypes = [_vp, C.POINTER(C.c_size_t), C.POINTER(C.c_double), C.POINTER(C.c_int)]
+    L.glb_batch_result.argtypes = [_vp, C.c_int, _vp, _vp]
+    L.glb_batch_destroy.argtypes = [_vp]
+    L.glb_server_create.argtypes = [_vp, C.c_int, C.c_size_t, C.c_int, C.c_int, C.POINTER(_vp)]
+    L.glb_server_submit.argtypes = [_vp, C.c_int, C.c_size_t, _vp, C.c_double, _vp, _vp,
+                                    C.POINTER(C.c_longlong)]
+    L.glb_server_wait.argtypes = [_vp, C.c_longlong, C.c_double, _vp]
+    L.glb_server_poll.argtypes = [_vp, C.c_longlong, C.POINTER(C.c_int)]
+    L.glb_server_stats.argtypes = [_vp, _vp]
+    L.glb_server_destroy.argtypes = [_vp]
     _lib = L
     return L
 
@@ -379,3 +398,103 @@ class GridMap:
 
     def alpha(self):
         return self.positions() - self.y
+
+
+# ----------------------------------------------------------- batched lenses
+class GridBatch:
+    """GridMaps of many lenses shot by one persistent launch (optionally
+    replayed from a CUDA graph).  The lenses must outlive the batch."""
+
+    def __init__(self, lenses: Sequence[Lens], n1d: Sequence[int], centers, ranges, precision=PREC_SPLIT):
+        L = load_library()
+        self.lenses = list(lenses)
+        self.n1d = np.ascontiguousarray(n1d, dtype=np.uint64)
+        c = np.ascontiguousarray(centers, dtype=np.float64).reshape(-1, 2)
+        r = np.ascontiguousarray(ranges, dtype=np.float64)
+        handles = (_vp * len(self.lenses))(*[l._h for l in self.lenses])
+        h = _vp()
+        _check(L.glb_batch_create_grids(handles, len(self.lenses), _p(self.n1d), _p(c), _p(r), precision,
+                                        C.byref(h)))
+        self._h = h
+
+    def run(self, use_graph=True) -> float:
+        """Shoots every grid; returns the device milliseconds of the launch."""
+        L = load_library()
+        _check(L.glb_batch_run(self._h, int(use_graph)))
+        return self.info()[1]
+
+    def autotune(self):
+        b, ms = C.c_int(0), C.c_double(0)
+        _check(load_library().glb_batch_autotune(self._h, C.byref(b), C.byref(ms)))
+        return b.value, ms.value
+
+    def set_block(self, block: int):
+        _check(load_library().glb_batch_set_block(self._h, block))
+
+    def info(self):
+        n, ms, b = C.c_size_t(0), C.c_double(0), C.c_int(0)
+        _check(load_library().glb_batch_info(self._h, C.byref(n), C.byref(ms), C.byref(b)))
+        return n.value, ms.value, b.value
+
+    def result(self, i: int):
+        n = int(self.n1d[i]) ** 2
+        y, A = np.zeros((n, 2)), np.zeros((n, 4))
+        _check(load_library().glb_batch_result(self._h, i, _p(y), _p(A)))
+        return y, A
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            load_library().glb_batch_destroy(self._h)
+            self._h = None
+
+
+# ---------------------------------------------------------- served requests
+class Server:
+    """Resident request loop over lenses kept on the device, with continuous
+    batching (see glb_server_create).  The models must outlive the server."""
+
+    def __init__(self, models: Sequence[Lens], max_rays_per_batch: int = 0, precision=PREC_SPLIT, nslots: int = 3):
+        L = load_library()
+        self.models = list(models)
+        handles = (_vp * len(self.models))(*[m._h for m in self.models])
+        h = _vp()
+        _check(L.glb_server_create(handles, len(self.models), max_rays_per_batch, precision, nslots, C.byref(h)))
+        self._h = h
+        self._live = {}
+
+    def submit(self, model: int, x, zs: float = -1.0) -> int:
+        x = _f64(x, (-1, 2))
+        n = len(x)
+        y, A = np.zeros((n, 2)), np.zeros((n, 4))
+        t = C.c_longlong(0)
+        _check(load_library().glb_server_submit(self._h, model, n, _p(x), float(zs), _p(y), _p(A), C.byref(t)))
+        self._live[t.value] = (x, y, A)
+        return t.value
+
+    def wait(self, ticket: int, timeout: float = 0.0):
+        """-> (y, A, (t_submit, t_start, t_done))"""
+        times = np.zeros(3)
+        rc = load_library().glb_server_wait(self._h, ticket, timeout, _p(times))
+        if rc == GLB_ERR_TIMEOUT:
+            raise TimeoutError(load_library().glb_last_error().decode())
+        x, y, A = self._live.pop(ticket)
+        _check(rc)
+        return y, A, tuple(times)
+
+    def poll(self, ticket: int) -> bool:
+        d = C.c_int(0)
+        _check(load_library().glb_server_poll(self._h, ticket, C.byref(d)))
+        return bool(d.value)
+
+    def stats(self):
+        s = np.zeros(6)
+        _check(load_library().glb_server_stats(self._h, _p(s)))
+        return dict(rays=s[0], requests=s[1], batches=s[2], busy_s=s[3], ray_budget=s[4], pending=s[5])
+
+    def close(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            load_library().glb_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()

@@ -1,0 +1,816 @@
+// Batched and served ray shooting.  Included once at the end of rayshoot.cu
+// (same translation unit: it uses that file's kernels, lens objects and
+// helpers).
+//
+// Both patterns run one persistent kernel, k_batch, over a table of chunks.
+// A chunk is up to 32 rays of one lens, handled by one warp from the first to
+// the last plane with the recursion state in registers:
+//   * grid tiles (8 x 4 rays of a GridMap, generated in the kernel from
+//     PositionFromIndex) for many lens realisations of uneven size in one
+//     launch, replayed from a CUDA graph (glb_batch_*);
+//   * ray lists (a served request's rays, sorted along a Morton curve inside
+//     the request) for the resident request loop (glb_server_*).
+// Warps take chunks from a global atomic counter until the table is done, so
+// uneven lenses and requests balance across the SMs.  A chunk never mixes
+// lenses or requests, so every ray's arithmetic, and even its warp's joint
+// traversal, is the same whatever else is in the batch.
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <thread>
+#include <unordered_map>
+
+namespace {
+
+struct LensDev {
+  const PlaneDev *planes;
+  const HaloDev *halos;
+  const double *planez, *Dl;
+  int np;
+  int jmax_default;
+  double dls_default, dds_default;  // the lens's own source plane (Point* overload)
+  double charge;
+  Cosmo cosmo;
+};
+
+struct Chunk {
+  int lens;
+  int kind;   // 0: grid tile of 8 x 4 rays, 1: ray list
+  int n1d;    // grid side
+  int lanes;  // list: rays in this chunk (<= 32)
+  int a, b;   // grid: tile origin (ix0, iy0); list: first sorted ray
+  long long out;  // grid: output offset of the lens's grid
+  double c0, c1, range;
+  double zs;  // source redshift; < 0 for the lens's own source plane
+};
+
+// LensPlaneSingular::force for one plane (planes.cpp:114-161): the plane's
+// halos summed into out = {alpha0, alpha1, kappa, gamma0, gamma1}.
+template <int PREC>
+__device__ __forceinline__ void plane_force(const PlaneDev &P, const HaloDev *halos, const NFWTables *tab,
+                                            double xx0, double xx1, bool valid, double *out) {
+  for (int h = 0; h < P.nhalo; ++h) {
+    const HaloDev *H = halos + P.halo0 + h;
+    const double xc0 = xx0 - H->px, xc1 = xx1 - H->py;
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    if (H->kind == HALO_PARTICLES) {
+      particle_halo_acc<PREC, false>(H->tree, xc0, xc1, valid, acc);
+      acc[0] = -acc[0];
+      acc[1] = -acc[1];
+    } else if (valid) {
+      analytic_halo(H, tab, xc0, xc1, acc);
+    }
+    out[0] -= acc[0];
+    out[1] -= acc[1];
+    out[2] += acc[2];
+    out[3] += acc[3];
+    out[4] += acc[4];
+  }
+}
+
+template <int PREC>
+__global__ void __launch_bounds__(256) k_batch(const Chunk *chunks, int nchunks, const LensDev *lenses,
+                                               NFWTables tab, const double *xs, const unsigned *outidx,
+                                               double *y, double *A, int *counter) {
+  const int lane = threadIdx.x & 31;
+  for (;;) {
+    int c = 0;
+    if (lane == 0) c = atomicAdd(counter, 1);
+    c = __shfl_sync(kFull, c, 0);
+    if (c >= nchunks) break;
+    const Chunk ch = chunks[c];
+    const LensDev &L = lenses[ch.lens];
+    bool valid;
+    double t0 = 0, t1 = 0;
+    long long oi = 0;
+    if (ch.kind == 0) {
+      const int ix = ch.a + (lane & 7), iy = ch.b + (lane >> 3);
+      valid = ix < ch.n1d && iy < ch.n1d;
+      if (valid) {
+        const long long idx = (long long)ix + (long long)iy * ch.n1d;
+        oi = ch.out + idx;
+        if (ch.n1d == 1) {
+          t0 = ch.c0;
+          t1 = ch.c1;
+        } else {  // PositionFromIndex (TreeCode_link/utilities.cpp:149-158)
+          t0 = ch.c0 + ch.range * (1.0 * (double)ix / (double)(ch.n1d - 1) - 0.5);
+          t1 = ch.c1 + ch.range * (1.0 * (double)iy / (double)(ch.n1d - 1) - 0.5);
+        }
+      }
+    } else {
+      valid = lane < ch.lanes;
+      if (valid) {
+        const int k = ch.a + lane;
+        t0 = xs[2 * (size_t)k];
+        t1 = xs[2 * (size_t)k + 1];
+        oi = outidx[k];
+      }
+    }
+    int jmax = L.jmax_default;
+    double dls = L.dls_default, dds = L.dds_default;
+    if (ch.zs >= 0 && valid) {
+      SrcArgs sa{L.cosmo, L.planez, L.Dl, L.np};
+      find_source_plane(sa, ch.zs, jmax, dls, dds);
+    }
+    int jw = valid ? jmax : 0;
+    for (int o = 16; o > 0; o >>= 1) jw = max(jw, __shfl_xor_sync(kFull, jw, o));
+    double sa0 = t0, sa1 = t1;
+    double A0 = 1, A1 = 0, A2 = 0, A3 = 1, s0 = 1, s1 = 0, s2 = 0, s3 = 1;
+    for (int j = 0; j < jw; ++j) {
+      const bool v = valid && j < jmax;
+      const PlaneDev P = L.planes[j];
+      double f[5] = {0, 0, 0, 0, 0};
+      plane_force<PREC>(P, L.halos, &tab, t0 * P.Dphys, t1 * P.Dphys, v, f);
+      if (v) {
+        // include/lens.h:1027-1066
+        double G0 = (f[2] + f[3]) * P.Gfac, G1 = f[4] * P.Gfac, G2 = f[4] * P.Gfac, G3 = (f[2] - f[3]) * P.Gfac;
+        sa0 -= L.charge * f[0];
+        sa1 -= L.charge * f[1];
+        double aa = P.aa, bb = P.bb;
+        if (j >= jmax - 1) {
+          aa = dls;
+          bb = dds;
+        }
+        t0 = bb * t0 + aa * sa0;
+        t1 = bb * t1 + aa * sa1;
+        s0 -= G0 * A0 + G1 * A2;
+        s1 -= G0 * A1 + G1 * A3;
+        s2 -= G2 * A0 + G3 * A2;
+        s3 -= G2 * A1 + G3 * A3;
+        A0 = A0 * bb + s0 * aa;
+        A1 = A1 * bb + s1 * aa;
+        A2 = A2 * bb + s2 * aa;
+        A3 = A3 * bb + s3 * aa;
+      }
+    }
+    if (valid) {
+      y[2 * oi] = t0;
+      y[2 * oi + 1] = t1;
+      A[4 * oi] = A0;
+      A[4 * oi + 1] = A1;
+      A[4 * oi + 2] = A2;
+      A[4 * oi + 3] = A3;
+    }
+  }
+}
+
+// Descriptor of a lens for k_batch; the lens's device tables must be current.
+int make_lens_dev(glb_lens *l, LensDev &d) {
+  if (int rc = upload_lens(l)) return rc;
+  size_t np = l->main.size();
+  d.planes = l->d_planes.p;
+  d.halos = l->d_halos.p;
+  d.planez = l->d_planez.p;
+  d.Dl = l->d_Dl.p;
+  d.np = (int)np;
+  d.charge = l->charge;
+  d.cosmo = l->cosmo;
+  d.jmax_default = (int)np;
+  d.dls_default = 0;
+  d.dds_default = 0;
+  if (np > 0) {
+    double source_z = l->toggle_source_plane ? l->zs_implant : l->plane_z.back();
+    if (source_z == l->plane_z.back()) {
+      d.dls_default = l->dDl.back() / l->Dl.back();
+      d.dds_default = l->Dl[np - 1] / l->Dl.back();
+    } else {
+      double Ds = coordist(l->cosmo, source_z), Dls;
+      int jm;
+      if (source_z <= l->plane_z[0]) {
+        jm = 0;
+        Dls = Ds;
+      } else {
+        jm = (int)np;
+        while (l->plane_z[jm - 1] > source_z) --jm;
+        Dls = coordist2(l->cosmo, l->plane_z[jm - 1], source_z);
+      }
+      d.jmax_default = jm;
+      d.dls_default = Dls / Ds;
+      if (jm > 0) d.dds_default = l->Dl[jm - 1] / Ds;
+    }
+  }
+  return 0;
+}
+
+int persistent_grid(int block, int precision, int *grid) {
+  int dev = 0, sms = 0, per_sm = 0;
+  CKR(cudaGetDevice(&dev));
+  CKR(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  if (precision == GLB_PREC_SPLIT)
+    CKR(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<GLB_PREC_SPLIT>, block, 0));
+  else
+    CKR(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<GLB_PREC_FP64>, block, 0));
+  *grid = sms * std::max(per_sm, 1);
+  return 0;
+}
+
+}  // namespace
+
+// ================================================================ batch plan
+struct glb_batch {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int precision = GLB_PREC_FP64;
+  int block = 128, grid = 0;
+  std::vector<glb_lens *> lenses;
+  std::vector<size_t> n1d, offset;
+  size_t total = 0;
+  DBuf<LensDev> d_lenses;
+  DBuf<Chunk> d_chunks;
+  int nchunks = 0;
+  DBuf<double> y, A;
+  DBuf<int> counter;
+  NFWTables tab{};
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  float last_ms = 0;
+};
+
+namespace {
+int batch_enqueue(glb_batch *b) {
+  CKR(cudaMemsetAsync(b->counter.p, 0, sizeof(int), b->stream));
+  if (b->precision == GLB_PREC_SPLIT)
+    k_batch<GLB_PREC_SPLIT><<<b->grid, b->block, 0, b->stream>>>(b->d_chunks.p, b->nchunks, b->d_lenses.p, b->tab,
+                                                                 nullptr, nullptr, b->y.p, b->A.p, b->counter.p);
+  else
+    k_batch<GLB_PREC_FP64><<<b->grid, b->block, 0, b->stream>>>(b->d_chunks.p, b->nchunks, b->d_lenses.p, b->tab,
+                                                                nullptr, nullptr, b->y.p, b->A.p, b->counter.p);
+  CKR(cudaGetLastError());
+  return 0;
+}
+}  // namespace
+
+extern "C" {
+
+int glb_batch_create_grids(glb_lens *const *lenses, int nlens, const size_t *n1d, const double *centers,
+                           const double *ranges, int precision, glb_batch **out) {
+  if (!out || !lenses || !n1d || !centers || !ranges || nlens <= 0) return fail(GLB_ERR_ARG, "null argument");
+  if (precision != GLB_PREC_FP64 && precision != GLB_PREC_SPLIT) return fail(GLB_ERR_ARG, "unknown precision");
+  if (int rc = need_device()) return rc;
+  auto b = std::make_unique<glb_batch>();
+  CKR(cudaGetDevice(&b->device));
+  CKR(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+  CKR(cudaEventCreate(&b->e0));
+  CKR(cudaEventCreate(&b->e1));
+  b->precision = precision;
+  std::vector<LensDev> L(nlens);
+  std::vector<Chunk> C;
+  for (int i = 0; i < nlens; ++i) {
+    if (!lenses[i]) return fail(GLB_ERR_ARG, "null lens");
+    if (lenses[i]->device != b->device) return fail(GLB_ERR_ARG, "all lenses of a batch must be on one device");
+    if (n1d[i] < 1 || n1d[i] > 46340) return fail(GLB_ERR_ARG, "grid side must be in [1, 46340]");
+    if (!(ranges[i] > 0)) return fail(GLB_ERR_ARG, "GridMap range is <= 0!");
+    if (int rc = make_lens_dev(lenses[i], L[i])) return rc;
+    b->lenses.push_back(lenses[i]);
+    b->n1d.push_back(n1d[i]);
+    b->offset.push_back(b->total);
+    int N = (int)n1d[i];
+    for (int iy = 0; iy < N; iy += 4)
+      for (int ix = 0; ix < N; ix += 8) {
+        Chunk c;
+        memset(&c, 0, sizeof(c));
+        c.lens = i;
+        c.kind = 0;
+        c.n1d = N;
+        c.a = ix;
+        c.b = iy;
+        c.out = (long long)b->total;
+        c.c0 = centers[2 * i];
+        c.c1 = centers[2 * i + 1];
+        c.range = ranges[i];
+        c.zs = -1;
+        C.push_back(c);
+      }
+    b->total += (size_t)N * N;
+  }
+  if (C.size() > 0x7fffffffull) return fail(GLB_ERR_ARG, "too many chunks");
+  // the largest lenses' chunks first: uneven lenses finish together
+  std::stable_sort(C.begin(), C.end(), [&](const Chunk &x, const Chunk &y) { return x.n1d > y.n1d; });
+  b->nchunks = (int)C.size();
+  CKR(b->d_lenses.alloc(nlens));
+  CKR(b->d_chunks.alloc(C.size()));
+  CKR(b->y.alloc(2 * b->total));
+  CKR(b->A.alloc(4 * b->total));
+  CKR(b->counter.alloc(1));
+  CKR(cudaMemcpy(b->d_lenses.p, L.data(), nlens * sizeof(LensDev), cudaMemcpyHostToDevice));
+  CKR(cudaMemcpy(b->d_chunks.p, C.data(), C.size() * sizeof(Chunk), cudaMemcpyHostToDevice));
+  if (int rc = device_nfw_tables(b->tab)) return rc;
+  if (int rc = persistent_grid(b->block, precision, &b->grid)) return rc;
+  *out = b.release();
+  return 0;
+}
+
+int glb_batch_run(glb_batch *b, int use_graph) {
+  if (!b) return fail(GLB_ERR_ARG, "null batch");
+  if (int rc = set_dev(b->device)) return rc;
+  CKR(cudaEventRecord(b->e0, b->stream));
+  if (use_graph) {
+    if (!b->exec) {
+      CKR(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+      int rc = batch_enqueue(b);
+      cudaGraph_t g = nullptr;
+      cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+      if (rc) return rc;
+      CKR(e);
+      b->graph = g;
+      CKR(cudaGraphInstantiate(&b->exec, b->graph, 0));
+    }
+    CKR(cudaGraphLaunch(b->exec, b->stream));
+  } else {
+    if (int rc = batch_enqueue(b)) return rc;
+  }
+  CKR(cudaEventRecord(b->e1, b->stream));
+  CKR(cudaEventSynchronize(b->e1));
+  CKR(cudaEventElapsedTime(&b->last_ms, b->e0, b->e1));
+  return 0;
+}
+
+// Project autotuner: times the candidate block sizes (each with its persistent
+// grid) and keeps the fastest.  The graph is rebuilt on the next graph run.
+int glb_batch_autotune(glb_batch *b, int *best_block, double *best_ms) {
+  if (!b) return fail(GLB_ERR_ARG, "null batch");
+  if (int rc = set_dev(b->device)) return rc;
+  const int cands[3] = {64, 128, 256};
+  double best = 1e300;
+  int bb = b->block, bg = b->grid;
+  for (int c : cands) {
+    b->block = c;
+    if (int rc = persistent_grid(c, b->precision, &b->grid)) return rc;
+    double t = 1e300;
+    for (int rep = 0; rep < 2; ++rep) {
+      if (int rc = glb_batch_run(b, 0)) return rc;
+      t = std::min(t, (double)b->last_ms);
+    }
+    if (t < best) {
+      best = t;
+      bb = c;
+      bg = b->grid;
+    }
+  }
+  b->block = bb;
+  b->grid = bg;
+  if (b->exec) {
+    cudaGraphExecDestroy(b->exec);
+    cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+  }
+  if (best_block) *best_block = bb;
+  if (best_ms) *best_ms = best;
+  return 0;
+}
+
+int glb_batch_set_block(glb_batch *b, int block) {
+  if (!b || (block != 64 && block != 128 && block != 256)) return fail(GLB_ERR_ARG, "block must be 64, 128 or 256");
+  if (int rc = set_dev(b->device)) return rc;
+  b->block = block;
+  if (int rc = persistent_grid(block, b->precision, &b->grid)) return rc;
+  if (b->exec) {
+    cudaGraphExecDestroy(b->exec);
+    cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+  }
+  return 0;
+}
+
+int glb_batch_info(glb_batch *b, size_t *total_rays, double *last_ms, int *block) {
+  if (!b) return fail(GLB_ERR_ARG, "null batch");
+  if (total_rays) *total_rays = b->total;
+  if (last_ms) *last_ms = b->last_ms;
+  if (block) *block = b->block;
+  return 0;
+}
+
+int glb_batch_result(glb_batch *b, int i, double *y, double *A) {
+  if (!b || i < 0 || i >= (int)b->lenses.size()) return fail(GLB_ERR_ARG, "bad lens index");
+  if (int rc = set_dev(b->device)) return rc;
+  size_t n = b->n1d[i] * b->n1d[i], o = b->offset[i];
+  if (y) CKR(cudaMemcpy(y, b->y.p + 2 * o, 2 * n * sizeof(double), cudaMemcpyDeviceToHost));
+  if (A) CKR(cudaMemcpy(A, b->A.p + 4 * o, 4 * n * sizeof(double), cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int glb_batch_destroy(glb_batch *b) {
+  if (!b) return 0;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  if (b->e0) cudaEventDestroy(b->e0);
+  if (b->e1) cudaEventDestroy(b->e1);
+  cudaStream_t s = b->stream;
+  delete b;
+  if (s) cudaStreamDestroy(s);
+  return 0;
+}
+
+}  // extern "C"
+
+// ===================================================================== server
+namespace {
+
+__global__ void k_req_keys(const double *x, size_t n, const unsigned *req_of, const double *bbox,
+                           unsigned long long *keys, unsigned *idx) {
+  size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  unsigned r = req_of[i];
+  const double *b = bbox + 4 * r;
+  double sx = b[2] > b[0] ? 65535.0 / (b[2] - b[0]) : 0.0, sy = b[3] > b[1] ? 65535.0 / (b[3] - b[1]) : 0.0;
+  unsigned qx = (unsigned)fmin(fmax((x[2 * i] - b[0]) * sx, 0.0), 65535.0);
+  unsigned qy = (unsigned)fmin(fmax((x[2 * i + 1] - b[1]) * sy, 0.0), 65535.0);
+  keys[i] = ((unsigned long long)r << 32) | (spread16(qx) | (spread16(qy) << 1));
+  idx[i] = (unsigned)i;
+}
+
+__global__ void k_gather_sorted(const double *x, const unsigned *perm, size_t n, double *xs) {
+  size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  unsigned i = perm[k];
+  xs[2 * k] = x[2 * (size_t)i];
+  xs[2 * k + 1] = x[2 * (size_t)i + 1];
+}
+
+constexpr int kMaxReqPerBatch = 65536;
+
+struct Req {
+  long long ticket;
+  int model;
+  size_t n;
+  const double *x;
+  double zs;
+  double *y, *A;
+  double bbox[4];
+  double t_submit = 0, t_start = 0, t_done = 0;
+  std::atomic<int> done{0};
+  int status = 0;
+};
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+struct Slot {
+  cudaStream_t s = nullptr;
+  cudaEvent_t ev = nullptr;
+  double *hx = nullptr, *hy = nullptr, *hA = nullptr;  // pinned staging
+  unsigned *hreq = nullptr;
+  DBuf<double> x, xs, y, A, bbox;
+  DBuf<unsigned long long> keys, keys2;
+  DBuf<unsigned> idx, perm, req_of;
+  DBuf<Chunk> chunks;
+  DBuf<char> tmp;
+  DBuf<int> counter;
+  std::vector<std::shared_ptr<Req>> reqs;
+  std::vector<size_t> offs;
+  size_t n = 0;
+};
+
+}  // namespace
+
+struct glb_server {
+  int device = 0;
+  int precision = GLB_PREC_FP64;
+  size_t cap = 0;  // rays per batch (the admission budget of one slot)
+  std::vector<glb_lens *> models;
+  DBuf<LensDev> d_lenses;
+  NFWTables tab{};
+  int grid = 0;
+  std::vector<std::unique_ptr<Slot>> slots;
+  std::mutex mu;
+  std::condition_variable cv_submit, cv_done;
+  std::deque<std::shared_ptr<Req>> pending;
+  std::deque<int> free_slots;
+  std::deque<int> inflight;  // slot indices in launch order
+  std::unordered_map<long long, std::shared_ptr<Req>> all;
+  long long next_ticket = 1;
+  bool stop = false;
+  int error = 0;
+  std::string error_msg;
+  std::thread dispatcher, completer;
+  // statistics
+  unsigned long long batches = 0, rays_done = 0, reqs_done = 0;
+  double busy_t0 = 0, busy_t1 = 0;
+};
+
+namespace {
+
+int launch_slot(glb_server *S, Slot &sl) {
+  cudaStream_t s = sl.s;
+  size_t n = 0, nr = sl.reqs.size();
+  sl.offs.resize(nr);
+  std::vector<double> bb(4 * nr);
+  for (size_t r = 0; r < nr; ++r) {
+    Req &q = *sl.reqs[r];
+    sl.offs[r] = n;
+    memcpy(sl.hx + 2 * n, q.x, 2 * q.n * sizeof(double));
+    for (size_t i = 0; i < q.n; ++i) sl.hreq[n + i] = (unsigned)r;
+    memcpy(&bb[4 * r], q.bbox, 4 * sizeof(double));
+    n += q.n;
+  }
+  sl.n = n;
+  CKR(cudaMemcpyAsync(sl.x.p, sl.hx, 2 * n * sizeof(double), cudaMemcpyHostToDevice, s));
+  CKR(cudaMemcpyAsync(sl.req_of.p, sl.hreq, n * sizeof(unsigned), cudaMemcpyHostToDevice, s));
+  CKR(cudaMemcpyAsync(sl.bbox.p, bb.data(), bb.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+  k_req_keys<<<nblk(n, 256), 256, 0, s>>>(sl.x.p, n, sl.req_of.p, sl.bbox.p, sl.keys.p, sl.idx.p);
+  int bits = 32;
+  while ((1ull << (bits - 32)) < nr + 1 && bits < 64) ++bits;
+  size_t tb = sl.tmp.n;
+  CKR(cub::DeviceRadixSort::SortPairs(sl.tmp.p, tb, sl.keys.p, sl.keys2.p, sl.idx.p, sl.perm.p, (int)n, 0, bits, s));
+  k_gather_sorted<<<nblk(n, 256), 256, 0, s>>>(sl.x.p, sl.perm.p, n, sl.xs.p);
+  // chunks: requests stay contiguous in sorted order; 32 rays per chunk
+  std::vector<Chunk> C;
+  for (size_t r = 0; r < nr; ++r) {
+    Req &q = *sl.reqs[r];
+    for (size_t c = 0; c < q.n; c += 32) {
+      Chunk k;
+      memset(&k, 0, sizeof(k));
+      k.lens = q.model;
+      k.kind = 1;
+      k.lanes = (int)std::min<size_t>(32, q.n - c);
+      k.a = (int)(sl.offs[r] + c);
+      k.zs = q.zs;
+      C.push_back(k);
+    }
+  }
+  CKR(cudaMemcpyAsync(sl.chunks.p, C.data(), C.size() * sizeof(Chunk), cudaMemcpyHostToDevice, s));
+  CKR(cudaMemsetAsync(sl.counter.p, 0, sizeof(int), s));
+  if (S->precision == GLB_PREC_SPLIT)
+    k_batch<GLB_PREC_SPLIT><<<S->grid, 128, 0, s>>>(sl.chunks.p, (int)C.size(), S->d_lenses.p, S->tab, sl.xs.p,
+                                                    sl.perm.p, sl.y.p, sl.A.p, sl.counter.p);
+  else
+    k_batch<GLB_PREC_FP64><<<S->grid, 128, 0, s>>>(sl.chunks.p, (int)C.size(), S->d_lenses.p, S->tab, sl.xs.p,
+                                                   sl.perm.p, sl.y.p, sl.A.p, sl.counter.p);
+  CKR(cudaGetLastError());
+  CKR(cudaMemcpyAsync(sl.hy, sl.y.p, 2 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CKR(cudaMemcpyAsync(sl.hA, sl.A.p, 4 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CKR(cudaEventRecord(sl.ev, s));
+  return 0;
+}
+
+// Continuous batching: whenever a slot is free, every pending request that fits
+// the slot's ray budget (in arrival order) is admitted into one batch and
+// launched, while earlier batches are still running on the other slots.
+void dispatcher_main(glb_server *S) {
+  cudaSetDevice(S->device);
+  for (;;) {
+    int si;
+    std::vector<std::shared_ptr<Req>> take;
+    {
+      std::unique_lock<std::mutex> lk(S->mu);
+      S->cv_submit.wait(lk, [&] { return S->stop || (!S->pending.empty() && !S->free_slots.empty()); });
+      if (S->stop) return;
+      si = S->free_slots.front();
+      S->free_slots.pop_front();
+      size_t budget = S->cap, used = 0;
+      while (!S->pending.empty() && used + S->pending.front()->n <= budget && (int)take.size() < kMaxReqPerBatch) {
+        used += S->pending.front()->n;
+        take.push_back(S->pending.front());
+        S->pending.pop_front();
+      }
+    }
+    Slot &sl = *S->slots[si];
+    sl.reqs = take;
+    double t = now_s();
+    for (auto &q : take) q->t_start = t;
+    int rc = launch_slot(S, sl);
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (rc) {
+      S->error = rc;
+      S->error_msg = t_err;
+      for (auto &q : take) {
+        q->status = rc;
+        q->done.store(1);
+      }
+      S->free_slots.push_back(si);
+      S->cv_done.notify_all();
+    } else {
+      if (S->busy_t0 == 0) S->busy_t0 = t;
+      S->inflight.push_back(si);
+      S->cv_done.notify_all();
+    }
+  }
+}
+
+// Completion: waits for batches in launch order and hands results back.
+void completer_main(glb_server *S) {
+  cudaSetDevice(S->device);
+  for (;;) {
+    int si;
+    {
+      std::unique_lock<std::mutex> lk(S->mu);
+      S->cv_done.wait(lk, [&] { return S->stop || !S->inflight.empty(); });
+      if (S->inflight.empty() && S->stop) return;
+      si = S->inflight.front();
+    }
+    Slot &sl = *S->slots[si];
+    cudaError_t e = cudaEventSynchronize(sl.ev);
+    double t = now_s();
+    for (size_t r = 0; r < sl.reqs.size(); ++r) {
+      Req &q = *sl.reqs[r];
+      if (e == cudaSuccess) {
+        memcpy(q.y, sl.hy + 2 * sl.offs[r], 2 * q.n * sizeof(double));
+        memcpy(q.A, sl.hA + 4 * sl.offs[r], 4 * q.n * sizeof(double));
+      } else {
+        q.status = GLB_ERR_CUDA;
+      }
+    }
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->inflight.pop_front();
+    for (auto &q : sl.reqs) {
+      q->t_done = t;
+      q->done.store(1);
+      S->rays_done += q->n;
+      S->reqs_done += 1;
+    }
+    S->batches += 1;
+    S->busy_t1 = t;
+    sl.reqs.clear();
+    S->free_slots.push_back(si);
+    S->cv_submit.notify_all();
+    S->cv_done.notify_all();
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int glb_server_create(glb_lens *const *models, int nmodels, size_t max_rays_per_batch, int precision, int nslots,
+                      glb_server **out) {
+  if (!out || !models || nmodels <= 0) return fail(GLB_ERR_ARG, "null argument");
+  if (precision != GLB_PREC_FP64 && precision != GLB_PREC_SPLIT) return fail(GLB_ERR_ARG, "unknown precision");
+  if (nslots < 1 || nslots > 8) return fail(GLB_ERR_ARG, "nslots must be in [1, 8]");
+  if (int rc = need_device()) return rc;
+  auto S = std::make_unique<glb_server>();
+  CKR(cudaGetDevice(&S->device));
+  S->precision = precision;
+  // admission budget: the requested rays per batch, bounded by free HBM
+  // (about 200 bytes of device memory per ray and slot)
+  size_t freeb = 0, totb = 0;
+  CKR(cudaMemGetInfo(&freeb, &totb));
+  size_t by_mem = freeb / 2 / (size_t)nslots / 200;
+  S->cap = std::min<size_t>(max_rays_per_batch ? max_rays_per_batch : (size_t)4 << 20, by_mem);
+  S->cap = std::min<size_t>(S->cap, (size_t)1 << 30);
+  if (S->cap < 32) return fail(GLB_ERR_OOM, "not enough free device memory for the server");
+  std::vector<LensDev> L(nmodels);
+  for (int i = 0; i < nmodels; ++i) {
+    if (!models[i] || models[i]->device != S->device) return fail(GLB_ERR_ARG, "models must be lenses on one device");
+    if (int rc = make_lens_dev(models[i], L[i])) return rc;
+    S->models.push_back(models[i]);
+  }
+  CKR(S->d_lenses.alloc(nmodels));
+  CKR(cudaMemcpy(S->d_lenses.p, L.data(), nmodels * sizeof(LensDev), cudaMemcpyHostToDevice));
+  if (int rc = device_nfw_tables(S->tab)) return rc;
+  if (int rc = persistent_grid(128, precision, &S->grid)) return rc;
+  size_t cap = S->cap, maxchunks = cap / 32 + kMaxReqPerBatch + 1;
+  for (int i = 0; i < nslots; ++i) {
+    auto sl = std::make_unique<Slot>();
+    CKR(cudaStreamCreateWithFlags(&sl->s, cudaStreamNonBlocking));
+    CKR(cudaEventCreateWithFlags(&sl->ev, cudaEventBlockingSync | cudaEventDisableTiming));
+    CKR(cudaMallocHost((void **)&sl->hx, 2 * cap * sizeof(double)));
+    CKR(cudaMallocHost((void **)&sl->hy, 2 * cap * sizeof(double)));
+    CKR(cudaMallocHost((void **)&sl->hA, 4 * cap * sizeof(double)));
+    CKR(cudaMallocHost((void **)&sl->hreq, cap * sizeof(unsigned)));
+    CKR(sl->x.alloc(2 * cap));
+    CKR(sl->xs.alloc(2 * cap));
+    CKR(sl->y.alloc(2 * cap));
+    CKR(sl->A.alloc(4 * cap));
+    CKR(sl->bbox.alloc(4 * (size_t)kMaxReqPerBatch));
+    CKR(sl->keys.alloc(cap));
+    CKR(sl->keys2.alloc(cap));
+    CKR(sl->idx.alloc(cap));
+    CKR(sl->perm.alloc(cap));
+    CKR(sl->req_of.alloc(cap));
+    CKR(sl->chunks.alloc(maxchunks));
+    CKR(sl->counter.alloc(1));
+    size_t tb = 0;
+    CKR(cub::DeviceRadixSort::SortPairs(nullptr, tb, sl->keys.p, sl->keys2.p, sl->idx.p, sl->perm.p, (int)cap, 0, 64,
+                                        sl->s));
+    CKR(sl->tmp.alloc(tb));
+    S->slots.push_back(std::move(sl));
+    S->free_slots.push_back(i);
+  }
+  glb_server *p = S.release();
+  p->dispatcher = std::thread(dispatcher_main, p);
+  p->completer = std::thread(completer_main, p);
+  *out = p;
+  return 0;
+}
+
+int glb_server_submit(glb_server *S, int model, size_t n, const double *x, double zs, double *y, double *A,
+                      long long *ticket) {
+  if (!S || !ticket || (n > 0 && (!x || !y || !A))) return fail(GLB_ERR_ARG, "null argument");
+  if (model < 0 || model >= (int)S->models.size()) return fail(GLB_ERR_ARG, "unknown model");
+  if (n > S->cap) return fail(GLB_ERR_ARG, "request larger than the server's ray budget per batch");
+  auto q = std::make_shared<Req>();
+  q->model = model;
+  q->n = n;
+  q->x = x;
+  q->zs = zs;
+  q->y = y;
+  q->A = A;
+  q->bbox[0] = q->bbox[1] = 1e300;
+  q->bbox[2] = q->bbox[3] = -1e300;
+  for (size_t i = 0; i < n; ++i) {
+    q->bbox[0] = std::min(q->bbox[0], x[2 * i]);
+    q->bbox[1] = std::min(q->bbox[1], x[2 * i + 1]);
+    q->bbox[2] = std::max(q->bbox[2], x[2 * i]);
+    q->bbox[3] = std::max(q->bbox[3], x[2 * i + 1]);
+  }
+  q->t_submit = now_s();
+  std::lock_guard<std::mutex> lk(S->mu);
+  if (S->stop) return fail(GLB_ERR_ARG, "server stopped");
+  q->ticket = S->next_ticket++;
+  if (n == 0) {
+    q->t_start = q->t_done = q->t_submit;
+    q->done.store(1);
+  } else {
+    S->pending.push_back(q);
+    S->cv_submit.notify_all();
+  }
+  S->all[q->ticket] = q;
+  *ticket = q->ticket;
+  return 0;
+}
+
+int glb_server_wait(glb_server *S, long long ticket, double timeout_s, double *times) {
+  if (!S) return fail(GLB_ERR_ARG, "null server");
+  std::shared_ptr<Req> q;
+  {
+    std::unique_lock<std::mutex> lk(S->mu);
+    auto it = S->all.find(ticket);
+    if (it == S->all.end()) return fail(GLB_ERR_ARG, "unknown ticket");
+    q = it->second;
+    auto pred = [&] { return q->done.load() != 0; };
+    if (timeout_s > 0) {
+      if (!S->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), pred))
+        return fail(GLB_ERR_TIMEOUT, "request not finished within the timeout");
+    } else {
+      S->cv_done.wait(lk, pred);
+    }
+    S->all.erase(ticket);
+  }
+  if (times) {
+    times[0] = q->t_submit;
+    times[1] = q->t_start;
+    times[2] = q->t_done;
+  }
+  if (q->status) return fail(q->status, "request failed on the device");
+  return 0;
+}
+
+int glb_server_poll(glb_server *S, long long ticket, int *done) {
+  if (!S || !done) return fail(GLB_ERR_ARG, "null argument");
+  std::lock_guard<std::mutex> lk(S->mu);
+  auto it = S->all.find(ticket);
+  if (it == S->all.end()) return fail(GLB_ERR_ARG, "unknown ticket");
+  *done = it->second->done.load();
+  return 0;
+}
+
+int glb_server_stats(glb_server *S, double *stats) {
+  if (!S || !stats) return fail(GLB_ERR_ARG, "null argument");
+  std::lock_guard<std::mutex> lk(S->mu);
+  stats[0] = (double)S->rays_done;
+  stats[1] = (double)S->reqs_done;
+  stats[2] = (double)S->batches;
+  stats[3] = S->busy_t1 - S->busy_t0;
+  stats[4] = (double)S->cap;
+  stats[5] = (double)S->pending.size();
+  return 0;
+}
+
+int glb_server_destroy(glb_server *S) {
+  if (!S) return 0;
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->stop = true;
+  }
+  S->cv_submit.notify_all();
+  S->cv_done.notify_all();
+  if (S->dispatcher.joinable()) S->dispatcher.join();
+  // let the batches already on the GPU finish before the slots go away
+  for (auto &sl : S->slots) cudaStreamSynchronize(sl->s);
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+  }
+  S->cv_done.notify_all();
+  if (S->completer.joinable()) S->completer.join();
+  cudaSetDevice(S->device);
+  for (auto &sl : S->slots) {
+    cudaStreamSynchronize(sl->s);
+    cudaFreeHost(sl->hx);
+    cudaFreeHost(sl->hy);
+    cudaFreeHost(sl->hA);
+    cudaFreeHost(sl->hreq);
+    cudaEventDestroy(sl->ev);
+    cudaStreamDestroy(sl->s);
+  }
+  delete S;
+  return 0;
+}
+
+}  // extern "C"

@@ -1396,3 +1396,5 @@ extern "C" int glb_lens_rayshoot_noalloc(glb_lens *l, size_t n, const double *x_
   CKR(cudaGetLastError());
   return 0;
 }
+
+#include "batch.cuh"
