@@ -230,6 +230,7 @@ struct glb_batch {
 
 namespace {
 int batch_enqueue(glb_batch *b) {
+  (void)cudaGetLastError();  // launch errors below are this launch's own
   CKR(cudaMemsetAsync(b->counter.p, 0, sizeof(int), b->stream));
   if (b->precision == GLB_PREC_SPLIT)
     k_batch<GLB_PREC_SPLIT><<<b->grid, b->block, 0, b->stream>>>(b->d_chunks.p, b->nchunks, b->d_lenses.p, b->tab,
@@ -237,7 +238,10 @@ int batch_enqueue(glb_batch *b) {
   else
     k_batch<GLB_PREC_FP64><<<b->grid, b->block, 0, b->stream>>>(b->d_chunks.p, b->nchunks, b->d_lenses.p, b->tab,
                                                                 nullptr, nullptr, b->y.p, b->A.p, b->counter.p);
-  CKR(cudaGetLastError());
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return fail(GLB_ERR_CUDA, std::string("CUDA: ") + cudaGetErrorString(e) + " launching k_batch with block " +
+                                  std::to_string(b->block) + " grid " + std::to_string(b->grid));
   return 0;
 }
 }  // namespace
