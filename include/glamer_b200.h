@@ -48,7 +48,8 @@ enum {
 /* Precision of the tree walk. */
 enum {
   GLB_PREC_FP64 = 0,  /* plain FP64 walk, the reference's arithmetic */
-  GLB_PREC_SPLIT = 1  /* FP32 walk with compensated sums, FP64 offsets and recursion */
+  GLB_PREC_SPLIT = 1, /* FP32 walk with compensated sums, FP64 offsets and recursion */
+  GLB_PREC_FP32 = 2   /* plain FP32 tree walk (tree-force calls only; the precision sweep) */
 };
 
 /* Message of the last failure on this thread ("" if none). */
@@ -76,6 +77,22 @@ int glb_tree_destroy(glb_tree *t);
  * kappa n, gamma 3n, phi n; gamma[2] is always 0 as in the reference. */
 int glb_tree_force2D_recur(glb_tree *t, size_t n, const double *rays, double *alpha, double *kappa,
                            double *gamma, double *phi);
+
+/* force2D_recur for n rays already on the device (2n doubles, physical Mpc),
+ * in any precision form; out_dev gets 5 doubles per ray {alpha0, alpha1,
+ * kappa, gamma0, gamma1} (no potential).  Enqueued on `stream` (NULL: the
+ * tree's own stream).  Rays are walked 32 to a warp in the given order, so
+ * spatially sorted rays walk fastest. */
+int glb_tree_force_device(glb_tree *t, size_t n, const double *rays_dev, double *out_dev, int precision,
+                          void *stream);
+
+/* No counterpart in the reference: FP64 direct summation over all n particles
+ * (device records) at nrays device rays -- the point mass plus the B-spline
+ * correction within two sizes and the inv_area sheet, as at a tree leaf --
+ * for reports of a tree form's absolute error.  out_dev: 5 doubles per ray as
+ * glb_tree_force_device. */
+int glb_direct_sum_device(const glb_particle *particles_dev, size_t n, double inv_area, const double *rays_dev,
+                          size_t nrays, double *out_dev, void *stream);
 
 /* Per-branch build data in depth-first order, 16 doubles per branch
  * (level, p1x, p1y, p2x, p2y, nparticles, Nbig_particles, mass, com_x, com_y,

@@ -36,6 +36,7 @@ LIB_PATH = os.path.join(HERE, "libglamer_b200.so")
 
 PREC_FP64 = 0
 PREC_SPLIT = 1
+PREC_FP32 = 2
 
 GLB_ERR_ARG = -1
 GLB_ERR_CUDA = -2
@@ -49,7 +50,8 @@ GLB_ERR_TIMEOUT = -8
 # every symbol include/glamer_b200.h declares
 EXPORTED = [
     "glb_last_error", "glb_version", "glb_set_option",
-    "glb_tree_create", "glb_tree_destroy", "glb_tree_force2D_recur", "glb_tree_export", "glb_tree_build_ms",
+    "glb_tree_create", "glb_tree_destroy", "glb_tree_force2D_recur", "glb_tree_force_device", "glb_tree_export",
+    "glb_tree_build_ms", "glb_direct_sum_device",
     "glb_halo_particles", "glb_halo_nfw", "glb_halo_nsie", "glb_halo_set_theta", "glb_halo_force",
     "glb_halo_params", "glb_halo_destroy",
     "glb_lens_create", "glb_lens_destroy", "glb_lens_insert_halo", "glb_lens_nplanes", "glb_lens_planes",
@@ -89,6 +91,8 @@ def load_library():
     L.glb_tree_destroy.argtypes = [_vp]
     L.glb_tree_force2D_recur.argtypes = [_vp, C.c_size_t, _vp, _vp, _vp, _vp, _vp]
     L.glb_tree_export.argtypes = [_vp, C.POINTER(C.c_size_t), _vp]
+    L.glb_tree_force_device.argtypes = [_vp, C.c_size_t, _vp, _vp, C.c_int, _vp]
+    L.glb_direct_sum_device.argtypes = [_vp, C.c_size_t, C.c_double, _vp, C.c_size_t, _vp, _vp]
     L.glb_tree_build_ms.argtypes = [_vp, C.POINTER(C.c_double)]
     L.glb_halo_particles.argtypes = [_vp, C.c_size_t, C.c_double, C.c_double, C.c_double, C.POINTER(_vp)]
     L.glb_halo_nfw.argtypes = [C.c_float, C.c_float, C.c_double, C.c_float, C.c_float, C.c_float, C.POINTER(_vp)]
@@ -178,6 +182,10 @@ class TreeQuadParticles:
         a, k, g, ph = _forces(len(r))
         _check(load_library().glb_tree_force2D_recur(self._h, len(r), _p(r), _p(a), _p(k), _p(g), _p(ph)))
         return a, k, g, ph
+
+    def force_device(self, n: int, rays_ptr: int, out_ptr: int, precision=PREC_FP64, stream=None):
+        """force2D_recur on device rays (raw pointers): out = 5 doubles per ray."""
+        _check(load_library().glb_tree_force_device(self._h, n, rays_ptr, out_ptr, precision, stream))
 
     def export(self) -> np.ndarray:
         L = load_library()
@@ -398,6 +406,12 @@ class GridMap:
 
     def alpha(self):
         return self.positions() - self.y
+
+
+def direct_sum_device(n: int, particles_ptr: int, inv_area: float, nrays: int, rays_ptr: int, out_ptr: int,
+                      stream=None):
+    """FP64 direct summation (no tree) over device particles at device rays."""
+    _check(load_library().glb_direct_sum_device(particles_ptr, n, inv_area, rays_ptr, nrays, out_ptr, stream))
 
 
 # ----------------------------------------------------------- batched lenses

@@ -336,14 +336,18 @@ __device__ __forceinline__ void particle_halo_acc(const TreeDev &T, double rx, d
       for (int j = -1; j < 2; ++j) {
         if (PREC == GLB_PREC_FP64)
           walk_f64<PHI, COUNT>(T, rx + i * T.period_x, ry + j * T.period_y, valid, acc, wc);
+        else if (PREC == GLB_PREC_FP32)
+          walk_split<true>(T, rx + i * T.period_x, ry + j * T.period_y, valid, acc);
         else
-          walk_split(T, rx + i * T.period_x, ry + j * T.period_y, valid, acc);
+          walk_split<false>(T, rx + i * T.period_x, ry + j * T.period_y, valid, acc);
       }
   } else {
     if (PREC == GLB_PREC_FP64)
       walk_f64<PHI, COUNT>(T, rx, ry, valid, acc, wc);
+    else if (PREC == GLB_PREC_FP32)
+      walk_split<true>(T, rx, ry, valid, acc);
     else
-      walk_split(T, rx, ry, valid, acc);
+      walk_split<false>(T, rx, ry, valid, acc);
   }
 }
 
@@ -487,6 +491,66 @@ __global__ void __launch_bounds__(128) k_halo_force(HaloDev H, NFWTables tab, si
   }
   if (!valid) return;
   for (int c = 0; c < 6; ++c) out[6 * k + c] = acc[c];
+}
+
+// force2D_recur on device rays in the three precision forms (no potential):
+// out = 5 doubles per ray {alpha0, alpha1, kappa, gamma0, gamma1}.
+template <int PREC>
+__global__ void __launch_bounds__(128) k_tree_force(TreeDev T, size_t n, const double *x, double *out) {
+  const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  const bool valid = k < n;
+  if (!__any_sync(kFull, valid)) return;
+  double x0 = 0, x1 = 0;
+  if (valid) {
+    x0 = x[2 * k];
+    x1 = x[2 * k + 1];
+  }
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  particle_halo_acc<PREC, false>(T, x0, x1, valid, acc);
+  if (!valid) return;
+  for (int c = 0; c < 5; ++c) out[5 * k + c] = acc[c];
+}
+
+// FP64 direct summation over every particle (no tree): the point mass and the
+// B-spline correction within two sizes, with the inv_area sheet -- the same
+// kernel as the tree's leaves (quadTree.h:1017-1077), for absolute-accuracy
+// reports.  Particles are staged through shared memory, one ray per thread.
+__global__ void __launch_bounds__(256) k_direct_sum(const glb_particle_rec *p, size_t n, double inv_area,
+                                                    const double *x, size_t nr, double *out) {
+  __shared__ float4 tile[256];
+  const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  const bool valid = k < nr;
+  double rx = 0, ry = 0;
+  if (valid) {
+    rx = x[2 * k];
+    ry = x[2 * k + 1];
+  }
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  for (size_t base = 0; base < n; base += 256) {
+    const size_t i = base + threadIdx.x;
+    if (i < n) tile[threadIdx.x] = make_float4(p[i].x[0], p[i].x[1], p[i].Mass, p[i].Size);
+    __syncthreads();
+    const int cnt = (int)min((size_t)256, n - base);
+    if (valid)
+      for (int j = 0; j < cnt; ++j) {
+        const float4 P = tile[j];
+        const double x0 = (double)P.x - rx, x1 = (double)P.y - ry;
+        double rcm2 = x0 * x0 + x1 * x1;
+        if (rcm2 < 1e-20) rcm2 = 1e-20;
+        const double m = (double)P.z, ir2 = 1.0 / rcm2, prefac = m * ir2 * (1.0 / kPi);
+        acc[0] += (inv_area * m - prefac) * x0;
+        acc[1] += (inv_area * m - prefac) * x1;
+        const double tmp = -2.0 * prefac * ir2;
+        acc[3] += 0.5 * (x0 * x0 - x1 * x1) * tmp;
+        acc[4] += x0 * x1 * tmp;
+        acc[2] -= m * inv_area;
+        const double size = (double)P.w;
+        if (rcm2 < 4 * size * size) bspline_f64<false>(x0, x1, sqrt(rcm2), m, size, 0.0, acc);
+      }
+    __syncthreads();
+  }
+  if (valid)
+    for (int c = 0; c < 5; ++c) out[5 * k + c] = acc[c];
 }
 
 inline int nblk(size_t n, int t) { return (int)((n + t - 1) / t); }
@@ -774,6 +838,40 @@ int glb_tree_force2D_recur(glb_tree *t, size_t n, const double *rays, double *al
     return 0;
   }
   return force_generic(H, t->device, t->stream, n, rays, alpha, kappa, gamma, phi);
+}
+
+int glb_tree_force_device(glb_tree *t, size_t n, const double *rays_dev, double *out_dev, int precision,
+                          void *stream) {
+  if (!t || (n > 0 && (!rays_dev || !out_dev))) return fail(GLB_ERR_ARG, "null argument");
+  if (precision < GLB_PREC_FP64 || precision > GLB_PREC_FP32) return fail(GLB_ERR_ARG, "unknown precision");
+  if (int rc = set_dev(t->device)) return rc;
+  if (n == 0) return 0;
+  cudaStream_t s = stream ? (cudaStream_t)stream : t->stream;
+  if (t->tree->nparticles == 0) {
+    CKR(cudaMemsetAsync(out_dev, 0, 5 * n * sizeof(double), s));
+    return 0;
+  }
+  (void)cudaGetLastError();
+  if (precision == GLB_PREC_FP64)
+    k_tree_force<GLB_PREC_FP64><<<nblk(n, 128), 128, 0, s>>>(t->tree->dev, n, rays_dev, out_dev);
+  else if (precision == GLB_PREC_SPLIT)
+    k_tree_force<GLB_PREC_SPLIT><<<nblk(n, 128), 128, 0, s>>>(t->tree->dev, n, rays_dev, out_dev);
+  else
+    k_tree_force<GLB_PREC_FP32><<<nblk(n, 128), 128, 0, s>>>(t->tree->dev, n, rays_dev, out_dev);
+  CKR(cudaGetLastError());
+  return 0;
+}
+
+int glb_direct_sum_device(const glb_particle *particles_dev, size_t n, double inv_area, const double *rays_dev,
+                          size_t nrays, double *out_dev, void *stream) {
+  if ((n > 0 && !particles_dev) || (nrays > 0 && (!rays_dev || !out_dev))) return fail(GLB_ERR_ARG, "null argument");
+  if (int rc = need_device()) return rc;
+  if (nrays == 0) return 0;
+  (void)cudaGetLastError();
+  k_direct_sum<<<nblk(nrays, 256), 256, 0, (cudaStream_t)stream>>>(
+      reinterpret_cast<const glb_particle_rec *>(particles_dev), n, inv_area, rays_dev, nrays, out_dev);
+  CKR(cudaGetLastError());
+  return 0;
 }
 
 int glb_tree_export(glb_tree *t, size_t *nbranches, double *out) {

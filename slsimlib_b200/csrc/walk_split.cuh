@@ -48,6 +48,9 @@ __device__ __noinline__ bool node_test_f64(const GNode *nd, double rx, double ry
   return (dx * dx + dy * dy) < (which ? nd->near2 : nd->open2);
 }
 
+// x-width of a node record (GNodeS.width), read only by the plain FP32 form.
+__device__ __forceinline__ float c2w(const float4 *sp) { return __ldg(sp + 2).z; }
+
 struct Near64 {
   double a0, a1, k, g0, g1;
 };
@@ -79,13 +82,48 @@ __device__ __noinline__ Near64 near_particle_f64(float4 Q, double rx, double ry,
   return o;
 }
 
+// b_spline_profile (include/quadTree.h:147-190) in FP32, for the plain FP32
+// form only.
+__device__ __forceinline__ void bspline_f32(float x0, float x1, float r, float Mass, float size, float *f) {
+  const float ipi = (float)(1.0 / kPi);
+  const float q = r / size;
+  float M, sigma;
+  if (q > 2.f) {
+    sigma = 0.f;
+    M = 1.f;
+  } else {
+    const float q2 = q * q, q3 = q2 * q;
+    sigma = (8.f - 12.f * q + 6.f * q2 - q3) / 4.f;
+    if (q > 1.f) {
+      sigma *= 10.f / size / size / 7.f * ipi;
+      M = (-1.f + 20.f * q2 * (1.f - q + 3.f * q2 / 8.f - q3 / 20.f)) / 7.f;
+    } else {
+      sigma = 10.f * (sigma - 1.f + 3.f * q - 3.f * q2 + q3) / size / size / 7.f * ipi;
+      M = 10.f * q2 * (1.f - 3.f * q / 4.f + 3.f * q3 / 10.f) / 7.f;
+    }
+  }
+  const float alpha_r = (M - 1.f) * ipi / r;
+  const float gt = alpha_r / r - sigma;
+  f[0] -= Mass * alpha_r * x0 / r;
+  f[1] -= Mass * alpha_r * x1 / r;
+  f[3] -= gt * Mass * (x0 * x0 - x1 * x1) / r / r;
+  f[4] -= gt * Mass * 2.f * x0 * x1 / r / r;
+  f[2] += Mass * sigma;
+}
+
+// PURE = true is the plain FP32 form of the precision sweep: FP32 offsets
+// from FP32 coordinates, FP32 opening tests and sums throughout, FP32
+// near field; it keeps no FP64 arithmetic and so no guarantee of the FP64
+// form's interaction set or precision.
+template <bool PURE = false>
 __device__ __forceinline__ void walk_split(const TreeDev &T, double rx, double ry, bool valid, double *acc) {
   const float inv_pi = (float)(1.0 / kPi);
   const bool screen = T.screen2 != 0.0;
   const float s2f = (float)T.screen2;
   const float iaf = (float)T.inv_area;
   const float rxh = (float)rx, ryh = (float)ry;
-  const float rxl = (float)(rx - (double)rxh), ryl = (float)(ry - (double)ryh);
+  const float rxl = PURE ? 0.f : (float)(rx - (double)rxh), ryl = PURE ? 0.f : (float)(ry - (double)ryh);
+  float pf[5] = {0.f, 0.f, 0.f, 0.f, 0.f};  // PURE: the FP32 total
   F32Acc fa;
   fa.zero();
   int resume = valid ? 0 : 0x7fffffff;
@@ -97,13 +135,14 @@ __device__ __forceinline__ void walk_split(const TreeDev &T, double rx, double r
     const int4 c3 = __ldg(reinterpret_cast<const int4 *>(sp + 3));
     const int skip = max(c3.x, node + 1);  // forward progress even on a malformed array
     const bool act = node >= resume;
-    const float dxf = (c0.x - rxh) + (c0.z - rxl), dyf = (c0.y - ryh) + (c0.w - ryl);
+    const float dxf = PURE ? (c0.x - rxh) : (c0.x - rxh) + (c0.z - rxl);
+    const float dyf = PURE ? (c0.y - ryh) : (c0.y - ryh) + (c0.w - ryl);
     const float r2f = dxf * dxf + dyf * dyf;
     bool open = false;
     if (act) {
       const float d = r2f - c1.x;
       open = d < 0.f;
-      if (fabsf(d) <= kAmbiguous * c1.x) open = node_test_f64(T.nodes + node, rx, ry, 0);
+      if (!PURE && fabsf(d) <= kAmbiguous * c1.x) open = node_test_f64(T.nodes + node, rx, ry, 0);
     }
     if (act && !open) {
       // far field: monopole + quadrupole (quadTree.h:1090-1123)
@@ -122,7 +161,12 @@ __device__ __forceinline__ void walk_split(const TreeDev &T, double rx, double r
       fa.g0 -= ms * ir2 * ((dxf * dxf - dyf * dyf) * ir2);
       fa.g1 -= ms * ir2 * (2.0f * dxf * dyf * ir2);
       fa.k -= iaf * mass;
-      if (++fa.cnt >= 32) fa.flush(acc);
+      if (PURE) {
+        pf[0] += fa.a0; pf[1] += fa.a1; pf[2] += fa.k; pf[3] += fa.g0; pf[4] += fa.g1;
+        fa.zero();
+      } else if (++fa.cnt >= 32) {
+        fa.flush(acc);
+      }
       resume = skip;
     }
     if (!__any_sync(kFull, open)) {
@@ -133,7 +177,7 @@ __device__ __forceinline__ void walk_split(const TreeDev &T, double rx, double r
     if (open) {
       const float e = r2f - c1.y;
       nearc = e < 0.f;
-      if (fabsf(e) <= kAmbiguous * c1.y) nearc = node_test_f64(T.nodes + node, rx, ry, 1);
+      if (!PURE && fabsf(e) <= kAmbiguous * c1.y) nearc = node_test_f64(T.nodes + node, rx, ry, 1);
     }
     if (c3.y) {  // leaf
       const int p0 = c3.z, p1 = p0 + c3.w;
@@ -145,8 +189,19 @@ __device__ __forceinline__ void walk_split(const TreeDev &T, double rx, double r
           const float4 P = __ldg(T.prel + p);
           if (open) {
             const float x0 = P.x + dxf, x1 = P.y + dyf;
-            const float rcm2f = x0 * x0 + x1 * x1;
-            if (rcm2f < fmaxf(4.0001f * P.w * P.w, 1e-12f)) {  // near or (unsoftened) coincident
+            float rcm2f = x0 * x0 + x1 * x1;
+            if (PURE) {
+              // plain FP32: point mass, then the B-spline if within two sizes
+              const float scr = screen ? __expf(-rcm2f * s2f) : 1.0f;
+              const float rr = fmaxf(rcm2f, 1e-20f);
+              const float m = P.z, ir2 = __fdividef(1.0f, rr), prefac = m * scr * ir2 * inv_pi;
+              pf[0] += (iaf * m - prefac) * x0;
+              pf[1] += (iaf * m - prefac) * x1;
+              pf[3] -= prefac * ir2 * (x0 * x0 - x1 * x1);
+              pf[4] -= prefac * ir2 * (2.0f * x0 * x1);
+              pf[2] -= m * iaf;
+              if (nearc && P.w < c2w(sp) && rr < 4.f * P.w * P.w) bspline_f32(x0, x1, sqrtf(rr), m, P.w, pf);
+            } else if (rcm2f < fmaxf(4.0001f * P.w * P.w, 1e-12f)) {  // near or (unsoftened) coincident
               const Near64 o = near_particle_f64(__ldg(T.parts + p), rx, ry, T.screen2, T.inv_area, nearc,
                                                  T.nodes[node].width);
               acc[0] += o.a0;
@@ -178,7 +233,11 @@ __device__ __forceinline__ void walk_split(const TreeDev &T, double rx, double r
         const int b0 = c3.z, b1 = b0 + c3.w;
         for (int b = b0; b < b1; ++b) {
           const float4 P = __ldg(T.bigs + b);
-          if (nearc) {
+          if (PURE && nearc) {
+            const float x0 = P.x - rxh, x1 = P.y - ryh;
+            const float rr = fmaxf(x0 * x0 + x1 * x1, 1e-20f);
+            if (rr < 4.f * P.w * P.w) bspline_f32(x0, x1, sqrtf(rr), P.z, P.w, pf);
+          } else if (nearc) {
             const double x0 = (double)P.x - rx, x1 = (double)P.y - ry;
             double rcm2 = x0 * x0 + x1 * x1;
             if (rcm2 < 1e-20) rcm2 = 1e-20;
@@ -190,7 +249,11 @@ __device__ __forceinline__ void walk_split(const TreeDev &T, double rx, double r
       node = node + 1;
     }
   }
-  fa.flush(acc);
+  if (PURE) {
+    for (int c = 0; c < 5; ++c) acc[c] += (double)pf[c];
+  } else {
+    fa.flush(acc);
+  }
 }
 
 }  // namespace glb

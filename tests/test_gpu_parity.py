@@ -265,3 +265,36 @@ def test_split_precision_deflection_tolerance(n_total, n_planes):
         for name in ("kappa", "gamma", "invmag"):
             med, p999 = st[name]
             assert med <= 1e-6 and p999 <= 1e-5, (name, st)
+
+
+# --------------------------------------------- tree-force forms, direct sum
+def test_tree_force_device_forms_and_direct_sum():
+    import torch
+    rng = np.random.default_rng(12)
+    p = synth.nfw_particles(rng, 30000, 1e14, 5.0, 0.3, 1e-3)
+    rays = rng.uniform(-0.1, 0.1, (1000, 2))
+    t = glb.TreeQuadParticles(p, bucket=20, theta_force=0.1, inv_screening_scale=1.0)
+    a, k, g, _ = t.force2D_recur(rays)
+    ref = np.concatenate([a, k[:, None], g[:, :2]], axis=1)
+    dr = torch.from_numpy(rays).cuda()
+    outs = {}
+    for prec in (glb.PREC_FP64, glb.PREC_SPLIT, glb.PREC_FP32):
+        o = torch.zeros((len(rays), 5), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        t.force_device(len(rays), dr.data_ptr(), o.data_ptr(), prec, None)
+        torch.cuda.synchronize()
+        outs[prec] = o.cpu().numpy()
+    assert np.max(vec_err(outs[glb.PREC_FP64][:, :2], ref[:, :2])) < 1e-12
+    e_split = vec_err(outs[glb.PREC_SPLIT][:, :2], ref[:, :2])
+    assert np.median(e_split) < 1e-6 and e_split.max() < 1e-5
+    e32 = vec_err(outs[glb.PREC_FP32][:, :2], ref[:, :2])
+    assert np.median(e32) < 1e-4  # the plain FP32 form: reported, loosely bounded
+    # FP64 direct sum on the GPU against the oracle's
+    pd = torch.from_numpy(p.view(np.uint8)).cuda()
+    o = torch.zeros((64, 5), dtype=torch.float64, device="cuda")
+    dr64 = dr[:64].contiguous()
+    torch.cuda.synchronize()
+    glb.direct_sum_device(len(p), pd.data_ptr(), 0.0, 64, dr64.data_ptr(), o.data_ptr(), None)
+    torch.cuda.synchronize()
+    ds = H.direct_sum(p, rays[:64])
+    assert np.max(vec_err(o.cpu().numpy()[:, :2], ds[:, :2])) < 1e-10
