@@ -177,6 +177,268 @@ def run_reference_arm(args, rank):
     print(json.dumps(line))
 
 
+# ------------------------------------------------------------ other workloads
+def _tile_order(n1d):
+    """Grid indices (x fastest) reordered into 8 x 4 tiles, one tile per warp."""
+    ix = np.arange(n1d)
+    iy = np.arange(n1d)
+    X, Y = np.meshgrid(ix, iy)
+    key = ((Y // 4) * ((n1d + 7) // 8) + (X // 8)) * 32 + (Y % 4) * 8 + (X % 8)
+    return np.argsort(key.ravel(), kind="stable")
+
+
+def _timed(fn, stream, steps):
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def _base_line(args, metric, unit, value, ms, dtype, workload, **extra):
+    d = {"metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype,
+         "data": "synthetic (seeded)", "config": {"workload": workload}}
+    d.update(extra)
+    return d
+
+
+def run_single(args):
+    """One NFW particle plane (2^18 particles, 1e14 Msun, c=5, z=0.3, 1 kpc),
+    512^2 rays over 30 arcsec, z_s=2, through GridMap in the plain FP64 form."""
+    import torch
+    import slsimlib_b200 as glb
+    from slsimlib_b200 import synth
+    spec = synth.single_plane_nfw(seed=1)
+    lens = make_lens(spec)
+    n1d, rng = 512, 30 * synth.ARCSEC
+    x_host = synth.grid_positions(n1d, range_rad=rng)
+    n = n1d * n1d
+    x = torch.from_numpy(x_host).cuda()
+    y = torch.empty((n, 2), dtype=torch.float64, device="cuda")
+    A = torch.empty((n, 4), dtype=torch.float64, device="cuda")
+    st = torch.cuda.Stream()
+    torch.cuda.set_stream(st)
+    out = {}
+    for prec in (glb.PREC_FP64, glb.PREC_SPLIT):
+        f = lambda: lens.rayshoot_device(n, x.data_ptr(), None, y.data_ptr(), A.data_ptr(), prec, st.cuda_stream)
+        for _ in range(args.warmup):
+            f()
+        torch.cuda.synchronize()
+        out[prec] = (_timed(f, st, args.steps), y.cpu().numpy().copy(), A.cpu().numpy().copy())
+    ms = out[glb.PREC_FP64][0]
+    line = _base_line(args, "rays/s/GPU (plain FP64 form)", "rays/s", n / (ms / 1e3), ms, "f64",
+                      "single NFW particle plane: 2^18 particles, 512^2 rays over 30 arcsec, z_l=0.3, z_s=2")
+    line["split"] = {"value": n / (out[glb.PREC_SPLIT][0] / 1e3), "unit": "rays/s",
+                     "errors_vs_fp64": error_stats(x_host, out[1][1], out[1][2], out[0][1], out[0][2])}
+    if not args.no_cpu:
+        from tests import harness as H
+        if H.ref_available():
+            R = H.RefDriver()
+            tf = R._file()
+            R.run([f"threads {tf}"])
+            thr = int(np.fromfile(tf)[0])
+            yr, Ar, secs = R.grid(spec, n1d, range_rad=rng)
+            line["cpu_baseline"] = {"value": n / secs, "unit": "rays/s", "cores": thr, "kind": "reference",
+                                    "sample": "the full 512^2 GridMap"}
+            line["parity_vs_reference"] = {
+                "y_max_rel": float(np.max(np.abs(out[0][1] - yr) / np.abs(yr))),
+                "A_max_abs": float(np.max(np.abs(out[0][2] - Ar)))}
+    print(json.dumps(line))
+
+
+def run_sweep(args):
+    """Precision sweep on one large plane: 2^24 triaxial-NFW particles
+    (1e15 Msun, c=4, axes 1/0.8/0.6) + 10% uniform background, 4096^2 rays
+    over 40 arcsec at z_l=0.3; opening angles 0.05/0.1/0.3; FP64, split and
+    plain FP32 trees; errors against an FP64 direct sum on 1000 seeded rays."""
+    import torch
+    import slsimlib_b200 as glb
+    from slsimlib_b200 import synth
+    rs = np.random.default_rng(3)
+    cosmo = synth.Cosmology()
+    n_halo = 2 ** 24 if not args.small else 2 ** 20
+    p = synth.nfw_particles(rs, n_halo, 1e15, 4.0, 0.3, 1e-3, cosmo=cosmo, axis_ratios=(0.8, 0.6))
+    nb = int(round(0.1 * n_halo))
+    lo = p["x"][:, :2].min(axis=0)
+    hi = p["x"][:, :2].max(axis=0)
+    bg = np.zeros(nb, dtype=synth.PARTICLE_DTYPE)
+    bg["x"][:, :2] = rs.uniform(lo, hi, size=(nb, 2)).astype(np.float32)
+    bg["Mass"] = p["Mass"][0]
+    bg["Size"] = np.float32(1e-3)
+    parts = np.concatenate([p, bg])
+    n1d = 4096 if not args.small else 1024
+    da = cosmo.angdist(0.3)
+    ang = synth.grid_positions(n1d, range_rad=40 * synth.ARCSEC)
+    rays = (ang * da)[_tile_order(n1d)]
+    n = len(rays)
+    dr = torch.from_numpy(np.ascontiguousarray(rays)).cuda()
+    out = torch.empty((n, 5), dtype=torch.float64, device="cuda")
+    sub = np.random.default_rng(4).choice(n, size=1000, replace=False)
+    drs = dr[torch.from_numpy(sub).cuda()].contiguous()
+    pdev = torch.from_numpy(parts.view(np.uint8)).cuda()
+    ds = torch.empty((1000, 5), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    glb.direct_sum_device(len(parts), pdev.data_ptr(), 0.0, 1000, drs.data_ptr(), ds.data_ptr(), None)
+    torch.cuda.synchronize()
+    ds = ds.cpu().numpy()
+    st = torch.cuda.Stream()
+    torch.cuda.set_stream(st)
+    results = []
+    for theta in (0.05, 0.1, 0.3):
+        tree = glb.TreeQuadParticles(parts, bucket=20, theta_force=theta)
+        for prec, name in ((glb.PREC_FP64, "fp64"), (glb.PREC_SPLIT, "split"), (glb.PREC_FP32, "fp32")):
+            f = lambda: tree.force_device(n, dr.data_ptr(), out.data_ptr(), prec, st.cuda_stream)
+            f()
+            torch.cuda.synchronize()
+            ms = _timed(f, st, max(1, args.steps // 2))
+            o = out.cpu().numpy()[sub]
+            na = np.hypot(ds[:, 0], ds[:, 1])
+            e = np.hypot(o[:, 0] - ds[:, 0], o[:, 1] - ds[:, 1]) / na
+            results.append({"theta": theta, "form": name, "rays_per_s": n / (ms / 1e3), "ms": ms,
+                            "alpha_err_vs_direct": {"median": float(np.median(e)), "p999": float(np.percentile(e, 99.9))},
+                            "build_ms": tree.build_ms()})
+        del tree
+    best = [r for r in results if r["theta"] == 0.1 and r["form"] == "split"][0]
+    line = _base_line(args, "rays/s/GPU of the split tree at theta=0.1 (one plane)", "rays/s", best["rays_per_s"],
+                      best["ms"], "f32+f64", f"precision sweep: {len(parts)} particles, {n1d}^2 rays over 40 arcsec")
+    line["sweep"] = results
+    print(json.dumps(line))
+
+
+def _random_lens_c4(seed):
+    from slsimlib_b200 import synth
+    r = np.random.default_rng(seed)
+    n_p = int(2 ** r.uniform(14, 20))
+    m = 10 ** r.uniform(12, 15)
+    c = r.uniform(3, 10)
+    side = int(round(2 ** r.uniform(6, 10)))
+    zs = r.uniform(1, 3)
+    three = r.random() < 0.5
+    zl = r.uniform(0.2, 0.8)
+    zls = [zl - 0.15, zl, zl + 0.15] if three else [zl]
+    halos = []
+    for z in zls:
+        k = n_p // len(zls)
+        halos.append(synth.ParticlePlane(synth.nfw_particles(r, k, m / len(zls), c, z, 1e-3), z))
+    return synth.LensSpec(zsource=max(zs, zls[-1] + 0.05), halos=halos), side
+
+
+def run_batched(args):
+    """256 independent single- or three-plane NFW particle lenses (N_p in
+    2^14-2^20, M in 1e12-1e15, c in 3-10, grid side in 64-1024, z_s in 1-3)
+    shot by one persistent launch replayed from a CUDA graph, block size
+    picked by the autotuner; split precision."""
+    import multiprocessing as mp
+    import slsimlib_b200 as glb
+    from slsimlib_b200 import synth
+    nl = 256 if not args.small else 32
+    with mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
+        specs = pool.map(_random_lens_c4, [4000 + i for i in range(nl)])
+    lenses = [make_lens(s) for s, _ in specs]
+    sides = [side for _, side in specs]
+    rng = 30 * synth.ARCSEC
+    b = glb.GridBatch(lenses, sides, [(0.0, 0.0)] * nl, [rng] * nl, glb.PREC_SPLIT)
+    block, tune_ms = b.autotune()
+    for _ in range(args.warmup):
+        b.run(True)
+    ms = [b.run(True) for _ in range(args.steps)]
+    total = sum(s * s for s in sides)
+    rp = sum(s * s * l.getNplanes() for s, l in zip(sides, lenses))
+    # the FP64 form of the same batch, for the error of the split form
+    b64 = glb.GridBatch(lenses, sides, [(0.0, 0.0)] * nl, [rng] * nl, glb.PREC_FP64)
+    ms64 = b64.run(True)
+    errs = []
+    for i in range(0, nl, max(1, nl // 16)):
+        y, A = b.result(i)
+        y64, A64 = b64.result(i)
+        x = synth.grid_positions(sides[i], range_rad=rng)
+        errs.append(error_stats(x, y, A, y64, A64)["alpha"])
+    m = float(np.median(ms))
+    line = _base_line(args, "rays/s/GPU, batched uneven lenses in one persistent launch", "rays/s", total / (m / 1e3),
+                      m, "f32+f64", f"{nl} lens realisations, {total} rays, {rp} ray-planes, CUDA graph",
+                      ray_planes_per_s=rp / (m / 1e3), autotune={"block": block, "ms": tune_ms},
+                      plain_fp64={"value": total / (ms64 / 1e3), "unit": "rays/s"},
+                      errors_vs_fp64_alpha={"median_of_medians": float(np.median([e["median"] for e in errs])),
+                                            "max_p999": float(max(e["p999"] for e in errs))})
+    print(json.dumps(line))
+
+
+def _c5_model(seed):
+    from slsimlib_b200 import synth
+    return synth.light_cone(seed=seed)
+
+
+def run_served(args):
+    """32 resident light-cone models; Poisson request stream at swept rates;
+    request sizes log-uniform in 1e3-5e5 rays in 1-8 Gaussian blobs
+    (sigma 0.05-1 arcsec); z_s uniform in 1-3; split precision."""
+    import multiprocessing as mp
+    import threading
+    import slsimlib_b200 as glb
+    from slsimlib_b200 import synth
+    nm = 32 if not args.small else 4
+    with mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
+        specs = pool.map(_c5_model, [5000 + i for i in range(nm)])
+    models = [make_lens(s) for s in specs]
+    srv = glb.Server(models, max_rays_per_batch=2_000_000, precision=glb.PREC_SPLIT, nslots=3)
+    r = np.random.default_rng(5)
+    half = 30 * synth.ARCSEC
+
+    def request():
+        n = int(10 ** r.uniform(3, np.log10(5e5)))
+        nb = int(r.integers(1, 9))
+        cen = r.uniform(-half, half, size=(nb, 2))
+        sig = 10 ** r.uniform(np.log10(0.05), 0) * synth.ARCSEC
+        which = r.integers(0, nb, size=n)
+        x = cen[which] + r.normal(0, sig, size=(n, 2))
+        return int(r.integers(0, nm)), x, float(r.uniform(1, 3))
+
+    sweep = []
+    nreq = 120 if not args.small else 30
+    for lam in (5.0, 20.0, 60.0):
+        reqs = [request() for _ in range(nreq)]
+        gaps = r.exponential(1 / lam, size=nreq)
+        tickets = []
+        t0 = time.perf_counter()
+        tnext = t0
+        for (m, x, zs), g in zip(reqs, gaps):
+            tnext += g
+            d = tnext - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            tickets.append(srv.submit(m, x, zs))
+        lat, rays = [], 0
+        tdone = 0
+        for (m, x, zs), t in zip(reqs, tickets):
+            y, A, tm = srv.wait(t, timeout=600)
+            lat.append((tm[2] - tm[0]) * 1e3)
+            rays += len(x)
+            tdone = max(tdone, tm[2])
+        wall = time.perf_counter() - t0
+        sweep.append({"rate_req_per_s": lam, "requests": nreq, "rays": rays, "rays_per_s": rays / wall,
+                      "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))})
+    st = srv.stats()
+    # error of served (split) results against the plain FP64 path on a few requests
+    errs = []
+    for _ in range(4):
+        m, x, zs = request()
+        y, A, _ = srv.wait(srv.submit(m, x, zs), timeout=600)
+        y64, A64 = models[m].rayshooterInternal(x, np.full(len(x), zs), precision=glb.PREC_FP64)
+        errs.append(error_stats(x, y, A, y64, A64)["alpha"])
+    srv.close()
+    top = max(sweep, key=lambda s: s["rays_per_s"])
+    line = _base_line(args, "rays/s/GPU served; p50/p99 request ms", "rays/s", top["rays_per_s"],
+                      None, "f32+f64", f"{nm} resident light-cone models, Poisson request stream",
+                      sweep=sweep, server=st,
+                      errors_vs_fp64_alpha={"median": float(np.median([e["median"] for e in errs])),
+                                            "max_p999": float(max(e["p999"] for e in errs))})
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -185,7 +447,16 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--small", action="store_true", help="a reduced workload for quick checks")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--workload", default="lightcone",
+                    choices=["lightcone", "single", "sweep", "batched", "served"],
+                    help="lightcone (default): the 10-plane light cone; the others are the single plane, the "
+                         "precision sweep, batched uneven lenses and the served request stream")
     args = ap.parse_args()
+    if args.impl == "ours" and args.workload != "lightcone":
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        return {"single": run_single, "sweep": run_sweep, "batched": run_batched, "served": run_served}[
+            args.workload](args)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
