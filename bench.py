@@ -447,6 +447,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--small", action="store_true", help="a reduced workload for quick checks")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--n1d", type=int, default=0,
+                    help="rays per side of the light-cone grid (default 2048; a profiling size, not a bench line)")
     ap.add_argument("--workload", default="lightcone",
                     choices=["lightcone", "single", "sweep", "batched", "served"],
                     help="lightcone (default): the 10-plane light cone; the others are the single plane, the "
@@ -473,6 +475,8 @@ def main():
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     spec, n1d = workload(args.small)
+    if args.n1d:
+        n1d = args.n1d
     n = n1d * n1d
     lens = make_lens(spec)
     x_host = synth.grid_positions(n1d, range_rad=FIELD_ARCSEC * synth.ARCSEC)

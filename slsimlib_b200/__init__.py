@@ -32,7 +32,8 @@ __all__ = [
 ]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libglamer_b200.so")
+# SLSIMLIB_B200_LIB selects another build of the library (e.g. for A/B timing of kernel variants)
+LIB_PATH = os.environ.get("SLSIMLIB_B200_LIB") or os.path.join(HERE, "libglamer_b200.so")
 
 PREC_FP64 = 0
 PREC_SPLIT = 1

@@ -59,7 +59,12 @@ __device__ __forceinline__ void plane_force(const PlaneDev &P, const HaloDev *ha
       acc[0] = -acc[0];
       acc[1] = -acc[1];
     } else if (valid) {
-      analytic_halo(H, tab, xc0, xc1, acc);
+      const Force5 f = analytic_halo(H, tab, xc0, xc1);
+      acc[0] = f.a0;
+      acc[1] = f.a1;
+      acc[2] = f.k;
+      acc[3] = f.g0;
+      acc[4] = f.g1;
     }
     out[0] -= acc[0];
     out[1] -= acc[1];

@@ -36,11 +36,15 @@ struct __align__(16) GNode {
 // FP32 node of the split-precision walk (64 bytes).  The centre of mass is a
 // double-float pair (hi + lo, both FP32), so that a ray offset computed as
 // (cxh - rxh) + (cxl - rxl) carries FP32 relative precision however far the
-// node sits from the origin.
+// node sits from the origin.  Mass and quadrupole are stored divided by pi;
+// the width is rounded up to FP32, so that for an FP32 softening length
+// size < width_ru holds exactly when size < width does.  Rows 0, 1 and 3 are
+// read by every opening test (issued together, so that their latencies
+// overlap), row 2 by far-field terms and leaves.
 struct __align__(16) GNodeS {
   float cxh, cyh, cxl, cyl;
-  float open2, near2, mass, q0;
-  float q1, q2, width, pad;
+  float open2, near2, mpi, q0pi;
+  float q1pi, q2pi, width_ru, pad;
   int skip, leaf, start, count;  // leaf: particle range; internal: big-particle range
 };
 
@@ -49,7 +53,7 @@ struct TreeDev {
   const GNodeS *snodes;
   const float4 *parts;  // sorted particles {x, y, mass, size}
   const float4 *bigs;   // big-particle list of internal nodes
-  const float4 *prel;   // sorted particles relative to their leaf's centre of mass (FP32)
+  const float4 *prel;   // sorted particles {x - leaf cx, y - leaf cy, -mass/pi, near radius^2} (FP32)
   int nnodes;
   int nparticles;
   double inv_area;
@@ -60,6 +64,10 @@ struct TreeDev {
   // read by its far-field potential (quadTree.h:1103-1104)
   double phi_mass, phi_q0, phi_q1, phi_q2;
   double phiintconst;
+  // masses of one sign: the split walk adds the inv_area sheet's deflection in
+  // closed form from the root's mass and centre instead of term by term
+  int sheet_closed;
+  double root_mass, root_cx, root_cy;
 };
 
 enum HaloKind { HALO_PARTICLES = 0, HALO_NFW = 1, HALO_NSIE = 2 };

@@ -353,12 +353,19 @@ __device__ __forceinline__ void particle_halo_acc(const TreeDev &T, double rx, d
 
 // Analytic halo of a plane at one position; kept out of line so that the rare
 // NFW / NSIE arithmetic does not add to the register budget of the tree walk.
-__device__ __noinline__ void analytic_halo(const HaloDev *H, const NFWTables *tab, double x0, double x1,
-                                           double *acc) {
+// The result comes back by value: a caller's accumulator array passed by
+// pointer to an out-of-line function would be moved to local memory, and the
+// tree walk's flushes into it with it.
+struct Force5 {
+  double a0, a1, k, g0, g1;
+};
+__device__ __noinline__ Force5 analytic_halo(const HaloDev *H, const NFWTables *tab, double x0, double x1) {
+  double acc[6] = {0, 0, 0, 0, 0, 0};
   if (H->kind == HALO_NFW)
     nfw_force<false>(H->nfw, *tab, x0, x1, acc);
   else
     nsie_force<false>(H->nsie, x0, x1, acc);
+  return Force5{acc[0], acc[1], acc[2], acc[3], acc[4]};
 }
 
 struct StepArgs {
@@ -378,8 +385,12 @@ struct StepArgs {
 
 // One lens plane for every ray: LensPlaneSingular::force + the recursion of
 // include/lens.h:1003-1066.
+// The split form is latency-bound (dependent node loads); capping it at 80
+// registers (6 blocks of 128 per SM) buys the occupancy that hides them.
+constexpr int split_min_blocks(int prec) { return prec == GLB_PREC_FP64 ? 1 : 6; }
+
 template <int PREC, bool COUNT = false>
-__global__ void __launch_bounds__(128) k_plane_step(StepArgs a) {
+__global__ void __launch_bounds__(128, split_min_blocks(PREC)) k_plane_step(StepArgs a) {
   const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   const bool inrange = k < a.n;
   const size_t n = a.n;
@@ -422,7 +433,12 @@ __global__ void __launch_bounds__(128) k_plane_step(StepArgs a) {
       acc[0] = -acc[0];
       acc[1] = -acc[1];
     } else if (valid) {
-      analytic_halo(H, &a.tab, xc0, xc1, acc);
+      const Force5 f = analytic_halo(H, &a.tab, xc0, xc1);
+      acc[0] = f.a0;
+      acc[1] = f.a1;
+      acc[2] = f.k;
+      acc[3] = f.g0;
+      acc[4] = f.g1;
     }
     al0 -= acc[0];
     al1 -= acc[1];
@@ -496,7 +512,8 @@ __global__ void __launch_bounds__(128) k_halo_force(HaloDev H, NFWTables tab, si
 // force2D_recur on device rays in the three precision forms (no potential):
 // out = 5 doubles per ray {alpha0, alpha1, kappa, gamma0, gamma1}.
 template <int PREC>
-__global__ void __launch_bounds__(128) k_tree_force(TreeDev T, size_t n, const double *x, double *out) {
+__global__ void __launch_bounds__(128, split_min_blocks(PREC)) k_tree_force(TreeDev T, size_t n, const double *x,
+                                                                            double *out) {
   const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   const bool valid = k < n;
   if (!__any_sync(kFull, valid)) return;

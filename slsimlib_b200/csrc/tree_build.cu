@@ -240,11 +240,15 @@ __global__ void k_leaf_moments(Slot *s, int lo, int hi, const glb_particle_rec *
     Syy += __shfl_xor_sync(kFullMask, Syy, o);
     Sxy += __shfl_xor_sync(kFullMask, Sxy, o);
   }
-  // particle offsets from the leaf's centre of mass, for the split-precision walk
+  // records of the split-precision walk: offset from the leaf's centre of
+  // mass, -mass/pi and the squared near-field radius (two softening lengths,
+  // widened by 2.5e-5 against FP32 rounding; at least 1e-12 so that
+  // coincident particles are sent to FP64)
   for (int k = b.start + lane; k < b.start + b.count; k += 32) {
     unsigned id = sidx[k];
+    const double sz = (double)p[multiradius ? id : 0].Size;
     prel[k] = make_float4((float)((double)p[id].x[0] - cx), (float)((double)p[id].x[1] - cy),
-                          p[multimass ? id : 0].Mass, p[multiradius ? id : 0].Size);
+                          (float)(-(double)p[multimass ? id : 0].Mass / kPi), (float)fmax(4.0001 * sz * sz, 1e-12));
   }
   if (lane == 0) {
     b.mass = M;
@@ -412,11 +416,11 @@ __global__ void k_emit_nodes(const Slot *s, int nslots, double theta, GNode *nod
   f.cyl = (float)(g.cy - (double)f.cyh);
   f.open2 = (float)g.open2;
   f.near2 = (float)g.near2;
-  f.mass = (float)g.mass;
-  f.q0 = (float)g.q0;
-  f.q1 = (float)g.q1;
-  f.q2 = (float)g.q2;
-  f.width = (float)g.width;
+  f.mpi = (float)(g.mass / kPi);
+  f.q0pi = (float)(g.q0 / kPi);
+  f.q1pi = (float)(g.q1 / kPi);
+  f.q2pi = (float)(g.q2 / kPi);
+  f.width_ru = __double2float_ru(g.width);
   f.pad = 0;
   f.skip = g.skip;
   f.leaf = g.leaf;
@@ -439,7 +443,13 @@ __global__ void k_gather_bigs(const float4 *parts, const unsigned *bval, int nb,
   bigs[b] = parts[bval[b]];
 }
 
+// out[0..3]: mass and quadrupole of the last branch of the moments walk (the
+// far-field potential's); out[4..7]: the root's mass, |mass| sum and centre.
 __global__ void k_phi_node(const Slot *s, double *out) {
+  out[4] = s[0].count > 0 ? s[0].mass : 0.0;
+  out[5] = s[0].count > 0 ? s[0].absm : 0.0;
+  out[6] = s[0].count > 0 ? s[0].comx : 0.0;
+  out[7] = s[0].count > 0 ? s[0].comy : 0.0;
   int cur = 0;
   for (int L = 0; L < kMaxDepth && s[cur].child >= 0; ++L) cur = s[cur].child + 3;
   const Slot &b = s[cur];
@@ -654,9 +664,9 @@ Status build_tree(const glb_particle_rec *hp, size_t n, const TreeParams &prm, b
   CK(T->snodes.alloc(nnodes));
   k_emit_nodes<<<nblk(nslots, 256), 256, 0, st>>>(slots.p, nslots, prm.theta, T->nodes.p, T->snodes.p);
   DBuf<double> phin;
-  CK(phin.alloc(4));
+  CK(phin.alloc(8));
   k_phi_node<<<1, 1, 0, st>>>(slots.p, phin.p);
-  double hphi[4];
+  double hphi[8];
   CK(cudaMemcpyAsync(hphi, phin.p, sizeof(hphi), cudaMemcpyDeviceToHost, st));
   if (want_export) {
     DBuf<double> ex;
@@ -677,6 +687,14 @@ Status build_tree(const glb_particle_rec *hp, size_t n, const TreeParams &prm, b
   T->dev.phi_q0 = hphi[1];
   T->dev.phi_q1 = hphi[2];
   T->dev.phi_q2 = hphi[3];
+  // With masses of one sign every cell's |m|-weighted centre is its
+  // m-weighted one, so the inv_area sheet summed over any walk's far-field
+  // cells and leaf particles is the root's term: inv_area M (centre - ray).
+  // Σ|m| and |Σm| are then the same sums of the same values, bit for bit.
+  T->dev.sheet_closed = hphi[5] == fabs(hphi[4]) ? 1 : 0;
+  T->dev.root_mass = hphi[4];
+  T->dev.root_cx = hphi[6];
+  T->dev.root_cy = hphi[7];
   T->dev.nodes = T->nodes.p;
   T->dev.snodes = T->snodes.p;
   T->dev.parts = T->parts.p;

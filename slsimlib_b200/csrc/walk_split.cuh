@@ -8,39 +8,70 @@
 //     one side of the threshold (further than 4e-6 relative, ~8x the FP32
 //     error bound); otherwise the test is repeated in FP64 on the exact
 //     node, so every ray interacts with exactly the cells of the FP64 form.
-//   * Far-field and leaf-particle terms are evaluated in FP32; a leaf
-//     particle's offset is (particle - leaf centre of mass, stored in FP32 at
-//     build time) + (leaf centre of mass - ray).
-//   * Particles within two softening lengths of the ray, whose point-mass term
-//     is cancelled by a B-spline correction, and the B-spline corrections
-//     themselves, are evaluated entirely in FP64.
+//   * Far-field and leaf-particle terms are evaluated in FP32, x/y pairs with
+//     the packed FP32x2 instructions of sm_100 (one issue slot per pair); a
+//     leaf particle's offset is (particle - leaf centre of mass, stored in
+//     FP32 at build time) + (leaf centre of mass - ray).
+//   * A leaf particle within two softening lengths whose B-spline correction
+//     the reference applies at the same leaf is evaluated as one softened
+//     mass: point mass and correction summed analytically, so the two terms
+//     that cancel as r -> 0 never meet in floating point.  Particles whose
+//     correction is applied at an ancestor node (softening >= leaf width),
+//     (nearly) coincident particles and the ancestors' corrections stay in
+//     FP64, exactly as walk_f64 evaluates them.
+//   * The inv_area sheet is added once per walk in FP64 where that is exact
+//     algebra (its kappa always; its deflection for masses of one sign), not
+//     as ~1e4 FP32 terms that cancel near the mass centre.
 //   * Sums are compensated by blocking: FP32 partial sums of at most 32 terms
 //     are flushed into FP64 totals, which bounds the accumulation error by the
 //     per-term rounding instead of letting it grow with the ~1e4 terms of a
 //     walk.
+// Node and particle records of this form carry mass / pi, quadrupole / pi,
+// -mass / pi and the squared near-field radius (GNodeS, TreeDev::prel).
 #pragma once
 #include "walk.cuh"
 
 namespace glb {
 
+// FP32 partial sums of one walk: alpha and gamma as x/y pairs for the packed
+// instructions (g.y holds gamma[1] / 2), kappa, and the number of terms
+// since the last flush into the FP64 totals.
 struct F32Acc {
-  float a0, a1, k, g0, g1;
+  float2 a, g;
+  float k;
   int cnt;
   __device__ __forceinline__ void zero() {
-    a0 = a1 = k = g0 = g1 = 0.f;
+    a = make_float2(0.f, 0.f);
+    g = make_float2(0.f, 0.f);
+    k = 0.f;
     cnt = 0;
   }
   __device__ __forceinline__ void flush(double *acc) {
-    acc[0] += (double)a0;
-    acc[1] += (double)a1;
+    acc[0] += (double)a.x;
+    acc[1] += (double)a.y;
     acc[2] += (double)k;
-    acc[3] += (double)g0;
-    acc[4] += (double)g1;
+    acc[3] += (double)g.x;
+    acc[4] += 2.0 * (double)g.y;
     zero();
   }
 };
 
 constexpr float kAmbiguous = 4e-6f;  // relative band around a threshold decided in FP64
+constexpr float kLog2e = 1.4426950408889634f;
+constexpr float kInvPiF = (float)(1.0 / kPi);
+
+// PTX approximate base-2 exponential and reciprocal (the MUFU unit).
+__device__ __forceinline__ float ex2_approx(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float rcp_approx(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float2 f2(float v) { return make_float2(v, v); }
 
 // Exact FP64 threshold test for the rare rays in the ambiguity band.
 __device__ __noinline__ bool node_test_f64(const GNode *nd, double rx, double ry, int which) {
@@ -48,15 +79,14 @@ __device__ __noinline__ bool node_test_f64(const GNode *nd, double rx, double ry
   return (dx * dx + dy * dy) < (which ? nd->near2 : nd->open2);
 }
 
-// x-width of a node record (GNodeS.width), read only by the plain FP32 form.
-__device__ __forceinline__ float c2w(const float4 *sp) { return __ldg(sp + 2).z; }
-
 struct Near64 {
   double a0, a1, k, g0, g1;
 };
 
-// A leaf particle within two softening lengths of the ray: the point mass and
-// its B-spline correction in FP64, exactly as walk_f64 evaluates them.
+// A leaf particle evaluated in FP64, exactly as walk_f64 does: the point mass
+// and, when the leaf applies it, its B-spline correction.  The inv_area
+// sheet's deflection is included with inv_area != 0; its kappa never (the
+// caller adds the sheet's kappa in closed form).
 __device__ __noinline__ Near64 near_particle_f64(float4 Q, double rx, double ry, double screen2, double inv_area,
                                                   bool nearc, double width) {
   Near64 o;
@@ -71,7 +101,6 @@ __device__ __noinline__ Near64 near_particle_f64(float4 Q, double rx, double ry,
   const double tmp = -2.0 * prefac * ir2;
   acc[3] = 0.5 * (y0 * y0 - y1 * y1) * tmp;
   acc[4] = y0 * y1 * tmp;
-  acc[2] = -m * inv_area;
   const double size = (double)Q.w;
   if (nearc && size < width && rr < 4 * size * size) bspline_f64<false>(y0, y1, sqrt(rr), m, size, 0.0, acc);
   o.a0 = acc[0];
@@ -82,10 +111,52 @@ __device__ __noinline__ Near64 near_particle_f64(float4 Q, double rx, double ry,
   return o;
 }
 
+// A softened particle at 0 < r < 2 size: the screened point mass of
+// quadTree.h:1017-1046 plus the B-spline correction of b_spline_profile
+// (quadTree.h:147-190), summed in closed form.  With q = r/size,
+// u = 2 - q and c = 10 / (7 pi size^2), the cubic spline's enclosed-mass
+// fraction M and surface density sigma give
+//   M / (pi r^2)          = c (1 - 3q/4 + 3q^3/10)             (q <= 1)
+//                         = (1 - u^4 (5/2 - u) / 7) / (pi r^2)  (1 < q < 2)
+//   sigma                 = c (1 - 3q^2/2 + 3q^3/4)             (q <= 1)
+//                         = c u^3 / 4                            (1 < q < 2)
+//   M/(pi r^2) - sigma    = c q (-3/4 + 3q/2 - 9q^2/20)          (q <= 1)
+// and, with E = exp(-r^2 s2) - 1 (screening of the point mass only),
+//   alpha += -m (E/(pi r^2) + M/(pi r^2)) x
+//   gamma += -m (E/(pi r^2) + M/(pi r^2) - sigma) (x0^2 - x1^2, 2 x0 x1) / r^2
+//   kappa +=  m sigma
+// which is algebraically the reference's sum but has no cancellation between
+// the point mass and its correction (both ~1/r as r -> 0).
+__device__ __forceinline__ void softened_f32(float2 x, float r2, float m, float size, float s2, F32Acc &fa) {
+  const float r = sqrtf(r2);
+  const float is = __fdividef(1.f, size);
+  const float q = r * is;
+  const float c = (float)(10.0 / 7.0 / kPi) * is * is;
+  float Mr, sg, sh;
+  if (q <= 1.f) {
+    const float q2 = q * q;
+    Mr = c * fmaf(q2 * q, 0.3f, fmaf(q, -0.75f, 1.f));
+    sg = c * fmaf(q2 * q, 0.75f, fmaf(q2, -1.5f, 1.f));
+    sh = c * q * fmaf(q, fmaf(q, -0.45f, 1.5f), -0.75f);
+  } else {
+    const float u = 2.f - q, u2 = u * u;
+    const float M = fmaf(-u2 * u2, (2.5f - u) * (float)(1.0 / 7.0), 1.f);
+    Mr = M * kInvPiF * __fdividef(1.f, r2);
+    sg = c * u2 * u * 0.25f;
+    sh = Mr - sg;
+  }
+  const float er = s2 != 0.f ? expm1f(-r2 * s2) * __fdividef(1.f, r2) * kInvPiF : 0.f;
+  const float ac = -m * (er + Mr);
+  const float gc = -m * (er + sh) * __fdividef(1.f, r2);
+  fa.a = __ffma2_rn(f2(ac), x, fa.a);
+  fa.g = __ffma2_rn(f2(gc), make_float2(x.x * x.x - x.y * x.y, x.x * x.y), fa.g);
+  fa.k = fmaf(m, sg, fa.k);
+}
+
 // b_spline_profile (include/quadTree.h:147-190) in FP32, for the plain FP32
 // form only.
 __device__ __forceinline__ void bspline_f32(float x0, float x1, float r, float Mass, float size, float *f) {
-  const float ipi = (float)(1.0 / kPi);
+  const float ipi = kInvPiF;
   const float q = r / size;
   float M, sigma;
   if (q > 2.f) {
@@ -112,15 +183,19 @@ __device__ __forceinline__ void bspline_f32(float x0, float x1, float r, float M
 }
 
 // PURE = true is the plain FP32 form of the precision sweep: FP32 offsets
-// from FP32 coordinates, FP32 opening tests and sums throughout, FP32
-// near field; it keeps no FP64 arithmetic and so no guarantee of the FP64
-// form's interaction set or precision.
+// from FP32 coordinates, FP32 opening tests and sums throughout, the
+// reference's FP32-evaluated B-spline; it keeps no FP64 arithmetic and so no
+// guarantee of the FP64 form's interaction set or precision.
 template <bool PURE = false>
 __device__ __forceinline__ void walk_split(const TreeDev &T, double rx, double ry, bool valid, double *acc) {
-  const float inv_pi = (float)(1.0 / kPi);
   const bool screen = T.screen2 != 0.0;
   const float s2f = (float)T.screen2;
-  const float iaf = (float)T.inv_area;
+  const float ns2l = -s2f * kLog2e;          // exp(-r2 s2) = 2^(r2 ns2l)
+  // inv_area sheet: in closed form at the end (masses of one sign), else term
+  // by term; piaf is the sheet per unit of mass/pi
+  const bool closed = !PURE && T.sheet_closed;
+  const bool sheet = T.inv_area != 0.0 && !closed;
+  const float piaf = sheet ? (float)(kPi * T.inv_area) : 0.f;
   const float rxh = (float)rx, ryh = (float)ry;
   const float rxl = PURE ? 0.f : (float)(rx - (double)rxh), ryl = PURE ? 0.f : (float)(ry - (double)ryh);
   float pf[5] = {0.f, 0.f, 0.f, 0.f, 0.f};  // PURE: the FP32 total
@@ -131,41 +206,41 @@ __device__ __forceinline__ void walk_split(const TreeDev &T, double rx, double r
   const int nn = T.nnodes;
   while (node < nn) {
     const float4 *sp = reinterpret_cast<const float4 *>(T.snodes + node);
-    const float4 c0 = __ldg(sp), c1 = __ldg(sp + 1);
-    const int4 c3 = __ldg(reinterpret_cast<const int4 *>(sp + 3));
+    const float4 c0 = __ldg(sp), c1 = __ldg(sp + 1);  // centre; open2, near2, mass/pi, q0/pi
+    const int4 c3 = __ldg(reinterpret_cast<const int4 *>(sp + 3));  // skip, leaf, start, count
     const int skip = max(c3.x, node + 1);  // forward progress even on a malformed array
     const bool act = node >= resume;
-    const float dxf = PURE ? (c0.x - rxh) : (c0.x - rxh) + (c0.z - rxl);
-    const float dyf = PURE ? (c0.y - ryh) : (c0.y - ryh) + (c0.w - ryl);
-    const float r2f = dxf * dxf + dyf * dyf;
+    const float2 d = PURE ? make_float2(c0.x - rxh, c0.y - ryh)
+                          : make_float2((c0.x - rxh) + (c0.z - rxl), (c0.y - ryh) + (c0.w - ryl));
+    const float2 dd = __fmul2_rn(d, d);
+    const float r2f = dd.x + dd.y;
     bool open = false;
     if (act) {
-      const float d = r2f - c1.x;
-      open = d < 0.f;
-      if (!PURE && fabsf(d) <= kAmbiguous * c1.x) open = node_test_f64(T.nodes + node, rx, ry, 0);
+      const float e = r2f - c1.x;
+      open = e < 0.f;
+      if (!PURE && fabsf(e) <= kAmbiguous * c1.x) open = node_test_f64(T.nodes + node, rx, ry, 0);
     }
     if (act && !open) {
-      // far field: monopole + quadrupole (quadTree.h:1090-1123)
+      // far field: monopole + quadrupole (quadTree.h:1090-1123); c1.z = mass/pi,
+      // c1.w, c2.x, c2.y = quadrupole/pi
       const float4 c2 = __ldg(sp + 2);
-      const float scr = screen ? __expf(-r2f * s2f) : 1.0f;
-      const float ir2 = __fdividef(1.0f, r2f);
-      const float ir4 = ir2 * ir2;
-      const float mass = c1.z, q0 = c1.w, q1 = c2.x, q2 = c2.y;
-      const float ms = mass * inv_pi * scr;
-      const float t = mass * iaf - ms * ir2;
-      const float qd = (q0 * dxf * dxf + q1 * dyf * dyf + 2.f * q2 * dxf * dyf);
-      const float qs = inv_pi * scr * ir4;
-      const float t4 = 4.f * qd * qs * ir2;
-      fa.a0 += (t + t4) * dxf - (q0 * dxf + q2 * dyf) * qs;
-      fa.a1 += (t + t4) * dyf - (q1 * dyf + q2 * dxf) * qs;
-      fa.g0 -= ms * ir2 * ((dxf * dxf - dyf * dyf) * ir2);
-      fa.g1 -= ms * ir2 * (2.0f * dxf * dyf * ir2);
-      fa.k -= iaf * mass;
-      if (PURE) {
-        pf[0] += fa.a0; pf[1] += fa.a1; pf[2] += fa.k; pf[3] += fa.g0; pf[4] += fa.g1;
-        fa.zero();
-      } else if (++fa.cnt >= 32) {
-        fa.flush(acc);
+      const float scr = screen ? ex2_approx(r2f * ns2l) : 1.0f;
+      const float ir2 = rcp_approx(r2f);
+      const float ms = c1.z * scr;                 // mass/pi, screened
+      const float sir4 = scr * ir2 * ir2;
+      const float qx = fmaf(c1.w, d.x, c2.y * d.y), qy = fmaf(c2.x, d.y, c2.y * d.x);
+      const float qd = fmaf(qx, d.x, qy * d.y);    // q0 dx^2 + q1 dy^2 + 2 q2 dx dy
+      const float t = fmaf(c1.z, piaf, -ms * ir2) + 4.f * qd * sir4 * ir2;
+      float2 a = __ffma2_rn(f2(t), d, PURE ? make_float2(0.f, 0.f) : fa.a);
+      a = __ffma2_rn(f2(-sir4), make_float2(qx, qy), a);
+      float2 g = __ffma2_rn(f2(-ms * ir2 * ir2), make_float2(dd.x - dd.y, d.x * d.y),
+                            PURE ? make_float2(0.f, 0.f) : fa.g);
+      if (PURE) {  // (the split form adds the sheet's kappa in closed form)
+        pf[0] += a.x; pf[1] += a.y; pf[2] -= piaf * c1.z; pf[3] += g.x; pf[4] += 2.f * g.y;
+      } else {
+        fa.a = a;
+        fa.g = g;
+        if (++fa.cnt >= 32) fa.flush(acc);
       }
       resume = skip;
     }
@@ -181,51 +256,63 @@ __device__ __forceinline__ void walk_split(const TreeDev &T, double rx, double r
     }
     if (c3.y) {  // leaf
       const int p0 = c3.z, p1 = p0 + c3.w;
+      const float wu = __ldg(sp + 2).z;  // leaf width rounded up to FP32: size < wu <=> size < width
       if (open && fa.cnt) fa.flush(acc);
       // particles in chunks of 32 so that the FP32 partial sums stay short
       for (int q0 = p0; q0 < p1; q0 += 32) {
         const int q1 = min(q0 + 32, p1);
         for (int p = q0; p < q1; ++p) {
-          const float4 P = __ldg(T.prel + p);
-          if (open) {
-            const float x0 = P.x + dxf, x1 = P.y + dyf;
-            float rcm2f = x0 * x0 + x1 * x1;
-            if (PURE) {
-              // plain FP32: point mass, then the B-spline if within two sizes
-              const float scr = screen ? __expf(-rcm2f * s2f) : 1.0f;
-              const float rr = fmaxf(rcm2f, 1e-20f);
-              const float m = P.z, ir2 = __fdividef(1.0f, rr), prefac = m * scr * ir2 * inv_pi;
-              pf[0] += (iaf * m - prefac) * x0;
-              pf[1] += (iaf * m - prefac) * x1;
-              pf[3] -= prefac * ir2 * (x0 * x0 - x1 * x1);
-              pf[4] -= prefac * ir2 * (2.0f * x0 * x1);
-              pf[2] -= m * iaf;
-              if (nearc && P.w < c2w(sp) && rr < 4.f * P.w * P.w) bspline_f32(x0, x1, sqrtf(rr), m, P.w, pf);
-            } else if (rcm2f < fmaxf(4.0001f * P.w * P.w, 1e-12f)) {  // near or (unsoftened) coincident
-              const Near64 o = near_particle_f64(__ldg(T.parts + p), rx, ry, T.screen2, T.inv_area, nearc,
+          const float4 P = __ldg(T.prel + p);  // {x - cx, y - cy, -mass/pi, near radius^2}
+          if (!open) continue;
+          const float2 x = __fadd2_rn(make_float2(P.x, P.y), d);
+          const float2 xx = __fmul2_rn(x, x);
+          const float r2 = xx.x + xx.y;
+          if (PURE) {
+            // plain FP32: point mass, then the B-spline if within two sizes
+            const float scr = screen ? ex2_approx(r2 * ns2l) : 1.0f;
+            const float rr = fmaxf(r2, 1e-20f);
+            const float ir2 = __fdividef(1.0f, rr);
+            const float npre = P.z * scr * ir2;    // -mass scr / (pi r^2)
+            const float ta = npre - piaf * P.z;
+            pf[0] += ta * x.x;
+            pf[1] += ta * x.y;
+            pf[3] += npre * ir2 * (xx.x - xx.y);
+            pf[4] += npre * ir2 * (2.0f * x.x * x.y);
+            pf[2] += piaf * P.z;
+            if (nearc && rr < P.w) {
+              const float4 Q = __ldg(T.parts + p);
+              if (Q.w < wu && rr < 4.f * Q.w * Q.w) bspline_f32(x.x, x.y, sqrtf(rr), Q.z, Q.w, pf);
+            }
+            continue;
+          }
+          bool point = true;
+          if (r2 < P.w) {  // within two softening lengths (or coincident)
+            const float4 Q = __ldg(T.parts + p);
+            if (r2 < 1e-12f || !(Q.w < wu)) {
+              const Near64 o = near_particle_f64(Q, rx, ry, T.screen2, sheet ? T.inv_area : 0.0, nearc,
                                                  T.nodes[node].width);
               acc[0] += o.a0;
               acc[1] += o.a1;
               acc[2] += o.k;
               acc[3] += o.g0;
               acc[4] += o.g1;
-            } else {
-              const float scr = screen ? __expf(-rcm2f * s2f) : 1.0f;
-              const float m = P.z;
-              const float ir2 = __fdividef(1.0f, rcm2f);
-              const float prefac = m * scr * ir2 * inv_pi;
-              const float ta = iaf * m - prefac;
-              fa.a0 += ta * x0;
-              fa.a1 += ta * x1;
-              // shear terms scaled by 1/r^2 first so that nothing overflows FP32
-              const float pi2 = prefac * ir2;
-              fa.g0 -= pi2 * (x0 * x0 - x1 * x1);
-              fa.g1 -= pi2 * (2.0f * x0 * x1);
-              fa.k -= m * iaf;
+              point = false;
+            } else if (nearc && r2 < 4.f * Q.w * Q.w) {
+              softened_f32(x, r2, Q.z, Q.w, s2f, fa);
+              if (sheet) fa.a = __ffma2_rn(f2(-piaf * P.z), x, fa.a);
+              point = false;
             }
           }
+          if (point) {
+            const float scr = screen ? ex2_approx(r2 * ns2l) : 1.0f;
+            const float ir2 = rcp_approx(r2);
+            const float npre = P.z * scr * ir2;  // -mass scr / (pi r^2)
+            fa.a = __ffma2_rn(f2(npre), x, fa.a);
+            fa.g = __ffma2_rn(f2(npre * ir2), make_float2(xx.x - xx.y, x.x * x.y), fa.g);
+            if (sheet) fa.a = __ffma2_rn(f2(-piaf * P.z), x, fa.a);  // inv_area * mass * x
+          }
         }
-        if (open) fa.flush(acc);
+        if (!PURE && open) fa.flush(acc);
       }
       node = skip;
     } else {
@@ -253,6 +340,17 @@ __device__ __forceinline__ void walk_split(const TreeDev &T, double rx, double r
     for (int c = 0; c < 5; ++c) acc[c] += (double)pf[c];
   } else {
     fa.flush(acc);
+    // the sheet's kappa is -inv_area x (total mass) for every walk (each
+    // particle's mass enters exactly once, in a cell or as a leaf particle);
+    // its deflection is closed-form for masses of one sign
+    if (T.inv_area != 0.0 && nn > 0) {
+      const double s = T.inv_area * T.root_mass;
+      acc[2] -= s;
+      if (closed) {
+        acc[0] += s * (T.root_cx - rx);
+        acc[1] += s * (T.root_cy - ry);
+      }
+    }
   }
 }
 

@@ -298,3 +298,38 @@ def test_tree_force_device_forms_and_direct_sum():
     torch.cuda.synchronize()
     ds = H.direct_sum(p, rays[:64])
     assert np.max(vec_err(o.cpu().numpy()[:, :2], ds[:, :2])) < 1e-10
+
+
+@pytest.mark.parametrize("inv_area,screen,negative", [(0.0, 0.0, False), (4.0, 0.0, False), (0.0, 1.0, False),
+                                                     (4.0, 30.0, False), (4.0, 1.0, True)])
+def test_split_tree_force_softened_regime(inv_area, screen, negative):
+    """Split form against the FP64 form where most leaf particles lie within two
+    softening lengths of the rays (softening larger than the core's leaves, so
+    B-spline corrections are applied both at leaves and at ancestors), with and
+    without the inv_area sheet (closed form for masses of one sign, term by
+    term for mixed signs) and screening: alpha, kappa and gamma within 1e-6
+    median / 1e-5 99.9th percentile; the plain FP32 form loosely."""
+    import torch
+    rng = np.random.default_rng(21)
+    p = synth.nfw_particles(rng, 60000, 1e14, 5.0, 0.3, 4e-3)
+    p["Size"][:500] = np.float32(2e-2)  # a few much larger softenings
+    if negative:
+        p["Mass"][::10] *= np.float32(-0.5)
+    rays = np.concatenate([rng.normal(0, 0.01, (3000, 2)), rng.uniform(-0.2, 0.2, (1000, 2))])
+    t = glb.TreeQuadParticles(p, inv_area=inv_area, bucket=20, theta_force=0.1, inv_screening_scale=screen)
+    dr = torch.from_numpy(rays).cuda()
+    outs = {}
+    for prec in (glb.PREC_FP64, glb.PREC_SPLIT, glb.PREC_FP32):
+        o = torch.zeros((len(rays), 5), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        t.force_device(len(rays), dr.data_ptr(), o.data_ptr(), prec, None)
+        torch.cuda.synchronize()
+        outs[prec] = o.cpu().numpy()
+    ref = outs[glb.PREC_FP64]
+    orc = H.OracleTree(p, bucket=20, theta=0.1, inv_area=inv_area, inv_screening=screen).force(rays[:100])
+    assert np.max(vec_err(ref[:100, :2], orc[:, :2])) < RTOL64  # the FP64 form is the reference's walk
+    s = outs[glb.PREC_SPLIT]
+    for name, e in (("alpha", vec_err(s[:, :2], ref[:, :2])), ("kappa", scal_err(s[:, 2], ref[:, 2], 1e-6)),
+                    ("gamma", vec_err(s[:, 3:5], ref[:, 3:5]))):
+        assert np.median(e) <= 1e-6 and np.percentile(e, 99.9) <= 1e-5, (name, np.median(e), e.max())
+    assert np.median(vec_err(outs[glb.PREC_FP32][:, :2], ref[:, :2])) < 1e-4
