@@ -75,7 +75,8 @@ __device__ __forceinline__ void plane_force(const PlaneDev &P, const HaloDev *ha
 }
 
 template <int PREC>
-__global__ void __launch_bounds__(256) k_batch(const Chunk *chunks, int nchunks, const LensDev *lenses,
+// capped at 80 registers (3 blocks of 256 per SM) for occupancy, as k_plane_step_split
+__global__ void __launch_bounds__(256, 3) k_batch(const Chunk *chunks, int nchunks, const LensDev *lenses,
                                                NFWTables tab, const double *xs, const unsigned *outidx,
                                                double *y, double *A, int *counter) {
   const int lane = threadIdx.x & 31;

@@ -385,12 +385,8 @@ struct StepArgs {
 
 // One lens plane for every ray: LensPlaneSingular::force + the recursion of
 // include/lens.h:1003-1066.
-// The split form is latency-bound (dependent node loads); capping it at 80
-// registers (6 blocks of 128 per SM) buys the occupancy that hides them.
-constexpr int split_min_blocks(int prec) { return prec == GLB_PREC_FP64 ? 1 : 6; }
-
 template <int PREC, bool COUNT = false>
-__global__ void __launch_bounds__(128, split_min_blocks(PREC)) k_plane_step(StepArgs a) {
+__device__ __forceinline__ void plane_step(const StepArgs &a) {
   const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   const bool inrange = k < a.n;
   const size_t n = a.n;
@@ -485,6 +481,15 @@ __global__ void __launch_bounds__(128, split_min_blocks(PREC)) k_plane_step(Step
   st[11 * n + k] = s3;
 }
 
+// The FP64 form keeps the compiler's own register choice; the split form is
+// latency-bound (dependent node loads), and capping it at 80 registers
+// (6 blocks of 128 per SM) buys the occupancy that hides them.
+template <int PREC, bool COUNT = false>
+__global__ void __launch_bounds__(128) k_plane_step(StepArgs a) {
+  plane_step<PREC, COUNT>(a);
+}
+__global__ void __launch_bounds__(128, 6) k_plane_step_split(StepArgs a) { plane_step<GLB_PREC_SPLIT>(a); }
+
 // force2D_recur / force_halo at arbitrary positions (walk-level API, with phi).
 __global__ void __launch_bounds__(128) k_halo_force(HaloDev H, NFWTables tab, size_t n, const double *x,
                                                     double *out) {
@@ -512,8 +517,7 @@ __global__ void __launch_bounds__(128) k_halo_force(HaloDev H, NFWTables tab, si
 // force2D_recur on device rays in the three precision forms (no potential):
 // out = 5 doubles per ray {alpha0, alpha1, kappa, gamma0, gamma1}.
 template <int PREC>
-__global__ void __launch_bounds__(128, split_min_blocks(PREC)) k_tree_force(TreeDev T, size_t n, const double *x,
-                                                                            double *out) {
+__device__ __forceinline__ void tree_force(const TreeDev &T, size_t n, const double *x, double *out) {
   const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   const bool valid = k < n;
   if (!__any_sync(kFull, valid)) return;
@@ -526,6 +530,15 @@ __global__ void __launch_bounds__(128, split_min_blocks(PREC)) k_tree_force(Tree
   particle_halo_acc<PREC, false>(T, x0, x1, valid, acc);
   if (!valid) return;
   for (int c = 0; c < 5; ++c) out[5 * k + c] = acc[c];
+}
+
+__global__ void __launch_bounds__(128) k_tree_force(TreeDev T, size_t n, const double *x, double *out) {
+  tree_force<GLB_PREC_FP64>(T, n, x, out);
+}
+// the FP32-arithmetic forms, capped at 80 registers as k_plane_step_split
+template <int PREC>
+__global__ void __launch_bounds__(128, 6) k_tree_force_lo(TreeDev T, size_t n, const double *x, double *out) {
+  tree_force<PREC>(T, n, x, out);
 }
 
 // FP64 direct summation over every particle (no tree): the point mass and the
@@ -734,7 +747,7 @@ int rayshoot_device(glb_lens *l, size_t n, const double *x, const double *zs, do
     if (d_counts)
       k_plane_step<GLB_PREC_FP64, true><<<nblk(n, 128), 128, 0, s>>>(a);
     else if (precision == GLB_PREC_SPLIT)
-      k_plane_step<GLB_PREC_SPLIT><<<nblk(n, 128), 128, 0, s>>>(a);
+      k_plane_step_split<<<nblk(n, 128), 128, 0, s>>>(a);
     else
       k_plane_step<GLB_PREC_FP64><<<nblk(n, 128), 128, 0, s>>>(a);
   }
@@ -870,11 +883,11 @@ int glb_tree_force_device(glb_tree *t, size_t n, const double *rays_dev, double 
   }
   (void)cudaGetLastError();
   if (precision == GLB_PREC_FP64)
-    k_tree_force<GLB_PREC_FP64><<<nblk(n, 128), 128, 0, s>>>(t->tree->dev, n, rays_dev, out_dev);
+    k_tree_force<<<nblk(n, 128), 128, 0, s>>>(t->tree->dev, n, rays_dev, out_dev);
   else if (precision == GLB_PREC_SPLIT)
-    k_tree_force<GLB_PREC_SPLIT><<<nblk(n, 128), 128, 0, s>>>(t->tree->dev, n, rays_dev, out_dev);
+    k_tree_force_lo<GLB_PREC_SPLIT><<<nblk(n, 128), 128, 0, s>>>(t->tree->dev, n, rays_dev, out_dev);
   else
-    k_tree_force<GLB_PREC_FP32><<<nblk(n, 128), 128, 0, s>>>(t->tree->dev, n, rays_dev, out_dev);
+    k_tree_force_lo<GLB_PREC_FP32><<<nblk(n, 128), 128, 0, s>>>(t->tree->dev, n, rays_dev, out_dev);
   CKR(cudaGetLastError());
   return 0;
 }
@@ -1503,7 +1516,7 @@ extern "C" int glb_lens_rayshoot_noalloc(glb_lens *l, size_t n, const double *x_
   for (int j = 0; j < jmax_launch; ++j) {
     a.j = j;
     if (precision == GLB_PREC_SPLIT)
-      k_plane_step<GLB_PREC_SPLIT><<<nblk(n, 128), 128, 0, s>>>(a);
+      k_plane_step_split<<<nblk(n, 128), 128, 0, s>>>(a);
     else
       k_plane_step<GLB_PREC_FP64><<<nblk(n, 128), 128, 0, s>>>(a);
   }
