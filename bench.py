@@ -40,6 +40,10 @@ FIELD_ARCSEC = 60.0
 # (nodes tested V, far-field cells F, leaf point masses P, big-particle checks B,
 # B-spline corrections S) and per ray-plane recursion
 FLOPS = {"V": 8, "F": 60, "P": 29, "B": 8, "S": 65, "rec": 50}
+# DRAM bytes (read + write) per ray of one split plane launch, from an ncu capture of
+# `bench.py --no-cpu --n1d 1536` (479 MB for 2,359,296 rays): the 96 B ray state read and
+# written once, plus the plane's L2-resident tree
+DRAM_BYTES_PER_RAY_PLANE = 203
 
 
 def workload(small: bool):
@@ -578,8 +582,10 @@ def main():
             "e2e": {"value": world * n * args.steps / e2e_s, "unit": "rays/s", "h2d_bytes_per_step": 16 * n,
                     "d2h_bytes_per_step": 48 * n},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": None,
-                         "kernel": "k_plane_step<split>", "kernel_ms_per_step": k_ms,
+                         "frac": achieved / peak, "traffic": DRAM_BYTES_PER_RAY_PLANE * n,
+                         "traffic_note": "dram read+write bytes per plane launch: ncu capture of one 1536^2 launch "
+                                         "(203 B/ray) scaled by rays",
+                         "kernel": "k_plane_step_split", "kernel_ms_per_step": k_ms,
                          "peak_note": "FP32 CUDA-core FMA rate at the sampled SM clock (148 SMs x 128 lanes x 2)",
                          "alg_flops_per_step": alg_flops,
                          "counts": {"V": V, "F": F, "P": P, "B": B, "S": S},
