@@ -18,6 +18,9 @@ constexpr double kPi = 3.14159265358979323846;  // include/standard.h:39 (M_PI)
 constexpr double kGrav = 4.7788e-20;              // include/standard.h:43
 constexpr double kLightspeed = 2.99792458e5;      // km/s
 constexpr int kMaxDepth = 32;                     // 2-bit Morton digits in a 64-bit key
+// Relative band around an opening threshold inside which the split-precision
+// walk repeats its FP32 test in FP64 (~8x the FP32 error of the test).
+constexpr float kAmbiguous = 4e-6f;
 
 // One tree node (preorder, non-empty).  96 bytes.
 struct __align__(16) GNode {
@@ -36,15 +39,17 @@ struct __align__(16) GNode {
 // FP32 node of the split-precision walk (64 bytes).  The centre of mass is a
 // double-float pair (hi + lo, both FP32), so that a ray offset computed as
 // (cxh - rxh) + (cxl - rxl) carries FP32 relative precision however far the
-// node sits from the origin.  Mass and quadrupole are stored divided by pi;
-// the width is rounded up to FP32, so that for an FP32 softening length
-// size < width_ru holds exactly when size < width does.  Rows 0, 1 and 3 are
-// read by every opening test (issued together, so that their latencies
-// overlap), row 2 by far-field terms and leaves.
+// node sits from the origin.  open_band is the half-width of the band around
+// open2 inside which the opening test is repeated in FP64.  Mass and
+// quadrupole are stored divided by pi; the width is rounded up to FP32, so
+// that for an FP32 softening length size < width_ru holds exactly when
+// size < width does.  Rows 0, 1 and 3 are read by every opening test (issued
+// together, so that their latencies overlap), row 2 by far-field terms and
+// leaves.
 struct __align__(16) GNodeS {
   float cxh, cyh, cxl, cyl;
-  float open2, near2, mpi, q0pi;
-  float q1pi, q2pi, width_ru, pad;
+  float open2, near2, mpi, open_band;
+  float q1pi, q2pi, width_ru, q0pi;
   int skip, leaf, start, count;  // leaf: particle range; internal: big-particle range
 };
 

@@ -421,7 +421,7 @@ __global__ void k_emit_nodes(const Slot *s, int nslots, double theta, GNode *nod
   f.q1pi = (float)(g.q1 / kPi);
   f.q2pi = (float)(g.q2 / kPi);
   f.width_ru = __double2float_ru(g.width);
-  f.pad = 0;
+  f.open_band = kAmbiguous * f.open2;
   f.skip = g.skip;
   f.leaf = g.leaf;
   f.start = g.leaf ? g.pstart : g.bstart;

@@ -56,7 +56,6 @@ struct F32Acc {
   }
 };
 
-constexpr float kAmbiguous = 4e-6f;  // relative band around a threshold decided in FP64
 constexpr float kLog2e = 1.4426950408889634f;
 constexpr float kInvPiF = (float)(1.0 / kPi);
 
@@ -198,6 +197,7 @@ __device__ __forceinline__ void walk_split(const TreeDev &T, double rx, double r
   const float piaf = sheet ? (float)(kPi * T.inv_area) : 0.f;
   const float rxh = (float)rx, ryh = (float)ry;
   const float rxl = PURE ? 0.f : (float)(rx - (double)rxh), ryl = PURE ? 0.f : (float)(ry - (double)ryh);
+  const float2 nrh = make_float2(-rxh, -ryh), nrl = make_float2(-rxl, -ryl);  // negated ray, hi and lo
   float pf[5] = {0.f, 0.f, 0.f, 0.f, 0.f};  // PURE: the FP32 total
   F32Acc fa;
   fa.zero();
@@ -206,29 +206,29 @@ __device__ __forceinline__ void walk_split(const TreeDev &T, double rx, double r
   const int nn = T.nnodes;
   while (node < nn) {
     const float4 *sp = reinterpret_cast<const float4 *>(T.snodes + node);
-    const float4 c0 = __ldg(sp), c1 = __ldg(sp + 1);  // centre; open2, near2, mass/pi, q0/pi
+    const float4 c0 = __ldg(sp), c1 = __ldg(sp + 1);  // centre; open2, near2, mass/pi, open band
     const int4 c3 = __ldg(reinterpret_cast<const int4 *>(sp + 3));  // skip, leaf, start, count
     const int skip = max(c3.x, node + 1);  // forward progress even on a malformed array
     const bool act = node >= resume;
-    const float2 d = PURE ? make_float2(c0.x - rxh, c0.y - ryh)
-                          : make_float2((c0.x - rxh) + (c0.z - rxl), (c0.y - ryh) + (c0.w - ryl));
+    const float2 d = PURE ? __fadd2_rn(make_float2(c0.x, c0.y), nrh)
+                          : __fadd2_rn(__fadd2_rn(make_float2(c0.x, c0.y), nrh), __fadd2_rn(make_float2(c0.z, c0.w), nrl));
     const float2 dd = __fmul2_rn(d, d);
     const float r2f = dd.x + dd.y;
     bool open = false;
     if (act) {
       const float e = r2f - c1.x;
       open = e < 0.f;
-      if (!PURE && fabsf(e) <= kAmbiguous * c1.x) open = node_test_f64(T.nodes + node, rx, ry, 0);
+      if (!PURE && fabsf(e) <= c1.w) open = node_test_f64(T.nodes + node, rx, ry, 0);  // c1.w: the band
     }
     if (act && !open) {
       // far field: monopole + quadrupole (quadTree.h:1090-1123); c1.z = mass/pi,
-      // c1.w, c2.x, c2.y = quadrupole/pi
+      // c2.w, c2.x, c2.y = quadrupole/pi
       const float4 c2 = __ldg(sp + 2);
       const float scr = screen ? ex2_approx(r2f * ns2l) : 1.0f;
       const float ir2 = rcp_approx(r2f);
       const float ms = c1.z * scr;                 // mass/pi, screened
       const float sir4 = scr * ir2 * ir2;
-      const float qx = fmaf(c1.w, d.x, c2.y * d.y), qy = fmaf(c2.x, d.y, c2.y * d.x);
+      const float qx = fmaf(c2.w, d.x, c2.y * d.y), qy = fmaf(c2.x, d.y, c2.y * d.x);
       const float qd = fmaf(qx, d.x, qy * d.y);    // q0 dx^2 + q1 dy^2 + 2 q2 dx dy
       const float t = fmaf(c1.z, piaf, -ms * ir2) + 4.f * qd * sir4 * ir2;
       float2 a = __ffma2_rn(f2(t), d, PURE ? make_float2(0.f, 0.f) : fa.a);
