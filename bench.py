@@ -161,7 +161,7 @@ def run_reference_arm(args, rank):
         return
     spec, n1d = workload(args.small)
     vals = []
-    nsample = 2048 if args.small else 4096
+    nsample = 2048 if args.small else 16384
     threads = 0
     for s in range(args.warmup + args.steps):
         r = cpu_reference(spec, n1d, nsample, seed=100 + s)
@@ -176,7 +176,8 @@ def run_reference_arm(args, rank):
             "config": {"workload": f"light cone: 10 planes, 4,194,304 particles + NSIE, {n1d}^2 rays over 60 arcsec",
                        "sample_rays_per_step": nsample},
             "cpu_baseline": {"value": v, "unit": "rays/s", "cores": threads, "kind": "reference",
-                             "sample": f"{nsample} seeded rays per step, all 11 planes, rate extrapolated per ray"},
+                             "sample": f"{nsample} seeded rays of the grid per step (a new sample each step), all "
+                                       f"planes, rate extrapolated per ray"},
             "e2e": {"value": v, "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
