@@ -536,7 +536,9 @@ void orc_direct_sum(const orc_particle *p, size_t n, double inv_area, const doub
 }
 
 /* =========================== halos ===================================== */
-enum { ORC_PARTICLES = 0, ORC_NFW = 1, ORC_NSIE = 2 };
+enum { ORC_PARTICLES = 0, ORC_NFW = 1, ORC_NSIE = 2, ORC_FIELD = 3 };
+
+typedef struct orc_halotree orc_halotree;
 
 struct orc_halo {
   int kind;
@@ -548,6 +550,7 @@ struct orc_halo {
   float sigma, fratio, pa, rcore, units;
   orc_tree *tree;
   orc_particle *owned;
+  orc_halotree *htree; /* ORC_FIELD: LensPlaneTree's TreeQuadHalos */
 };
 
 /* ---- NFW profile functions, AnalyticNSIE/nfw_lens.cpp:82-132 ---- */
@@ -752,10 +755,13 @@ void orc_halo_set_theta(orc_halo *h, double tx, double ty) {
   h->posHalo[0] = tx;
   h->posHalo[1] = ty;
 }
+static void halotree_free(orc_halotree *t);
+
 void orc_halo_free(orc_halo *h) {
   if (!h) return;
   orc_tree_free(h->tree);
   free(h->owned);
+  halotree_free(h->htree);
   free(h);
 }
 float orc_halo_mass(const orc_halo *h) { return h->mass; }
@@ -850,11 +856,16 @@ static void nsie_force(const orc_halo *h, const double *xcm, double *alpha, doub
   nsie_force_inner(h, xcm, alpha, kappa, gamma);
 }
 
+static void halotree_force2D(const orc_halotree *t, const double *ray, double *alpha, double *kappa,
+                             double *gamma, double *phi);
+
 /* One halo at one position; the particle halo overwrites and negates alpha
- * (include/particle_halo.h:426-434). */
+ * (include/particle_halo.h:426-434); a field plane's halo tree overwrites
+ * (LensPlaneTree::force, MultiPlane/planes.cpp:65-68). */
 static void halo_force_one(orc_halo *h, const double *xcm, double *alpha, double *kappa,
                            double *gamma, double *phi) {
   switch (h->kind) {
+    case ORC_FIELD: halotree_force2D(h->htree, xcm, alpha, kappa, gamma, phi); break;
     case ORC_PARTICLES:
       orc_tree_force2D_recur(h->tree, xcm, alpha, kappa, gamma, phi);
       alpha[0] *= -1;
@@ -880,6 +891,305 @@ void orc_halo_force(orc_halo *h, size_t n, const double *xcm, double *alpha, dou
   }
 }
 
+/* =================== TreeQuadHalos / LensPlaneTree ===================== */
+/* A quadtree over analytic haloes (include/quadTreeHalos.h:35-130) as built by
+ * LensPlaneTree (MultiPlane/planes.cpp:13-18). */
+typedef struct orc_hbranch {
+  size_t *particles;
+  size_t nparticles;
+  size_t *big;
+  size_t nbig;
+  double center[2];
+  double mass;
+  double p1[2], p2[2];
+  struct orc_hbranch *child[4];
+  struct orc_hbranch *brother;
+  double quad[3];
+  double rmax;
+  double r2crit;
+} orc_hbranch;
+
+struct orc_halotree {
+  int n;
+  orc_halo **halos;  /* owned */
+  double *xp;        /* 2n: LensHalo::getX at construction */
+  size_t *index;
+  double *work;
+  double inv_area;
+  int bucket;
+  double theta;
+  int periodic;
+  double inv_screen2;
+  double max_range;
+  double original_xl, original_yl;
+  orc_hbranch *top;
+};
+
+static void hbranch_free(orc_hbranch *b) {
+  if (!b) return;
+  for (int c = 0; c < 4; ++c) hbranch_free(b->child[c]);
+  free(b->big);
+  free(b);
+}
+
+static void halotree_free(orc_halotree *t) {
+  if (!t) return;
+  hbranch_free(t->top);
+  for (int i = 0; i < t->n; ++i) orc_halo_free(t->halos[i]);
+  free(t->halos);
+  free(t->xp);
+  free(t->index);
+  free(t->work);
+  free(t);
+}
+
+/* TreeQuadHalos::_BuildQTreeNB, include/quadTreeHalos.h:239-450.  Big
+ * haloes (Rmax beyond half the box) are listed at the branch and still passed
+ * on to its children; a leaf lists all of its haloes as big. */
+static void hbuild_rec(orc_halotree *t, orc_hbranch *cb, int at_top) {
+  size_t i, cut = 0, cut2 = 0, cutx = 0, cuty = 0;
+  size_t *particles = cb->particles;
+  const size_t np = cb->nparticles;
+  cb->center[0] = (cb->p1[0] + cb->p2[0]) / 2;
+  cb->center[1] = (cb->p1[1] + cb->p2[1]) / 2;
+  cb->quad[0] = cb->quad[1] = cb->quad[2] = 0;
+  cb->mass = 0.0;
+  double theta_range = 2 * t->theta;
+  if (t->max_range > 0) {
+    double boxsize = 1.732 * (cb->p2[0] - cb->p1[0]);
+    double d = sqrt(cb->center[0] * cb->center[0] + cb->center[1] * cb->center[1]) - t->max_range;
+    theta_range = boxsize / (d > boxsize ? d : boxsize);
+  }
+  if (np <= (size_t)t->bucket || t->theta > theta_range) {
+    cb->nbig = np;
+    cb->big = (size_t *)malloc((np ? np : 1) * sizeof(size_t));
+    for (i = 0; i < np; ++i) cb->big[i] = particles[i];
+    return;
+  }
+  double *x = t->work;
+  cb->nbig = 0;
+  for (i = 0; i < np; ++i) x[i] = (double)t->halos[particles[i]]->Rmax;
+  double half_box = (cb->p2[0] - cb->p1[0]) / 2;
+  quick_partition(half_box, &cut, particles, x, np);
+  if (cut < np) {
+    if (at_top) {
+      cb->nbig = cut2 = np - cut;
+    } else {
+      quick_partition(2 * half_box, &cut2, &particles[cut], &x[cut], np - cut);
+      cb->nbig = cut2;
+    }
+    cb->big = (size_t *)malloc((cut2 ? cut2 : 1) * sizeof(size_t));
+    for (i = cut; i < cut + cut2; ++i) cb->big[i - cut] = particles[i];
+  }
+  orc_hbranch *c[4];
+  for (int k = 0; k < 4; ++k) c[k] = (orc_hbranch *)calloc(1, sizeof(orc_hbranch));
+  for (int k = 0; k < 3; ++k) c[k]->brother = c[k + 1];
+  c[3]->brother = cb->brother;
+  for (int k = 0; k < 4; ++k) cb->child[k] = c[k];
+  c[0]->p1[0] = cb->center[0]; c[0]->p1[1] = cb->center[1]; c[0]->p2[0] = cb->p2[0]; c[0]->p2[1] = cb->p2[1];
+  c[1]->p1[0] = cb->p1[0]; c[1]->p1[1] = cb->center[1]; c[1]->p2[0] = cb->center[0]; c[1]->p2[1] = cb->p2[1];
+  c[2]->p1[0] = cb->center[0]; c[2]->p1[1] = cb->p1[1]; c[2]->p2[0] = cb->p2[0]; c[2]->p2[1] = cb->center[1];
+  c[3]->p1[0] = cb->p1[0]; c[3]->p1[1] = cb->p1[1]; c[3]->p2[0] = cb->center[0]; c[3]->p2[1] = cb->center[1];
+  const double xcut = cb->center[0], ycut = cb->center[1];
+  for (i = 0; i < np; ++i) x[i] = t->xp[2 * particles[i] + 1];
+  quick_partition(ycut, &cuty, particles, x, np);
+  if (cuty > 0) {
+    for (i = 0; i < cuty; ++i) x[i] = t->xp[2 * particles[i]];
+    quick_partition(xcut, &cutx, particles, x, cuty);
+    c[3]->nparticles = cutx;
+    c[3]->particles = cutx > 0 ? particles : NULL;
+    c[2]->nparticles = cuty - cutx;
+    c[2]->particles = cuty - cutx > 0 ? &particles[cutx] : NULL;
+  }
+  if (cuty < np) {
+    for (i = cuty; i < np; ++i) x[i - cuty] = t->xp[2 * particles[i]];
+    quick_partition(xcut, &cutx, &particles[cuty], x, np - cuty);
+    c[1]->nparticles = cutx;
+    c[1]->particles = cutx > 0 ? &particles[cuty] : NULL;
+    c[0]->nparticles = np - cuty - cutx;
+    c[0]->particles = np - cuty - cutx > 0 ? &particles[cuty + cutx] : NULL;
+  }
+  for (int k = 0; k < 4; ++k) hbuild_rec(t, c[k], 0);
+}
+
+/* TreeQuadHalos::CalcMoments, include/quadTreeHalos.h:453-513 (one branch). */
+static void hmoments_one(orc_halotree *t, orc_hbranch *cb) {
+  size_t i;
+  cb->rmax = sqrt(pow(cb->p2[0] - cb->p1[0], 2) + pow(cb->p2[1] - cb->p1[1], 2));
+  for (i = 0, cb->mass = 0; i < cb->nparticles; ++i) cb->mass += t->halos[cb->particles[i]]->mass;
+  cb->center[0] = cb->center[1] = 0;
+  for (i = 0; i < cb->nparticles; ++i) {
+    double tmp = t->halos[cb->particles[i]]->mass;
+    cb->center[0] += tmp * t->xp[2 * cb->particles[i]] / cb->mass;
+    cb->center[1] += tmp * t->xp[2 * cb->particles[i] + 1] / cb->mass;
+  }
+  cb->quad[0] = cb->quad[1] = cb->quad[2] = 0;
+  for (i = 0; i < cb->nparticles; ++i) {
+    double xcm0 = t->xp[2 * cb->particles[i]] - cb->center[0];
+    double xcm1 = t->xp[2 * cb->particles[i] + 1] - cb->center[1];
+    double xcut = pow(xcm0, 2) + pow(xcm1, 2);
+    double tmp = t->halos[cb->particles[i]]->mass;
+    cb->quad[0] += (xcut - 2 * xcm0 * xcm0) * tmp;
+    cb->quad[1] += (xcut - 2 * xcm1 * xcm1) * tmp;
+    cb->quad[2] += -2 * xcm0 * xcm1 * tmp;
+  }
+  double rcom = 0.0;
+  for (i = 0; i < 2; ++i) {
+    double a = pow(cb->center[i] - cb->p1[i], 2), b = pow(cb->center[i] - cb->p2[i], 2);
+    rcom += (a > b) ? a : b;
+  }
+  rcom = sqrt(rcom);
+  if (t->theta > 0.0) {
+    cb->r2crit = 1.15470 * rcom / (t->theta);
+    cb->r2crit *= cb->r2crit;
+  } else {
+    cb->r2crit = 1.0e100;
+  }
+}
+
+static void hmoments_rec(orc_halotree *t, orc_hbranch *b) {
+  hmoments_one(t, b);
+  if (b->child[0])
+    for (int k = 0; k < 4; ++k) hmoments_rec(t, b->child[k]);
+}
+
+/* LensPlaneTree(z, halos, n, sigma_background, inv_screening_scale),
+ * MultiPlane/planes.cpp:13-18: TreeQuadHalos(halos, n, sigma_background) with
+ * its defaults (bucket 5, theta 0.5, no periodic buffer, no screening), or
+ * with screening: bucket 5, theta 0.1, periodic buffer
+ * (include/quadTreeHalos.h:129-159, 173-236).  The haloes are moved to
+ * redshift z first (LensHalo::setZlensDist, as Lens::createFieldPlanes does,
+ * MultiPlane/lens.cpp:418-426).  Takes ownership of the haloes. */
+orc_halo *orc_halo_field_plane(orc_halo **halos, int n, double z, double sigma_back, double inv_screening,
+                               int *err) {
+  *err = 0;
+  orc_halotree *t = (orc_halotree *)calloc(1, sizeof(orc_halotree));
+  t->n = n;
+  t->halos = (orc_halo **)malloc((n ? n : 1) * sizeof(orc_halo *));
+  for (int i = 0; i < n; ++i) t->halos[i] = halos[i];
+  t->inv_area = sigma_back;
+  if (inv_screening != 0) {
+    t->bucket = 5; t->theta = 0.1; t->periodic = 1;
+  } else {
+    t->bucket = 5; t->theta = 0.5; t->periodic = 0;
+  }
+  t->inv_screen2 = inv_screening * inv_screening;
+  t->max_range = -1;
+  t->xp = (double *)malloc((2 * n + 2) * sizeof(double));
+  t->index = (size_t *)malloc((n ? n : 1) * sizeof(size_t));
+  t->work = (double *)malloc((n ? n : 1) * sizeof(double));
+  for (int i = 0; i < n; ++i) {
+    orc_halo *h = halos[i];
+    h->zlens = z;
+    h->Dist = orc_angdist(z);
+    t->xp[2 * i] = h->posHalo[0] * h->Dist; /* LensHalo::getX, include/lens_halos.h:95-99 */
+    t->xp[2 * i + 1] = h->posHalo[1] * h->Dist;
+    t->index[i] = i;
+  }
+  orc_halo *out = (orc_halo *)calloc(1, sizeof(orc_halo));
+  out->kind = ORC_FIELD;
+  out->zlens = z;
+  out->Dist = orc_angdist(z);
+  out->htree = t;
+  if (n > 0) {
+    /* TreeQuadHalos::BuildQTreeNB, include/quadTreeHalos.h:173-236 */
+    double p1[2] = {t->xp[0], t->xp[1]}, p2[2] = {t->xp[0], t->xp[1]};
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < 2; ++j) {
+        if (t->xp[2 * i + j] < p1[j]) p1[j] = t->xp[2 * i + j];
+        if (t->xp[2 * i + j] > p2[j]) p2[j] = t->xp[2 * i + j];
+      }
+    if (n == 1) {
+      p1[0] = -0.25; p1[1] = -0.25; p2[0] = 0.25; p2[1] = 0.25;
+    }
+    double lengths[2] = {p2[0] - p1[0], p2[1] - p1[1]};
+    t->original_xl = lengths[0];
+    t->original_yl = lengths[1];
+    if (lengths[0] == 0 || lengths[1] == 0) {
+      *err = 1; /* "particles in same place." */
+      t->n = 0; /* the caller keeps its haloes */
+      orc_halo_free(out);
+      return NULL;
+    }
+    int j = lengths[0] > lengths[1] ? 1 : 0;
+    p2[j] = p1[j] + lengths[!j];
+    t->top = (orc_hbranch *)calloc(1, sizeof(orc_hbranch));
+    t->top->p1[0] = p1[0]; t->top->p1[1] = p1[1];
+    t->top->p2[0] = p2[0]; t->top->p2[1] = p2[1];
+    t->top->nparticles = n;
+    t->top->particles = t->index;
+    hbuild_rec(t, t->top, 1);
+    hmoments_rec(t, t->top);
+  }
+  return out;
+}
+
+/* TreeQuadHalos::walkTree_iter, include/quadTreeHalos.h:648-815. */
+static void hwalk(const orc_halotree *t, const double *ray, double *alpha, double *kappa, double *gamma,
+                  double *phi) {
+  const orc_hbranch *b = t->top;
+  while (b) {
+    int descend = 1;
+    for (size_t i = 0; i < b->nbig; ++i) {
+      size_t k = b->big[i];
+      double xcm[2] = {t->xp[2 * k] - ray[0], t->xp[2 * k + 1] - ray[1]};
+      double rcm2 = xcm[0] * xcm[0] + xcm[1] * xcm[1];
+      (void)exp(-rcm2 * t->inv_screen2); /* screening: unused by force_halo without subtract_point */
+      halo_force_one(t->halos[k], xcm, alpha, kappa, gamma, phi);
+      double mass = t->halos[k]->mass;
+      double prefac = mass * t->inv_area;
+      alpha[0] += prefac * xcm[0];
+      alpha[1] += prefac * xcm[1];
+      *phi += -t->inv_area * rcm2 * mass * 0.5;
+      *kappa -= mass * t->inv_area;
+    }
+    if (b->child[0]) {
+      double xc[2] = {b->center[0] - ray[0], b->center[1] - ray[1]};
+      double rcm2cell = xc[0] * xc[0] + xc[1] * xc[1];
+      if (rcm2cell > b->r2crit) {
+        descend = 0;
+        double screening = exp(-rcm2cell * t->inv_screen2);
+        double tmp = b->mass * (t->inv_area - screening / rcm2cell / ORC_PI);
+        alpha[0] += tmp * xc[0];
+        alpha[1] += tmp * xc[1];
+        tmp = -2.0 * b->mass / ORC_PI / rcm2cell / rcm2cell * screening;
+        gamma[0] += 0.5 * (xc[0] * xc[0] - xc[1] * xc[1]) * tmp;
+        gamma[1] += xc[0] * xc[1] * tmp;
+        *phi += 0.5 * b->mass * log(rcm2cell) / ORC_PI * screening;
+        *phi -= 0.5 * (b->quad[0] * xc[0] * xc[0] + b->quad[1] * xc[1] * xc[1] + 2 * b->quad[2] * xc[0] * xc[1]) /
+                (ORC_PI * rcm2cell * rcm2cell) * screening;
+        alpha[0] -= (b->quad[0] * xc[0] + b->quad[2] * xc[1]) / (rcm2cell * rcm2cell) / ORC_PI * screening;
+        alpha[1] -= (b->quad[1] * xc[1] + b->quad[2] * xc[0]) / (rcm2cell * rcm2cell) / ORC_PI * screening;
+        tmp = 4 * (b->quad[0] * xc[0] * xc[0] + b->quad[1] * xc[1] * xc[1] + 2 * b->quad[2] * xc[0] * xc[1]) /
+              (rcm2cell * rcm2cell * rcm2cell) / ORC_PI * screening;
+        alpha[0] += tmp * xc[0];
+        alpha[1] += tmp * xc[1];
+        *kappa -= b->mass * t->inv_area;
+        *phi -= b->mass * t->inv_area * rcm2cell;
+      }
+    }
+    /* QBiterator::TreeWalkStep, include/qTreeNB.h:541-552 */
+    b = (descend && b->child[0]) ? b->child[0] : b->brother;
+  }
+}
+
+/* TreeQuadHalos::force2D, include/quadTreeHalos.h:556-592. */
+static void halotree_force2D(const orc_halotree *t, const double *ray, double *alpha, double *kappa,
+                             double *gamma, double *phi) {
+  alpha[0] = alpha[1] = gamma[0] = gamma[1] = gamma[2] = 0.0;
+  *kappa = *phi = 0.0;
+  if (t->n == 0) return;
+  if (t->periodic) {
+    for (int i = -1; i < 2; ++i)
+      for (int j = -1; j < 2; ++j) {
+        double r[2] = {ray[0] + i * t->original_xl, ray[1] + j * t->original_yl};
+        hwalk(t, r, alpha, kappa, gamma, phi);
+      }
+  } else {
+    hwalk(t, ray, alpha, kappa, gamma, phi);
+  }
+}
+
 /* ============================ Lens ===================================== */
 typedef struct {
   double z;
@@ -892,6 +1202,9 @@ struct orc_lens {
   int nmain;          /* main planes, kept sorted by main_Dl */
   orc_plane *main;
   double *main_Dl;
+  int nfield;         /* field planes (LensPlaneTree), in insertion order */
+  orc_plane *field;
+  double *field_Dl;
   int nhalos;
   orc_halo **owned;   /* every halo the lens holds */
   /* combined planes (combinePlanes) */
@@ -903,23 +1216,37 @@ struct orc_lens {
   double zs_implant;
 };
 
-/* Lens::combinePlanes, MultiPlane/lens.cpp:2397-2515 (no field planes). */
+/* Lens::combinePlanes, MultiPlane/lens.cpp:2397-2515: field and main planes
+ * sorted together by Dl (Utilities::sort_indexes), distances closer than
+ * MIN_PLANE_DIST pushed apart, the source pseudo-plane appended. */
 static void combine_planes(orc_lens *l) {
-  int n = l->nmain;
+  int n = l->nmain + l->nfield;
   free(l->planes); free(l->plane_z); free(l->Dl); free(l->dDl);
   l->np = n;
   l->planes = (orc_plane **)malloc((n + 1) * sizeof(orc_plane *));
   l->plane_z = (double *)malloc((n + 1) * sizeof(double));
   l->Dl = (double *)malloc((n + 1) * sizeof(double));
   l->dDl = (double *)malloc((n + 1) * sizeof(double));
-  /* main planes are already sorted by Dl; a stable index sort is the identity */
-  for (int i = 0; i < n; ++i) l->Dl[i] = l->main_Dl[i];
+  int *index = (int *)malloc((n + 1) * sizeof(int));
+  double *all = (double *)malloc((n + 1) * sizeof(double));
+  for (int i = 0; i < l->nfield; ++i) all[i] = l->field_Dl[i];
+  for (int i = 0; i < l->nmain; ++i) all[l->nfield + i] = l->main_Dl[i];
+  for (int i = 0; i < n; ++i) index[i] = i;
+  for (int i = 1; i < n; ++i) { /* stable insertion sort of the indexes by Dl */
+    int k = index[i], j = i - 1;
+    while (j >= 0 && all[index[j]] > all[k]) { index[j + 1] = index[j]; --j; }
+    index[j + 1] = k;
+  }
+  for (int i = 0; i < n; ++i) l->Dl[i] = all[index[i]];
   for (int i = 1; i < n; ++i)
     if ((l->Dl[i] - l->Dl[i - 1]) < ORC_MIN_PLANE_DIST) l->Dl[i] = l->Dl[i - 1] + ORC_MIN_PLANE_DIST;
   for (int i = 0; i < n; ++i) {
-    l->planes[i] = &l->main[i];
-    l->plane_z[i] = l->main[i].z;
+    int k = index[i];
+    l->planes[i] = k < l->nfield ? &l->field[k] : &l->main[k - l->nfield];
+    l->plane_z[i] = l->planes[i]->z;
   }
+  free(index);
+  free(all);
   if (n > 0 && l->zsource <= l->plane_z[n - 1]) l->zsource = l->plane_z[n - 1] + 0.1;
   l->plane_z[n] = l->zsource;
   l->Dl[n] = orc_coordist2(0, l->zsource);
@@ -939,7 +1266,8 @@ void orc_lens_free(orc_lens *l) {
   if (!l) return;
   for (int i = 0; i < l->nhalos; ++i) orc_halo_free(l->owned[i]);
   for (int i = 0; i < l->nmain; ++i) free(l->main[i].halos);
-  free(l->owned); free(l->main); free(l->main_Dl);
+  for (int i = 0; i < l->nfield; ++i) free(l->field[i].halos);
+  free(l->owned); free(l->main); free(l->main_Dl); free(l->field); free(l->field_Dl);
   free(l->planes); free(l->plane_z); free(l->Dl); free(l->dDl);
   free(l);
 }
@@ -1001,6 +1329,22 @@ void orc_lens_add_halo(orc_lens *l, orc_halo *h, int addplanes) {
   combine_planes(l);
 }
 
+/* A LensPlaneTree as one of the lens's field planes (Lens::createFieldPlanes,
+ * MultiPlane/lens.cpp:443-452; field_Dl = coorDist(z)); the lens takes
+ * ownership of the plane. */
+void orc_lens_add_field_plane(orc_lens *l, orc_halo *plane) {
+  l->owned = (orc_halo **)realloc(l->owned, (l->nhalos + 1) * sizeof(orc_halo *));
+  l->owned[l->nhalos++] = plane;
+  l->field = (orc_plane *)realloc(l->field, (l->nfield + 1) * sizeof(orc_plane));
+  l->field_Dl = (double *)realloc(l->field_Dl, (l->nfield + 1) * sizeof(double));
+  memset(&l->field[l->nfield], 0, sizeof(orc_plane));
+  l->field[l->nfield].z = plane->zlens;
+  l->field_Dl[l->nfield] = orc_coordist2(0, plane->zlens);
+  plane_push(&l->field[l->nfield], plane);
+  l->nfield++;
+  combine_planes(l);
+}
+
 int orc_lens_nplanes(const orc_lens *l) { return l->np; }
 void orc_lens_planes(const orc_lens *l, double *z, double *Dl, double *dDl) {
   for (int i = 0; i <= l->np; ++i) {
@@ -1059,8 +1403,13 @@ static void plane_force(orc_plane *p, const double *xx, double *alpha, double *k
     xt[0] = xx[0] - h->posHalo[0] * h->Dist; /* LensHalo::getX, lens_halos.h:95-99 */
     xt[1] = xx[1] - h->posHalo[1] * h->Dist;
     halo_force_one(h, xt, at, &kt, gt, &pt);
-    alpha[0] -= at[0];
-    alpha[1] -= at[1];
+    if (h->kind == ORC_FIELD) { /* LensPlaneTree::force: the tree's alpha as it is */
+      alpha[0] += at[0];
+      alpha[1] += at[1];
+    } else {
+      alpha[0] -= at[0];
+      alpha[1] -= at[1];
+    }
     *kappa += kt;
     gamma[0] += gt[0];
     gamma[1] += gt[1];

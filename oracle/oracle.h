@@ -88,6 +88,17 @@ float orc_halo_rmax(const orc_halo *h);
 void orc_halo_force(orc_halo *h, size_t n, const double *xcm, double *alpha,
                     double *kappa, double *gamma, double *phi);
 
+/* LensPlaneTree(z, halos, n, sigma_background, inv_screening_scale)
+ * (MultiPlane/planes.cpp:13-18) over NFW / NSIE haloes: a TreeQuadHalos
+ * (include/quadTreeHalos.h) as a halo of its own whose force is
+ * TreeQuadHalos::force2D (overwrites its outputs).  Takes ownership of the
+ * haloes and moves them to redshift z.  Returns NULL with *err = 1 when the
+ * haloes' positions span no area ("particles in same place."; the caller
+ * keeps its haloes then). */
+orc_halo *orc_halo_field_plane(orc_halo **halos, int n, double z,
+                               double sigma_back, double inv_screening,
+                               int *err);
+
 /* ---------------- Lens (MultiPlane/lens.cpp, include/lens.h) ---------- */
 typedef struct orc_lens orc_lens;
 orc_lens *orc_lens_create(double zsource);
@@ -95,6 +106,9 @@ void orc_lens_free(orc_lens *l);
 /* Lens::insertMainHalo / moveinMainHalo with addplanes (lens.h:149-185):
  * the lens takes ownership of h. */
 void orc_lens_add_halo(orc_lens *l, orc_halo *h, int addplanes);
+/* A field plane (orc_halo_field_plane) among the lens planes, as
+ * Lens::createFieldPlanes adds a LensPlaneTree; the lens takes ownership. */
+void orc_lens_add_field_plane(orc_lens *l, orc_halo *plane);
 int orc_lens_nplanes(const orc_lens *l);
 /* plane_redshifts, Dl, dDl (each nplanes+1 long, source pseudo-plane last) */
 void orc_lens_planes(const orc_lens *l, double *z, double *Dl, double *dDl);

@@ -25,6 +25,13 @@
  *                                                    TIMEFILE gets the ctor wall seconds
  *   rays XFILE N ZFILE OUT TIMEFILE                  rayshooterInternal(N, RAY*) with per-ray z
  *   points XFILE N OUT TIMEFILE                      rayshooterInternal(N, Point*)
+ *   fieldplane HFILE NH Z SIGMA_BACK INV_SCREEN XFILE N OUT
+ *        LensPlaneTree(Z, haloes, NH, SIGMA_BACK, INV_SCREEN)::force at N plane
+ *        positions -> per position alpha[2] kappa gamma[3] phi.  HFILE: 8
+ *        doubles per halo {kind, mass, a, b, c, d, tx, ty}: kind 0 = LensHaloNFW
+ *        (a = Rsize, b = concentration), 1 = LensHaloRealNSIE (a = sigma,
+ *        b = rcore, c = fratio, d = pa); each halo moved to Z with
+ *        setZlensDist, as Lens::createFieldPlanes does.
  */
 #include "slsimlib.h"
 #include "particle_halo.h"
@@ -264,6 +271,39 @@ int main() {
       }
       write_arr(out, o);
       write_time(tf, secs);
+    } else if (cmd == "fieldplane") {
+      std::string hf, xf, out;
+      size_t nh, n;
+      double z, sb, iscr;
+      in >> hf >> nh >> z >> sb >> iscr >> xf >> n >> out;
+      std::vector<double> hd = read_arr<double>(hf, 8 * nh);
+      std::vector<std::unique_ptr<LensHalo>> hs;
+      std::vector<LensHalo *> hp;
+      for (size_t i = 0; i < nh; ++i) {
+        const double *d = &hd[8 * i];
+        LensHalo *h;
+        if (d[0] == 0) {
+          h = new LensHaloNFW((float)d[1], (float)d[2], z, (float)d[3], 1.0f, 0.0f, cosmo);
+        } else {
+          LensHaloRealNSIE *nh2 = new LensHaloRealNSIE((float)d[1], z, (float)d[2], (float)d[3], (float)d[4],
+                                                       (float)d[5], cosmo);
+          fix_cored_nsie_mass(*nh2, (float)d[1]);
+          h = nh2;
+        }
+        h->setTheta(d[6], d[7]);
+        h->setZlensDist(z, cosmo);
+        hs.emplace_back(h);
+        hp.push_back(h);
+      }
+      LensPlaneTree plane((float)z, hp.data(), nh, sb, iscr);
+      std::vector<double> x = read_arr<double>(xf, 2 * n), o(7 * n);
+      for (size_t k = 0; k < n; ++k) {
+        double a[2] = {0, 0}, kk = 0, g[3] = {0, 0, 0}, ph = 0;
+        plane.force(a, &kk, g, &ph, &x[2 * k]);
+        double v[7] = {a[0], a[1], kk, g[0], g[1], g[2], ph};
+        std::copy(v, v + 7, &o[7 * k]);
+      }
+      write_arr(out, o);
     } else {
       fprintf(stderr, "glamer_ref: unknown command %s\n", cmd.c_str());
       return 2;

@@ -145,6 +145,19 @@ class NFWHalo:
 
 
 @dataclasses.dataclass
+class FieldPlane:
+    """A plane of field haloes (LensPlaneTree, MultiPlane/planes.cpp:13-18):
+    NFW / NSIE haloes at angular positions ``theta`` (their own redshifts are
+    replaced by the plane's), the background density ``sigma_back`` and the
+    screening scale ``inv_screening`` (0: none)."""
+
+    z: float
+    halos: List[object]
+    sigma_back: float = 0.0
+    inv_screening: float = 0.0
+
+
+@dataclasses.dataclass
 class LensSpec:
     """Haloes in insertion order (Lens::moveinMainHalo / insertMainHalo with
     addplanes = true) and the source redshift."""
@@ -209,3 +222,23 @@ def grid_positions(n1d: int, center=(0.0, 0.0), range_rad: float = 30 * ARCSEC) 
     x = center[0] + range_rad * (1.0 * (i % n1d) / (n1d - 1) - 0.5)
     y = center[1] + range_rad * (1.0 * (i // n1d) / (n1d - 1) - 0.5)
     return np.stack([x, y], axis=1)
+
+
+def field_halos(seed: int, n: int, z: float, field_arcsec: float = 60.0, mmin: float = 1e11,
+                mmax: float = 1e14, n_nsie: int = 0, cosmo: "Cosmology" = None) -> List[object]:
+    """n NFW haloes (mass log-uniform in [mmin, mmax], c = 5 (M/1e14)^-0.1,
+    truncated at r200) uniform in a square field, plus n_nsie NSIE haloes
+    (sigma 150-250 km/s, q 0.6-0.9): the field haloes of one plane."""
+    rng = np.random.default_rng(seed)
+    cosmo = cosmo or Cosmology()
+    out = []
+    half = 0.5 * field_arcsec * ARCSEC
+    for m in 10 ** rng.uniform(np.log10(mmin), np.log10(mmax), n):
+        th = tuple(float(v) for v in rng.uniform(-half, half, 2))
+        out.append(NFWHalo(float(m), float(cosmo.r200(m, z)), z, float(5.0 * (m / 1e14) ** -0.1), theta=th))
+    for _ in range(n_nsie):
+        th = tuple(float(v) for v in rng.uniform(-half, half, 2))
+        sig = float(rng.uniform(150, 250))
+        out.append(NSIEHalo(float(10 ** rng.uniform(12, 13)), z, sig, float(rng.uniform(5e-5, 2e-4)),
+                            float(rng.uniform(0.6, 0.9)), float(rng.uniform(0, np.pi)), theta=th))
+    return out

@@ -77,6 +77,47 @@ def lens_fixture():
     np.savez_compressed(os.path.join(OUT, "lens_small.npz"), **arrays)
 
 
+FIELD_CASES = ((0.0, 0.0), (1e12, 0.0), (0.0, 2.0), (5e11, 1.0))  # (sigma_back, inv_screening)
+
+
+def field_rows(halos):
+    """8 doubles per field halo, as the reference driver's fieldplane command reads them."""
+    rows = []
+    for h in halos:
+        if isinstance(h, synth.NFWHalo):
+            rows.append([0, h.mass, h.rsize, h.conc, 0, 0, h.theta[0], h.theta[1]])
+        else:
+            rows.append([1, h.mass, h.sigma, h.rcore, h.fratio, h.pa, h.theta[0], h.theta[1]])
+    return np.asarray(rows, dtype=np.float64)
+
+
+def field_halos_from_rows(rows, z):
+    out = []
+    for r in rows:
+        if r[0] == 0:
+            out.append(synth.NFWHalo(r[1], r[2], z, r[3], theta=(r[6], r[7])))
+        else:
+            out.append(synth.NSIEHalo(r[1], z, r[2], r[3], r[4], r[5], theta=(r[6], r[7])))
+    return out
+
+
+def field_fixture():
+    """LensPlaneTree::force of two field planes (NFW only; NFW + NSIE) for the
+    four (sigma_back, inv_screening) cases at 300 plane positions."""
+    z = 0.4
+    cos = synth.Cosmology()
+    half = 30 * synth.ARCSEC * cos.angdist(z)
+    xx = np.random.default_rng(15).uniform(-half, half, (300, 2))
+    R = H.RefDriver()
+    arrays = {"z": z, "xx": xx, "cases": np.asarray(FIELD_CASES)}
+    for name, halos in (("nfw", synth.field_halos(16, 300, z)),
+                        ("mixed", synth.field_halos(17, 150, z, n_nsie=12))):
+        arrays[name + "_rows"] = field_rows(halos)
+        for c, (sb, iscr) in enumerate(FIELD_CASES):
+            arrays[f"{name}_{c}"] = R.field_plane(synth.FieldPlane(z, halos, sb, iscr), xx)
+    np.savez_compressed(os.path.join(OUT, "field_plane.npz"), **arrays)
+
+
 def lens_spec_from_fixture(d) -> synth.LensSpec:
     """Rebuilds the LensSpec of lens_small.npz (insertion order as generated)."""
     halos = []
@@ -97,4 +138,5 @@ if __name__ == "__main__":
     tree_fixture()
     halo_fixture()
     lens_fixture()
+    field_fixture()
     print("golden fixtures written to", OUT)

@@ -74,6 +74,9 @@ def oracle_lib():
     L.orc_lens_rayshoot.argtypes = [_vp, C.c_size_t, _vp, _vp, _vp, _vp, C.c_int]
     L.orc_lens_plane_force.argtypes = [_vp, C.c_int, C.c_size_t, _vp, _vp, _vp, _vp, _vp]
     L.orc_grid_positions.argtypes = [C.c_size_t, _vp, C.c_double, _vp]
+    L.orc_halo_field_plane.restype = _vp
+    L.orc_halo_field_plane.argtypes = [_vp, C.c_int, C.c_double, C.c_double, C.c_double, C.POINTER(C.c_int)]
+    L.orc_lens_add_field_plane.argtypes = [_vp, _vp]
     _lib = L
     return L
 
@@ -146,6 +149,13 @@ def _make_halo(h):
         ptr = L.orc_halo_nsie(h.mass, h.z, h.sigma, h.rcore, h.fratio, h.pa)
     elif isinstance(h, synth.NFWHalo):
         ptr = L.orc_halo_nfw(h.mass, h.rsize, h.z, h.conc, 1.0, 0.0)
+    elif isinstance(h, synth.FieldPlane):
+        members = (_vp * max(1, len(h.halos)))(*[_make_halo(m) for m in h.halos])
+        err = C.c_int(0)
+        ptr = L.orc_halo_field_plane(members, len(h.halos), h.z, h.sigma_back, h.inv_screening, C.byref(err))
+        if err.value:
+            raise ValueError("particles in same place.")
+        return ptr
     else:
         raise TypeError(h)
     L.orc_halo_set_theta(ptr, h.theta[0], h.theta[1])
@@ -170,7 +180,10 @@ class OracleLens:
         L = oracle_lib()
         self.h = L.orc_lens_create(spec.zsource)
         for halo in spec.halos:
-            L.orc_lens_add_halo(self.h, _make_halo(halo), 1)
+            if isinstance(halo, synth.FieldPlane):
+                L.orc_lens_add_field_plane(self.h, _make_halo(halo))
+            else:
+                L.orc_lens_add_halo(self.h, _make_halo(halo), 1)
 
     def planes(self):
         L = oracle_lib()
@@ -263,6 +276,21 @@ class RefDriver:
         self.run([cmd])
         o = np.fromfile(of)
         return o[:-3].reshape(-1, 7), tuple(o[-3:])
+
+    def field_plane(self, fp: "synth.FieldPlane", xx):
+        """LensPlaneTree::force of a field plane at plane positions xx -> (n, 7)."""
+        rows = []
+        for h in fp.halos:
+            if isinstance(h, synth.NFWHalo):
+                rows.append([0, h.mass, h.rsize, h.conc, 0, 0, h.theta[0], h.theta[1]])
+            else:
+                rows.append([1, h.mass, h.sigma, h.rcore, h.fratio, h.pa, h.theta[0], h.theta[1]])
+        hf = self._file(np.asarray(rows, dtype=np.float64))
+        xx = np.ascontiguousarray(xx, dtype=np.float64).reshape(-1, 2)
+        xf = self._file(xx)
+        of = self._file()
+        self.run([f"fieldplane {hf} {len(rows)} {fp.z!r} {fp.sigma_back!r} {fp.inv_screening!r} {xf} {len(xx)} {of}"])
+        return np.fromfile(of).reshape(-1, 7)
 
     def lens_lines(self, spec: synth.LensSpec):
         lines = [f"lens {spec.zsource!r}"]
