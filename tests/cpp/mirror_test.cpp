@@ -126,7 +126,9 @@ int main(int argc, char **argv) {
     }
     REQUIRE(threw);
   }
-  REQUIRE(lens.getNplanes() == 3);  // NSIE merged into the z = 0.3 plane
+  // particle haloes keep their redshift as a float (0.3f), which puts the
+  // NSIE at z = 0.3 on a plane of its own: 0.3f, 0.3, 0.45, 0.6
+  REQUIRE(lens.getNplanes() == 4);
   REQUIRE(std::fabs(lens.getSourceZ() - zsrc) < 1e-12);
 
   // GridMap, copy- and move-built lenses agree bit for bit
