@@ -55,16 +55,7 @@ def workload(small: bool):
 
 def make_lens(spec):
     import slsimlib_b200 as glb
-    from slsimlib_b200 import synth
-    lens = glb.Lens(spec.zsource)
-    for h in spec.halos:
-        if isinstance(h, synth.ParticlePlane):
-            lens.insertMainHalo(glb.LensHaloParticles(h.particles, h.z, h.inv_area, h.max_range), True)
-        elif isinstance(h, synth.NSIEHalo):
-            lens.insertMainHalo(glb.LensHaloRealNSIE(h.mass, h.z, h.sigma, h.rcore, h.fratio, h.pa), True)
-        else:
-            lens.insertMainHalo(glb.LensHaloNFW(h.mass, h.rsize, h.z, h.conc), True)
-    return lens
+    return glb.lens_from_spec(spec)
 
 
 class ClockSampler:

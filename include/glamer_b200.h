@@ -125,6 +125,20 @@ int glb_halo_set_theta(glb_halo *h, double tx, double ty);
  * glb_tree_force2D_recur; analytic halos start from zero. */
 int glb_halo_force(glb_halo *h, size_t n, const double *xcm, double *alpha, double *kappa,
                    double *gamma, double *phi);
+/* LensPlaneTree(z, halos, n, sigma_background, inv_screening_scale)
+ * (MultiPlane/planes.cpp:13-18): a plane of field haloes whose force is
+ * TreeQuadHalos::force2D (include/quadTreeHalos.h:556-815) -- every halo of a
+ * visited branch evaluated in full, distant cells as monopole + quadrupole,
+ * the sigma_background sheet -- with the reference's tree (bucket 5, opening
+ * angle 0.5; with screening: opening angle 0.1, periodic buffer).  The members
+ * must be NFW or NSIE haloes (GLB_ERR_UNSUPPORTED otherwise); the plane takes
+ * ownership of them (on failure the caller keeps them) and moves them to
+ * redshift z (LensHalo::setZlensDist, as Lens::createFieldPlanes does,
+ * MultiPlane/lens.cpp:418-426).  glb_halo_force on the result gives
+ * LensPlaneTree::force at plane positions (outputs overwritten, alpha as the
+ * tree gives it).  Positions spanning no area: GLB_ERR_SAME_PLACE. */
+int glb_halo_field_plane(glb_halo *const *halos, int n, double z, double sigma_background,
+                         double inv_screening_scale, glb_halo **out);
 /* mass, Rsize, Rmax (float members of LensHalo) */
 int glb_halo_params(glb_halo *h, float *mass, float *rsize, float *rmax);
 int glb_halo_destroy(glb_halo *h);
@@ -139,6 +153,12 @@ int glb_lens_destroy(glb_lens *l);
  * takes ownership of h.  addplanes selects addMainHaloToPlane (1) or
  * addMainHaloToNearestPlane (0). */
 int glb_lens_insert_halo(glb_lens *l, glb_halo *h, int addplanes);
+/* A field plane (glb_halo_field_plane) among the lens planes, as
+ * Lens::createFieldPlanes adds each LensPlaneTree (MultiPlane/lens.cpp:443-452)
+ * and Lens::combinePlanes sorts field and main planes together by distance
+ * (lens.cpp:2397-2515).  The lens takes ownership of the plane; its tree is
+ * rebuilt for the lens's cosmology. */
+int glb_lens_insert_field_plane(glb_lens *l, glb_halo *plane);
 /* Lens::getNplanes and the plane_redshifts / Dl / dDl arrays (nplanes + 1
  * entries each, source pseudo-plane last; any pointer may be NULL). */
 int glb_lens_nplanes(glb_lens *l, int *nplanes);

@@ -54,8 +54,9 @@ EXPORTED = [
     "glb_tree_create", "glb_tree_destroy", "glb_tree_force2D_recur", "glb_tree_force_device", "glb_tree_export",
     "glb_tree_build_ms", "glb_direct_sum_device",
     "glb_halo_particles", "glb_halo_nfw", "glb_halo_nsie", "glb_halo_set_theta", "glb_halo_force",
-    "glb_halo_params", "glb_halo_destroy",
-    "glb_lens_create", "glb_lens_destroy", "glb_lens_insert_halo", "glb_lens_nplanes", "glb_lens_planes",
+    "glb_halo_params", "glb_halo_destroy", "glb_halo_field_plane",
+    "glb_lens_create", "glb_lens_destroy", "glb_lens_insert_halo", "glb_lens_insert_field_plane",
+    "glb_lens_nplanes", "glb_lens_planes",
     "glb_lens_reset_source", "glb_lens_rayshoot", "glb_lens_rayshoot_device", "glb_gridmap",
     "glb_lens_last_timing", "glb_lens_count_interactions", "glb_lens_rayshoot_noalloc",
     "glb_batch_create_grids", "glb_batch_run", "glb_batch_autotune", "glb_batch_set_block", "glb_batch_info",
@@ -103,6 +104,8 @@ def load_library():
     L.glb_halo_force.argtypes = [_vp, C.c_size_t, _vp, _vp, _vp, _vp, _vp]
     L.glb_halo_params.argtypes = [_vp, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)]
     L.glb_halo_destroy.argtypes = [_vp]
+    L.glb_halo_field_plane.argtypes = [_vp, C.c_int, C.c_double, C.c_double, C.c_double, C.POINTER(_vp)]
+    L.glb_lens_insert_field_plane.argtypes = [_vp, _vp]
     L.glb_lens_create.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, C.POINTER(_vp)]
     L.glb_lens_destroy.argtypes = [_vp]
     L.glb_lens_insert_halo.argtypes = [_vp, _vp, C.c_int]
@@ -296,6 +299,37 @@ class LensHaloRealNSIE(_Halo):
         return h
 
 
+class LensPlaneTree(_Halo):
+    """LensPlaneTree(z, halos, n, sigma_background, inv_screening_scale)
+    (MultiPlane/planes.cpp:13-18): a plane of NFW / NSIE field haloes walked
+    as TreeQuadHalos (include/quadTreeHalos.h).  force_halo gives
+    LensPlaneTree::force at plane positions; Lens.insertFieldPlane adds the
+    plane to a lens as Lens::createFieldPlanes does."""
+
+    def __init__(self, z, halos, sigma_background=0.0, inv_screening_scale=0.0):
+        self.z = float(z)
+        self.halos = list(halos)
+        self.sigma_background = float(sigma_background)
+        self.inv_screening_scale = float(inv_screening_scale)
+
+    def _create(self):
+        L = load_library()
+        members = [m._make() for m in self.halos]
+        arr = (_vp * max(1, len(members)))(*members)
+        h = _vp()
+        rc = L.glb_halo_field_plane(arr, len(members), self.z, self.sigma_background, self.inv_screening_scale,
+                                    C.byref(h))
+        if rc != 0:
+            msg = L.glb_last_error().decode()
+            for m in members:
+                L.glb_halo_destroy(m)
+            raise GlamerError(rc, msg)
+        return h
+
+    def _make(self):  # a field plane has no position of its own
+        return self._create()
+
+
 # -------------------------------------------------------------------- lens
 class Lens:
     """Lens(long *seed, z_source, COSMOLOGY) (MultiPlane/lens.cpp:59-77) for a
@@ -312,6 +346,11 @@ class Lens:
         _check(load_library().glb_lens_insert_halo(self._h, halo._make(), int(addplanes)))
 
     moveinMainHalo = insertMainHalo
+
+    def insertFieldPlane(self, plane: LensPlaneTree):
+        """A LensPlaneTree among the lens planes (Lens::createFieldPlanes,
+        MultiPlane/lens.cpp:443-452; combinePlanes sorts all planes by distance)."""
+        _check(load_library().glb_lens_insert_field_plane(self._h, plane._make()))
 
     def getNplanes(self) -> int:
         n = C.c_int(0)
@@ -513,3 +552,34 @@ class Server:
 
     def __del__(self):
         self.close()
+
+
+def halo_from_spec(h):
+    """The library halo for a halo description of slsimlib_b200.synth
+    (ParticlePlane, NFWHalo, NSIEHalo, FieldPlane)."""
+    from slsimlib_b200 import synth
+    if isinstance(h, synth.ParticlePlane):
+        out = LensHaloParticles(h.particles, h.z, h.inv_area, h.max_range)
+    elif isinstance(h, synth.NSIEHalo):
+        out = LensHaloRealNSIE(h.mass, h.z, h.sigma, h.rcore, h.fratio, h.pa)
+    elif isinstance(h, synth.NFWHalo):
+        out = LensHaloNFW(h.mass, h.rsize, h.z, h.conc)
+    elif isinstance(h, synth.FieldPlane):
+        return LensPlaneTree(h.z, [halo_from_spec(m) for m in h.halos], h.sigma_back, h.inv_screening)
+    else:
+        raise TypeError(h)
+    out.setTheta(*h.theta)
+    return out
+
+
+def lens_from_spec(spec) -> Lens:
+    """A Lens holding the haloes of a synth.LensSpec in insertion order (field
+    planes through insertFieldPlane, the rest through insertMainHalo)."""
+    lens = Lens(spec.zsource)
+    for h in spec.halos:
+        g = halo_from_spec(h)
+        if isinstance(g, LensPlaneTree):
+            lens.insertFieldPlane(g)
+        else:
+            lens.insertMainHalo(g, True)
+    return lens

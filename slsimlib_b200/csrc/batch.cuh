@@ -58,6 +58,13 @@ __device__ __forceinline__ void plane_force(const PlaneDev &P, const HaloDev *ha
       particle_halo_acc<PREC, false>(H->tree, xc0, xc1, valid, acc);
       acc[0] = -acc[0];
       acc[1] = -acc[1];
+    } else if (H->kind == HALO_FIELD) {
+      const Force6 f = field_plane_force<false>(&H->htree, tab, xc0, xc1, valid);
+      acc[0] = -f.a0;
+      acc[1] = -f.a1;
+      acc[2] = f.k;
+      acc[3] = f.g0;
+      acc[4] = f.g1;
     } else if (valid) {
       const Force5 f = analytic_halo(H, tab, xc0, xc1);
       acc[0] = f.a0;
@@ -164,7 +171,7 @@ __global__ void __launch_bounds__(256, 3) k_batch(const Chunk *chunks, int nchun
 // Descriptor of a lens for k_batch; the lens's device tables must be current.
 int make_lens_dev(glb_lens *l, LensDev &d) {
   if (int rc = upload_lens(l)) return rc;
-  size_t np = l->main.size();
+  size_t np = l->planes.size();
   d.planes = l->d_planes.p;
   d.halos = l->d_halos.p;
   d.planez = l->d_planez.p;

@@ -83,6 +83,18 @@ struct TreeParams {
 Status build_tree(const glb_particle_rec *host_particles, size_t n, const TreeParams &prm,
                   bool want_export, cudaStream_t stream, std::unique_ptr<Tree> &out);
 
+// TreeQuadHalos (include/quadTreeHalos.h:129-515) built on the host: branch
+// arrays in preorder, ready for upload.  xp: 2n halo positions (physical
+// Mpc), rmax / mass: the haloes' float members.  Returns false with `err` set
+// when the positions span no area ("particles in same place.").
+struct HaloTreeHost {
+  std::vector<HNode> nodes;
+  std::vector<int> bigs;
+  double period_x = 0, period_y = 0;
+};
+bool build_halo_tree(const std::vector<double> &xp, const std::vector<float> &rmax, const std::vector<float> &mass,
+                     int bucket, double theta, double max_range, HaloTreeHost &out, std::string &err);
+
 // Global options.
 extern int g_keep_tree_export;
 

@@ -75,7 +75,7 @@ struct TreeDev {
   double root_mass, root_cx, root_cy;
 };
 
-enum HaloKind { HALO_PARTICLES = 0, HALO_NFW = 1, HALO_NSIE = 2 };
+enum HaloKind { HALO_PARTICLES = 0, HALO_NFW = 1, HALO_NSIE = 2, HALO_FIELD = 3 };
 
 struct NFWDev {
   double mass, rscale, gmax, Rmax2;  // Rmax2: float(Rmax*Rmax) as the reference compares
@@ -94,12 +94,47 @@ struct NSIEDev {
   double dRmaxRsize;  // float(Rmax - Rsize)
 };
 
+// One branch of a field plane's halo tree (TreeQuadHalos, include/quadTreeHalos.h),
+// preorder with empty children kept (they carry no haloes and no far field).
+struct HNode {
+  double cx, cy;      // mass-weighted centre of the branch's haloes (CalcMoments)
+  double r2crit;      // (1.15470 rcom / theta)^2: the cell is used whole beyond it
+  double mass;
+  double q0, q1, q2;  // quadrupole about the centre
+  int skip;           // first branch after this subtree
+  int leaf;
+  int bstart, bcount; // big haloes of the branch (a leaf: all of its haloes)
+};
+
+// A member halo of a field plane: its position on the plane and profile.
+struct FieldHaloDev {
+  int kind;          // HALO_NFW or HALO_NSIE
+  double px, py;     // LensHalo::getX at the plane's redshift
+  double mass;       // LensHalo::get_mass (a float member)
+  NFWDev nfw;
+  NSIEDev nsie;
+};
+
+// LensPlaneTree's TreeQuadHalos on the device.
+struct HaloTreeDev {
+  const HNode *nodes;
+  const int *bigs;             // member indices, in the reference's list order
+  const FieldHaloDev *halos;
+  int nnodes;
+  int nhalos;
+  double inv_area;             // the plane's sigma_background
+  double screen2;              // inv_screening_scale^2
+  int periodic;
+  double period_x, period_y;   // original (unsquared) bbox lengths
+};
+
 struct HaloDev {
   int kind;
   double px, py;  // posHalo * Dist (physical Mpc), LensHalo::getX
   TreeDev tree;
   NFWDev nfw;
   NSIEDev nsie;
+  HaloTreeDev htree;
 };
 
 // One lens plane of the combined list, with the scalars of the recursion

@@ -23,6 +23,7 @@
 #include "halos.cuh"
 #include "walk.cuh"
 #include "walk_split.cuh"
+#include "walk_halos.cuh"
 
 using namespace glb;
 
@@ -134,8 +135,22 @@ struct glb_halo {
   NFWDev nfw{};
   NSIEDev nsie{};
   std::unique_ptr<Tree> tree;
+  std::unique_ptr<struct FieldTree> field;  // HALO_FIELD: a LensPlaneTree
   int device = 0;
   cudaStream_t stream = nullptr;
+};
+
+// LensPlaneTree (MultiPlane/planes.cpp:13-18): the member haloes (owned) and
+// their TreeQuadHalos on the device.
+struct FieldTree {
+  std::vector<std::unique_ptr<glb_halo>> members;
+  double sigma_back = 0, inv_screening = 0;
+  int bucket = 5, periodic = 0;
+  double theta = 0.5;
+  DBuf<HNode> nodes;
+  DBuf<int> bigs;
+  DBuf<FieldHaloDev> halos;
+  HaloTreeDev dev{};
 };
 
 // ====================================================================== lens
@@ -150,6 +165,8 @@ struct glb_lens {
   double charge = 0;
   std::vector<std::unique_ptr<glb_halo>> owned;
   std::vector<PlaneHost> main;  // sorted by Dl
+  std::vector<PlaneHost> field;  // LensPlaneTree planes, in insertion order
+  std::vector<PlaneHost *> planes;  // main and field planes in order of distance (combinePlanes)
   std::vector<double> plane_z, Dl, dDl;  // combined, source pseudo-plane last
   bool toggle_source_plane = false;
   double zs_implant = 0;
@@ -428,6 +445,14 @@ __device__ __forceinline__ void plane_step(const StepArgs &a) {
       // LensHaloParticles::force_halo negates alpha (particle_halo.h:432-433)
       acc[0] = -acc[0];
       acc[1] = -acc[1];
+    } else if (kind == HALO_FIELD) {
+      // LensPlaneTree::force is the tree's output as it is (planes.cpp:65-68)
+      const Force6 f = field_plane_force<false>(&H->htree, &a.tab, xc0, xc1, valid);
+      acc[0] = -f.a0;
+      acc[1] = -f.a1;
+      acc[2] = f.k;
+      acc[3] = f.g0;
+      acc[4] = f.g1;
     } else if (valid) {
       const Force5 f = analytic_halo(H, &a.tab, xc0, xc1);
       acc[0] = f.a0;
@@ -504,6 +529,8 @@ __global__ void __launch_bounds__(128) k_halo_force(HaloDev H, NFWTables tab, si
   double acc[6] = {0, 0, 0, 0, 0, 0};
   if (H.kind == HALO_PARTICLES) {
     particle_halo_acc<GLB_PREC_FP64, true>(H.tree, x0, x1, valid, acc);
+  } else if (H.kind == HALO_FIELD) {
+    field_plane_acc<true>(H.htree, tab, x0, x1, valid, acc);
   } else if (valid) {
     if (H.kind == HALO_NFW)
       nfw_force<true>(H.nfw, tab, x0, x1, acc);
@@ -597,6 +624,7 @@ HaloDev make_halo_dev(const glb_halo &h) {
   d.px = h.theta[0] * h.Dist;  // LensHalo::getX (include/lens_halos.h:95-99)
   d.py = h.theta[1] * h.Dist;
   if (h.tree) d.tree = h.tree->dev;
+  if (h.field) d.htree = h.field->dev;
   d.nfw = h.nfw;
   d.nsie = h.nsie;
   return d;
@@ -607,16 +635,29 @@ int set_dev(int device) {
   return 0;
 }
 
-// Lens::combinePlanes (MultiPlane/lens.cpp:2397-2515) without field planes.
+// Lens::combinePlanes (MultiPlane/lens.cpp:2397-2515): field and main planes
+// sorted together by Dl (field planes first among equal distances), planes
+// closer than MIN_PLANE_DIST pushed apart, the source pseudo-plane appended.
 void combine_planes(glb_lens *l) {
-  size_t n = l->main.size();
+  std::vector<std::pair<double, PlaneHost *>> all;
+  for (PlaneHost &p : l->field) all.emplace_back(p.Dl, &p);
+  for (PlaneHost &p : l->main) all.emplace_back(p.Dl, &p);
+  std::stable_sort(all.begin(), all.end(),
+                   [](const std::pair<double, PlaneHost *> &a, const std::pair<double, PlaneHost *> &b) {
+                     return a.first < b.first;
+                   });
+  size_t n = all.size();
+  l->planes.resize(n);
   l->plane_z.assign(n + 1, 0);
   l->Dl.assign(n + 1, 0);
   l->dDl.assign(n + 1, 0);
-  for (size_t i = 0; i < n; ++i) l->Dl[i] = l->main[i].Dl;
+  for (size_t i = 0; i < n; ++i) {
+    l->planes[i] = all[i].second;
+    l->Dl[i] = all[i].first;
+  }
   for (size_t i = 1; i < n; ++i)
     if ((l->Dl[i] - l->Dl[i - 1]) < 1e-6) l->Dl[i] = l->Dl[i - 1] + 1e-6;  // MIN_PLANE_DIST
-  for (size_t i = 0; i < n; ++i) l->plane_z[i] = l->main[i].z;
+  for (size_t i = 0; i < n; ++i) l->plane_z[i] = l->planes[i]->z;
   if (n > 0 && l->zsource <= l->plane_z[n - 1]) l->zsource = l->plane_z[n - 1] + 0.1;
   l->plane_z[n] = l->zsource;
   l->Dl[n] = coordist2(l->cosmo, 0, l->zsource);
@@ -627,7 +668,7 @@ void combine_planes(glb_lens *l) {
 
 int upload_lens(glb_lens *l) {
   if (!l->dirty) return 0;
-  size_t np = l->main.size();
+  size_t np = l->planes.size();
   std::vector<PlaneDev> P(np);
   std::vector<HaloDev> H;
   for (size_t j = 0; j < np; ++j) {
@@ -637,8 +678,8 @@ int upload_lens(glb_lens *l) {
     p.aa = l->dDl[j + 1] / l->Dl[j + 1];
     p.bb = l->Dl[j] / l->Dl[j + 1];
     p.halo0 = (int)H.size();
-    p.nhalo = (int)l->main[j].halos.size();
-    for (glb_halo *h : l->main[j].halos) H.push_back(make_halo_dev(*h));
+    p.nhalo = (int)l->planes[j]->halos.size();
+    for (glb_halo *h : l->planes[j]->halos) H.push_back(make_halo_dev(*h));
   }
   CKR(l->d_planes.alloc(std::max<size_t>(np, 1)));
   CKR(l->d_halos.alloc(std::max<size_t>(H.size(), 1)));
@@ -680,7 +721,7 @@ int ensure_ws(glb_lens *l, size_t n, bool per_ray) {
 int rayshoot_device(glb_lens *l, size_t n, const double *x, const double *zs, double *y, double *A,
                     int precision, cudaStream_t s, unsigned long long *d_counts = nullptr) {
   if (n == 0) return 0;
-  size_t np = l->main.size();
+  size_t np = l->planes.size();
   if (np == 0) {  // no lens plane (internal_rayshooter_multi.cpp:62-76)
     k_identity_rays<<<nblk(n, 256), 256, 0, s>>>(x, n, y, A);
     CKR(cudaGetLastError());
@@ -824,7 +865,7 @@ static int force_generic(const HaloDev &H, int device, cudaStream_t s, size_t n,
   if (!xcm) return fail(GLB_ERR_ARG, "null positions");
   if (int rc = set_dev(device)) return rc;
   NFWTables tab{};
-  if (H.kind == HALO_NFW)
+  if (H.kind == HALO_NFW || H.kind == HALO_FIELD)
     if (int rc = device_nfw_tables(tab)) return rc;
   DBuf<double> dx, dout;
   CKR(dx.alloc(2 * n));
@@ -1082,6 +1123,7 @@ int glb_halo_nsie(float mass, double z, float sigma, float rcore, float fratio, 
 
 int glb_halo_set_theta(glb_halo *h, double tx, double ty) {
   if (!h) return fail(GLB_ERR_ARG, "null halo");
+  if (h->kind == HALO_FIELD) return fail(GLB_ERR_ARG, "a field plane has no position of its own");
   h->theta[0] = tx;
   h->theta[1] = ty;
   return 0;
@@ -1119,6 +1161,7 @@ int glb_halo_destroy(glb_halo *h) {
   if (!h) return 0;
   cudaSetDevice(h->device);
   h->tree.reset();
+  h->field.reset();
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return 0;
@@ -1155,6 +1198,110 @@ int glb_lens_destroy(glb_lens *l) {
   cudaStream_t s = l->stream;
   delete l;
   if (s) cudaStreamDestroy(s);
+  return 0;
+}
+
+// TreeQuadHalos of a field plane for cosmology c: the member haloes are moved
+// to the plane's redshift (LensHalo::setZlensDist, lens.cpp:418-426), their
+// positions taken (LensHalo::getX) and the tree built on the host and
+// uploaded.
+static int build_field_tree(glb_halo *h, const Cosmo &c) {
+  FieldTree &F = *h->field;
+  const size_t n = F.members.size();
+  const double Dist = angdist(c, h->zlens);
+  h->Dist = Dist;
+  std::vector<double> xp(2 * n);
+  std::vector<float> rmax(n), mass(n);
+  std::vector<FieldHaloDev> fh(n);
+  for (size_t i = 0; i < n; ++i) {
+    glb_halo *m = F.members[i].get();
+    m->zlens = h->zlens;
+    m->Dist = Dist;
+    xp[2 * i] = m->theta[0] * Dist;
+    xp[2 * i + 1] = m->theta[1] * Dist;
+    rmax[i] = m->Rmax;
+    mass[i] = m->mass;
+    FieldHaloDev &d = fh[i];
+    memset(&d, 0, sizeof(d));
+    d.kind = m->kind;
+    d.px = xp[2 * i];
+    d.py = xp[2 * i + 1];
+    d.mass = (double)m->mass;
+    d.nfw = m->nfw;
+    d.nsie = m->nsie;
+  }
+  HaloTreeHost T;
+  std::string err;
+  if (!build_halo_tree(xp, rmax, mass, F.bucket, F.theta, -1, T, err)) return fail(GLB_ERR_SAME_PLACE, err);
+  if (int rc = set_dev(h->device)) return rc;
+  CKR(F.nodes.alloc(std::max<size_t>(T.nodes.size(), 1)));
+  CKR(F.bigs.alloc(std::max<size_t>(T.bigs.size(), 1)));
+  CKR(F.halos.alloc(std::max<size_t>(n, 1)));
+  if (!T.nodes.empty())
+    CKR(cudaMemcpyAsync(F.nodes.p, T.nodes.data(), T.nodes.size() * sizeof(HNode), cudaMemcpyHostToDevice,
+                        h->stream));
+  if (!T.bigs.empty())
+    CKR(cudaMemcpyAsync(F.bigs.p, T.bigs.data(), T.bigs.size() * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  if (n) CKR(cudaMemcpyAsync(F.halos.p, fh.data(), n * sizeof(FieldHaloDev), cudaMemcpyHostToDevice, h->stream));
+  CKR(cudaStreamSynchronize(h->stream));
+  HaloTreeDev &D = F.dev;
+  D.nodes = F.nodes.p;
+  D.bigs = F.bigs.p;
+  D.halos = F.halos.p;
+  D.nnodes = (int)T.nodes.size();
+  D.nhalos = (int)n;
+  D.inv_area = F.sigma_back;
+  D.screen2 = F.inv_screening * F.inv_screening;
+  D.periodic = F.periodic;
+  D.period_x = T.period_x;
+  D.period_y = T.period_y;
+  return 0;
+}
+
+int glb_halo_field_plane(glb_halo *const *halos, int n, double z, double sigma_background,
+                         double inv_screening_scale, glb_halo **out) {
+  if (!out || n < 0 || (n > 0 && !halos)) return fail(GLB_ERR_ARG, "null argument");
+  for (int i = 0; i < n; ++i) {
+    if (!halos[i]) return fail(GLB_ERR_ARG, "null halo");
+    if (halos[i]->kind != HALO_NFW && halos[i]->kind != HALO_NSIE)
+      return fail(GLB_ERR_UNSUPPORTED, "field planes hold NFW and NSIE haloes only");
+    for (int j = 0; j < i; ++j)
+      if (halos[j] == halos[i]) return fail(GLB_ERR_ARG, "a halo appears twice");
+  }
+  std::unique_ptr<glb_halo> h;
+  if (int rc = new_halo(h)) return rc;
+  h->kind = HALO_FIELD;
+  h->zlens = z;
+  h->field = std::make_unique<FieldTree>();
+  FieldTree &F = *h->field;
+  F.sigma_back = sigma_background;
+  F.inv_screening = inv_screening_scale;
+  if (inv_screening_scale != 0) {  // planes.cpp:17
+    F.bucket = 5;
+    F.theta = 0.1;
+    F.periodic = 1;
+  } else {  // TreeQuadHalos defaults, include/quadTreeHalos.h:37-45
+    F.bucket = 5;
+    F.theta = 0.5;
+    F.periodic = 0;
+  }
+  for (int i = 0; i < n; ++i) F.members.emplace_back(halos[i]);
+  // built for the default cosmology here and again for a lens's when inserted
+  if (int rc = build_field_tree(h.get(), Cosmo{0.3, 0.7, 0.7})) {
+    for (auto &m : F.members) m.release();  // on failure the caller keeps its haloes
+    return rc;
+  }
+  *out = h.release();
+  return 0;
+}
+
+int glb_lens_insert_field_plane(glb_lens *l, glb_halo *plane) {
+  if (!l || !plane) return fail(GLB_ERR_ARG, "null argument");
+  if (plane->kind != HALO_FIELD) return fail(GLB_ERR_ARG, "not a field plane (glb_halo_field_plane)");
+  if (int rc = build_field_tree(plane, l->cosmo)) return rc;
+  l->owned.emplace_back(plane);
+  l->field.push_back(PlaneHost{plane->zlens, coordist2(l->cosmo, 0, plane->zlens), {plane}});
+  combine_planes(l);
   return 0;
 }
 
@@ -1203,7 +1350,7 @@ int glb_lens_insert_halo(glb_lens *l, glb_halo *h, int addplanes) {
 
 int glb_lens_nplanes(glb_lens *l, int *nplanes) {
   if (!l || !nplanes) return fail(GLB_ERR_ARG, "null argument");
-  *nplanes = (int)l->main.size();
+  *nplanes = (int)l->planes.size();
   return 0;
 }
 
@@ -1226,7 +1373,7 @@ int glb_lens_reset_source(glb_lens *l, double z, int nearest, int *plane_index) 
     return 0;
   }
   double Ds = coordist2(l->cosmo, 0, z);
-  size_t np = l->main.size();
+  size_t np = l->planes.size();
   if (l->Dl.size() > 1) {
     // NR locate on Dl[0..np-1] (1-based bisection)
     unsigned long n = (unsigned long)np, ju = n + 1, jl = 0, jm;
@@ -1277,7 +1424,7 @@ static int rayshoot_host(glb_lens *l, size_t n, const double *x, const double *z
   CKR(cudaMemcpyAsync(y, dy, 2 * n * sizeof(double), cudaMemcpyDeviceToHost, l->stream));
   CKR(cudaMemcpyAsync(A, dA, 4 * n * sizeof(double), cudaMemcpyDeviceToHost, l->stream));
   CKR(cudaStreamSynchronize(l->stream));
-  if (l->main.size() > 0) {
+  if (l->planes.size() > 0) {
     cudaEventElapsedTime(&l->last_kernel_ms, l->ev[1], l->ev[2]);
     cudaEventElapsedTime(&l->last_total_ms, l->ev[0], l->ev[3]);
   }
@@ -1335,7 +1482,7 @@ int glb_lens_count_interactions(glb_lens *l, size_t n, const double *x, const do
 int glb_lens_last_timing(glb_lens *l, double *kernel_ms, double *total_ms) {
   if (!l) return fail(GLB_ERR_ARG, "null lens");
   if (int rc = set_dev(l->device)) return rc;
-  if (l->main.size() > 0 && cudaEventQuery(l->ev[0]) != cudaErrorNotReady) {
+  if (l->planes.size() > 0 && cudaEventQuery(l->ev[0]) != cudaErrorNotReady) {
     CKR(cudaEventSynchronize(l->ev[3]));
     cudaEventElapsedTime(&l->last_kernel_ms, l->ev[1], l->ev[2]);
     cudaEventElapsedTime(&l->last_total_ms, l->ev[0], l->ev[3]);
@@ -1419,8 +1566,8 @@ extern "C" int glb_lens_rayshoot_noalloc(glb_lens *l, size_t n, const double *x_
     return fail(GLB_ERR_ARG, "glb_lens_rayshoot_noalloc: at most 65536 rays per call");
   if (n > 0 && (!x_dev || !y_dev || !A_dev)) return fail(GLB_ERR_ARG, "null buffer");
   if (precision != GLB_PREC_FP64 && precision != GLB_PREC_SPLIT) return fail(GLB_ERR_ARG, "unknown precision");
-  size_t np = l->main.size(), nh = 0;
-  for (const PlaneHost &p : l->main) nh += p.halos.size();
+  size_t np = l->planes.size(), nh = 0;
+  for (const PlaneHost *p : l->planes) nh += p->halos.size();
   if (np > (size_t)kNoAllocMaxPlanes || nh > (size_t)kNoAllocMaxHalos)
     return fail(GLB_ERR_ARG, "glb_lens_rayshoot_noalloc: at most 64 planes and 256 halos");
   if (int rc = set_dev(l->device)) return rc;
@@ -1445,8 +1592,8 @@ extern "C" int glb_lens_rayshoot_noalloc(glb_lens *l, size_t n, const double *x_
     p.aa = l->dDl[j + 1] / l->Dl[j + 1];
     p.bb = l->Dl[j] / l->Dl[j + 1];
     p.halo0 = nhd;
-    p.nhalo = (int)l->main[j].halos.size();
-    for (glb_halo *h : l->main[j].halos) H[nhd++] = make_halo_dev(*h);
+    p.nhalo = (int)l->planes[j]->halos.size();
+    for (glb_halo *h : l->planes[j]->halos) H[nhd++] = make_halo_dev(*h);
   }
   PlaneDev *d_planes = (PlaneDev *)(S + kOffPlanes);
   HaloDev *d_halos = (HaloDev *)(S + kOffHalos);

@@ -224,8 +224,8 @@ def grid_positions(n1d: int, center=(0.0, 0.0), range_rad: float = 30 * ARCSEC) 
     return np.stack([x, y], axis=1)
 
 
-def field_halos(seed: int, n: int, z: float, field_arcsec: float = 60.0, mmin: float = 1e11,
-                mmax: float = 1e14, n_nsie: int = 0, cosmo: "Cosmology" = None) -> List[object]:
+def field_halos(seed: int, n: int, z: float, field_arcsec: float = 60.0, mmin: float = 1e10,
+                mmax: float = 1e13, n_nsie: int = 0, cosmo: "Cosmology" = None) -> List[object]:
     """n NFW haloes (mass log-uniform in [mmin, mmax], c = 5 (M/1e14)^-0.1,
     truncated at r200) uniform in a square field, plus n_nsie NSIE haloes
     (sigma 150-250 km/s, q 0.6-0.9): the field haloes of one plane."""

@@ -77,7 +77,7 @@ def lens_fixture():
     np.savez_compressed(os.path.join(OUT, "lens_small.npz"), **arrays)
 
 
-FIELD_CASES = ((0.0, 0.0), (1e12, 0.0), (0.0, 2.0), (5e11, 1.0))  # (sigma_back, inv_screening)
+FIELD_CASES = ((0.0, 0.0), (5.0, 0.0), (0.0, 2.0), (2.0, 1.0))  # (sigma_back, inv_screening)
 
 
 def field_rows(halos):

@@ -46,17 +46,7 @@ def force_err(f, ref):
 
 
 def make_lens(spec: synth.LensSpec) -> glb.Lens:
-    L = glb.Lens(spec.zsource)
-    for h in spec.halos:
-        if isinstance(h, synth.ParticlePlane):
-            hh = glb.LensHaloParticles(h.particles, h.z, h.inv_area, h.max_range)
-        elif isinstance(h, synth.NSIEHalo):
-            hh = glb.LensHaloRealNSIE(h.mass, h.z, h.sigma, h.rcore, h.fratio, h.pa)
-        else:
-            hh = glb.LensHaloNFW(h.mass, h.rsize, h.z, h.conc)
-        hh.setTheta(*h.theta)
-        L.insertMainHalo(hh, True)
-    return L
+    return glb.lens_from_spec(spec)
 
 
 # ------------------------------------------------------------------ trees
