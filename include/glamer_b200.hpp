@@ -10,6 +10,7 @@
 //   LensHaloParticles      include/particle_halo.h:58-93
 //   LensHaloNFW            include/lens_halos.h:749-757
 //   LensHaloRealNSIE       include/lens_halos.h:1027-1028
+//   LensPlaneTree          include/planes.h:35-63
 //   Lens                   include/lens.h:73-75, 150-185, 330-349, 458
 //   GridMap                include/gridmap.h:35, 80-83
 // Point and RAY types are taken as template parameters with the reference's
@@ -278,6 +279,44 @@ class LensHaloRealNSIE : public LensHalo {
   float m_, s_, rc_, f_, pa_;
 };
 
+// LensPlaneTree(z, halos, Nhalos, sigma_background, inv_screening_scale)
+// (include/planes.h:35-63, MultiPlane/planes.cpp:13-18): a plane of NFW /
+// NSIE field haloes walked as TreeQuadHalos.  The plane holds its own copies
+// of the haloes (moved to redshift z), so the caller's objects stay usable.
+class LensPlaneTree {
+ public:
+  LensPlaneTree(float z, LensHalo **my_halos, size_t Nhalos, PosType my_sigma_background,
+                PosType my_inv_screening_scale = 0) {
+    std::vector<glb_halo *> members;
+    try {
+      for (size_t i = 0; i < Nhalos; ++i) members.push_back(my_halos[i]->make_copy());
+    } catch (...) {
+      for (glb_halo *m : members) glb_halo_destroy(m);
+      throw;
+    }
+    glb_halo *h = nullptr;
+    const int rc = glb_halo_field_plane(members.data(), (int)members.size(), z, my_sigma_background,
+                                        my_inv_screening_scale, &h);
+    if (rc != GLB_OK) {
+      for (glb_halo *m : members) glb_halo_destroy(m);
+      check(rc);
+    }
+    h_.reset(h);
+  }
+  // LensPlaneTree::force (planes.cpp:65-68): outputs overwritten.
+  void force(PosType *alpha, KappaType *kappa, KappaType *gamma, KappaType *phi, PosType *xx) {
+    if (!h_) throw std::runtime_error("LensPlaneTree: plane has been moved into a Lens");
+    check(glb_halo_force(h_.get(), 1, xx, alpha, kappa, gamma, phi));
+  }
+  glb_halo *release() { return h_.release(); }
+
+ private:
+  struct Del {
+    void operator()(glb_halo *h) const { glb_halo_destroy(h); }
+  };
+  std::unique_ptr<glb_halo, Del> h_;
+};
+
 // ------------------------------------------------------------- the lens
 class Lens {
  public:
@@ -299,6 +338,13 @@ class Lens {
     glb_halo *h = halo_in.release();
     if (!h) throw std::invalid_argument("moveinMainHalo: halo already moved");
     check(glb_lens_insert_halo(l_.get(), h, addplanes ? 1 : 0));
+  }
+  // A field plane among the lens planes, as Lens::createFieldPlanes adds each
+  // LensPlaneTree (lens.cpp:443-452); the lens takes the plane.
+  void insertFieldPlane(LensPlaneTree &plane) {
+    glb_halo *h = plane.release();
+    if (!h) throw std::invalid_argument("insertFieldPlane: plane already moved");
+    check(glb_lens_insert_field_plane(l_.get(), h));
   }
   int getNplanes() const {
     int n = 0;

@@ -238,6 +238,37 @@ int main(int argc, char **argv) {
     REQUIRE(a1[0] == a[2] && a1[1] == a[3] && k1 == k[1] && g1[0] == gg[3]);
   }
 
+  // a field plane: its force through the mirror equals the C ABI's, and the
+  // lens gains one plane
+  {
+    g::LensHaloNFW f1(2e12f, 0.15f, 0.2, 7.0f, 1.0f, 0.0f, cosmo);
+    f1.setTheta(5 * arcsec, 1 * arcsec);
+    g::LensHaloNFW f2(8e11f, 0.1f, 0.2, 8.0f, 1.0f, 0.0f, cosmo);
+    f2.setTheta(-4 * arcsec, 6 * arcsec);
+    g::LensHaloRealNSIE f3(3e12f, 0.2, 180.0f, 1e-4f, 0.8f, 0.2f, cosmo);
+    f3.setTheta(-8 * arcsec, -3 * arcsec);
+    g::LensHalo *members[3] = {&f1, &f2, &f3};
+    g::LensPlaneTree plane(0.2f, members, 3, 0.0);
+    double xx[2] = {0.004, -0.003}, a[2], k, gg[3], ph;
+    plane.force(a, &k, gg, &ph, xx);
+    glb_halo *hs[3] = {f1.make_copy(), f2.make_copy(), f3.make_copy()}, *hp = nullptr;
+    g::check(glb_halo_field_plane(hs, 3, (double)0.2f, 0.0, 0.0, &hp));
+    double a2[2], k2, g2[3], ph2;
+    g::check(glb_halo_force(hp, 1, xx, a2, &k2, g2, &ph2));
+    glb_halo_destroy(hp);
+    REQUIRE(a[0] == a2[0] && a[1] == a2[1] && k == k2 && gg[0] == g2[0] && ph == ph2 && k > 0);
+    const int before = lens_copy.getNplanes();
+    lens_copy.insertFieldPlane(plane);
+    REQUIRE(lens_copy.getNplanes() == before + 1);
+    bool threw = false;
+    try {
+      plane.force(a, &k, gg, &ph, xx);
+    } catch (const std::runtime_error &) {
+      threw = true;
+    }
+    REQUIRE(threw);
+  }
+
   // the SPLIT precision through the mirror stays within the deflection bound
   {
     lens.precision = g::Precision::SPLIT;
