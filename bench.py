@@ -246,6 +246,44 @@ def run_single(args):
     print(json.dumps(line))
 
 
+def run_field(args):
+    """The 10-plane light cone plus nine field planes between its particle
+    planes (z = 0.2, 0.4, ..., 1.8), each of 400 NFW haloes (1e10-1e13 Msun)
+    and 4 NSIE haloes over the 60 arcsec field (LensPlaneTree, no screening);
+    2048^2 rays, split and plain FP64 forms."""
+    import torch
+    import slsimlib_b200 as glb
+    from slsimlib_b200 import synth
+    spec, n1d = workload(args.small)
+    for i in range(9):
+        z = 0.2 + 0.2 * i
+        spec.halos.append(synth.FieldPlane(z, synth.field_halos(600 + i, 400, z, n_nsie=4)))
+    lens = make_lens(spec)
+    x_host = synth.grid_positions(n1d, range_rad=FIELD_ARCSEC * synth.ARCSEC)
+    n = n1d * n1d
+    x = torch.from_numpy(x_host).cuda()
+    y = torch.empty((n, 2), dtype=torch.float64, device="cuda")
+    A = torch.empty((n, 4), dtype=torch.float64, device="cuda")
+    st = torch.cuda.Stream()
+    torch.cuda.set_stream(st)
+    out = {}
+    for prec in (glb.PREC_FP64, glb.PREC_SPLIT):
+        f = lambda: lens.rayshoot_device(n, x.data_ptr(), None, y.data_ptr(), A.data_ptr(), prec, st.cuda_stream)
+        for _ in range(args.warmup if prec == glb.PREC_SPLIT else 1):
+            f()
+        torch.cuda.synchronize()
+        steps = args.steps if prec == glb.PREC_SPLIT else 1
+        out[prec] = (_timed(f, st, steps), y.cpu().numpy().copy(), A.cpu().numpy().copy())
+    ms = out[glb.PREC_SPLIT][0]
+    line = _base_line(args, "rays/s/GPU, light cone with field planes (split form)", "rays/s", n / (ms / 1e3), ms,
+                      "f32+f64", f"light cone (10 particle planes, 4,194,304 particles, NSIE) + 9 field planes of "
+                                 f"404 haloes, {n1d}^2 rays over 60 arcsec" + (" [reduced]" if args.small else ""))
+    line["planes"] = lens.getNplanes()
+    line["plain_fp64"] = {"value": n / (out[glb.PREC_FP64][0] / 1e3), "unit": "rays/s"}
+    line["errors_vs_fp64"] = error_stats(x_host, out[1][1], out[1][2], out[0][1], out[0][2])
+    print(json.dumps(line))
+
+
 def run_sweep(args):
     """Precision sweep on one large plane: 2^24 triaxial-NFW particles
     (1e15 Msun, c=4, axes 1/0.8/0.6) + 10% uniform background, 4096^2 rays
@@ -446,14 +484,16 @@ def main():
     ap.add_argument("--n1d", type=int, default=0,
                     help="rays per side of the light-cone grid (default 2048; a profiling size, not a bench line)")
     ap.add_argument("--workload", default="lightcone",
-                    choices=["lightcone", "single", "sweep", "batched", "served"],
+                    choices=["lightcone", "single", "sweep", "batched", "served", "field"],
                     help="lightcone (default): the 10-plane light cone; the others are the single plane, the "
-                         "precision sweep, batched uneven lenses and the served request stream")
+                         "precision sweep, batched uneven lenses, the served request stream and the light cone "
+                         "with field planes")
     args = ap.parse_args()
     if args.impl == "ours" and args.workload != "lightcone":
         import torch
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-        return {"single": run_single, "sweep": run_sweep, "batched": run_batched, "served": run_served}[
+        return {"single": run_single, "sweep": run_sweep, "batched": run_batched, "served": run_served,
+                "field": run_field}[
             args.workload](args)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
