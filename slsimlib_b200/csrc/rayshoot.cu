@@ -167,6 +167,7 @@ struct glb_lens {
   std::vector<PlaneHost> main;  // sorted by Dl
   std::vector<PlaneHost> field;  // LensPlaneTree planes, in insertion order
   std::vector<PlaneHost *> planes;  // main and field planes in order of distance (combinePlanes)
+  std::vector<char> plane_field;    // per plane: holds a field plane (HALO_FIELD)
   std::vector<double> plane_z, Dl, dDl;  // combined, source pseudo-plane last
   bool toggle_source_plane = false;
   double zs_implant = 0;
@@ -402,7 +403,7 @@ struct StepArgs {
 
 // One lens plane for every ray: LensPlaneSingular::force + the recursion of
 // include/lens.h:1003-1066.
-template <int PREC, bool COUNT = false>
+template <int PREC, bool COUNT = false, bool FIELD = false>
 __device__ __forceinline__ void plane_step(const StepArgs &a) {
   const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   const bool inrange = k < a.n;
@@ -445,7 +446,7 @@ __device__ __forceinline__ void plane_step(const StepArgs &a) {
       // LensHaloParticles::force_halo negates alpha (particle_halo.h:432-433)
       acc[0] = -acc[0];
       acc[1] = -acc[1];
-    } else if (kind == HALO_FIELD) {
+    } else if (FIELD && kind == HALO_FIELD) {
       // LensPlaneTree::force is the tree's output as it is (planes.cpp:65-68)
       const Force6 f = field_plane_force<false>(&H->htree, &a.tab, xc0, xc1, valid);
       acc[0] = -f.a0;
@@ -509,11 +510,16 @@ __device__ __forceinline__ void plane_step(const StepArgs &a) {
 // The FP64 form keeps the compiler's own register choice; the split form is
 // latency-bound (dependent node loads), and capping it at 80 registers
 // (6 blocks of 128 per SM) buys the occupancy that hides them.
-template <int PREC, bool COUNT = false>
+// Planes holding a field plane (HALO_FIELD) use the FIELD instances, so that
+// the halo-tree walk adds no code to the kernels of particle planes.
+template <int PREC, bool COUNT = false, bool FIELD = false>
 __global__ void __launch_bounds__(128) k_plane_step(StepArgs a) {
-  plane_step<PREC, COUNT>(a);
+  plane_step<PREC, COUNT, FIELD>(a);
 }
-__global__ void __launch_bounds__(128, 6) k_plane_step_split(StepArgs a) { plane_step<GLB_PREC_SPLIT>(a); }
+template <bool FIELD = false>
+__global__ void __launch_bounds__(128, 6) k_plane_step_split(StepArgs a) {
+  plane_step<GLB_PREC_SPLIT, false, FIELD>(a);
+}
 
 // force2D_recur / force_halo at arbitrary positions (walk-level API, with phi).
 __global__ void __launch_bounds__(128) k_halo_force(HaloDev H, NFWTables tab, size_t n, const double *x,
@@ -658,6 +664,9 @@ void combine_planes(glb_lens *l) {
   for (size_t i = 1; i < n; ++i)
     if ((l->Dl[i] - l->Dl[i - 1]) < 1e-6) l->Dl[i] = l->Dl[i - 1] + 1e-6;  // MIN_PLANE_DIST
   for (size_t i = 0; i < n; ++i) l->plane_z[i] = l->planes[i]->z;
+  l->plane_field.assign(n, 0);
+  for (size_t i = 0; i < n; ++i)
+    for (const glb_halo *h : l->planes[i]->halos) l->plane_field[i] |= h->kind == HALO_FIELD;
   if (n > 0 && l->zsource <= l->plane_z[n - 1]) l->zsource = l->plane_z[n - 1] + 0.1;
   l->plane_z[n] = l->zsource;
   l->Dl[n] = coordist2(l->cosmo, 0, l->zsource);
@@ -785,10 +794,17 @@ int rayshoot_device(glb_lens *l, size_t n, const double *x, const double *zs, do
   CKR(cudaEventRecord(l->ev[1], s));
   for (int j = 0; j < jmax_launch; ++j) {
     a.j = j;
-    if (d_counts)
+    const bool fld = l->plane_field[j] != 0;
+    if (d_counts && fld)
+      k_plane_step<GLB_PREC_FP64, true, true><<<nblk(n, 128), 128, 0, s>>>(a);
+    else if (d_counts)
       k_plane_step<GLB_PREC_FP64, true><<<nblk(n, 128), 128, 0, s>>>(a);
+    else if (precision == GLB_PREC_SPLIT && fld)
+      k_plane_step_split<true><<<nblk(n, 128), 128, 0, s>>>(a);
     else if (precision == GLB_PREC_SPLIT)
       k_plane_step_split<<<nblk(n, 128), 128, 0, s>>>(a);
+    else if (fld)
+      k_plane_step<GLB_PREC_FP64, false, true><<<nblk(n, 128), 128, 0, s>>>(a);
     else
       k_plane_step<GLB_PREC_FP64><<<nblk(n, 128), 128, 0, s>>>(a);
   }
@@ -1662,8 +1678,13 @@ extern "C" int glb_lens_rayshoot_noalloc(glb_lens *l, size_t n, const double *x_
   }
   for (int j = 0; j < jmax_launch; ++j) {
     a.j = j;
-    if (precision == GLB_PREC_SPLIT)
+    const bool fld = l->plane_field[j] != 0;
+    if (precision == GLB_PREC_SPLIT && fld)
+      k_plane_step_split<true><<<nblk(n, 128), 128, 0, s>>>(a);
+    else if (precision == GLB_PREC_SPLIT)
       k_plane_step_split<<<nblk(n, 128), 128, 0, s>>>(a);
+    else if (fld)
+      k_plane_step<GLB_PREC_FP64, false, true><<<nblk(n, 128), 128, 0, s>>>(a);
     else
       k_plane_step<GLB_PREC_FP64><<<nblk(n, 128), 128, 0, s>>>(a);
   }
