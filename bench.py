@@ -622,7 +622,9 @@ def main():
                          "alg_flops_per_step": alg_flops,
                          "counts": {"V": V, "F": F, "P": P, "B": B, "S": S},
                          "lane_efficiency": {"nodes": V / max(Wn, 1), "leaf_particles": P / max(Wp, 1)}},
-            "gpu_launches": args.steps * (4 + nplanes),
+            # per step: ray bbox, Morton keys, the 6 kernels of the CUB radix sort compiled into the
+            # library, state init, one plane step per plane, finish (ncu launch list)
+            "gpu_launches": args.steps * (10 + nplanes),
             "clocks": clocks,
         }
         if cpu:
