@@ -185,6 +185,18 @@ int glb_lens_rayshoot_device(glb_lens *l, size_t n, const double *x_dev, const d
 int glb_gridmap(glb_lens *l, size_t n1d, const double *center, double range, double *y, double *A,
                 int precision);
 
+/* GridMap(lens, N1d, center, range).writePixelMap(lensvar)
+ * (include/gridmap.h:529-598): the grid shot on the GPU and reduced there to
+ * one map value per grid point (N1d^2 doubles, GridMap order, x fastest), so
+ * no per-ray y / A arrays reach the host.  lensvar is the reference's
+ * LensingVariable (include/standard.h:89-102): 0 DELAYT (0 on this path),
+ * 1 ALPHA, 2 ALPHA1, 3 ALPHA2, 4 KAPPA, 5 GAMMA, 6 GAMMA1, 7 GAMMA2, 8 GAMMA3,
+ * 9 INVMAG; 10 PHI and 11 SurfBrightness return GLB_ERR_UNSUPPORTED (the
+ * reference throws std::runtime_error for PHI; surface brightness needs the
+ * sources, which are outside this library). */
+int glb_gridmap_pixelmap(glb_lens *l, size_t n1d, const double *center, double range, int lensvar, double *map,
+                         int precision);
+
 /* No counterpart in the reference.  glb_lens_rayshoot_device for callers that
  * cannot allocate device memory while they shoot rays: cudaMalloc / cudaFree
  * synchronise the whole device and can fail under a memory cap, which grid

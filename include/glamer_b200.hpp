@@ -23,6 +23,7 @@
 #ifndef GLAMER_B200_HPP
 #define GLAMER_B200_HPP
 
+#include <cmath>
 #include <cstddef>
 #include <memory>
 #include <stdexcept>
@@ -439,6 +440,10 @@ class Lens {
   std::unique_ptr<glb_lens, Del> l_;
 };
 
+// LensingVariable (include/standard.h:89-102)
+enum class LensingVariable { DELAYT, ALPHA, ALPHA1, ALPHA2, KAPPA, GAMMA, GAMMA1, GAMMA2, GAMMA3, INVMAG, PHI,
+                             SurfBrightness };
+
 // ------------------------------------------------------------- GridMap
 // GridMap(LensHndl, N1d, center, range) (gridmap.h:35, gridmap.cpp:93-120):
 // the grid is generated and shot on the GPU; y and A are kept per point in
@@ -477,6 +482,42 @@ class GridMap {
   double gamma2(size_t i) const { return 0.5 * (A_[4 * i + 1] + A_[4 * i + 2]); }
   double gamma3(size_t i) const { return 0.5 * (A_[4 * i + 2] - A_[4 * i + 1]); }
   double invmag(size_t i) const { return A_[4 * i] * A_[4 * i + 3] - A_[4 * i + 1] * A_[4 * i + 2]; }
+
+  // GridMap::writePixelMap (gridmap.h:529-598) as a plain array in grid
+  // order (x fastest) from this GridMap's points.
+  std::vector<double> writePixelMap(LensingVariable lensvar) const {
+    const size_t n = getNumberOfPoints();
+    std::vector<double> m(n, 0.0);
+    for (size_t i = 0; i < n; ++i) {
+      double x[2];
+      image(i, x);
+      const double d0 = x[0] - y_[2 * i], d1 = x[1] - y_[2 * i + 1];
+      switch (lensvar) {
+        case LensingVariable::DELAYT: m[i] = 0; break;
+        case LensingVariable::ALPHA: m[i] = std::sqrt(d0 * d0 + d1 * d1); break;
+        case LensingVariable::ALPHA1: m[i] = d0; break;
+        case LensingVariable::ALPHA2: m[i] = d1; break;
+        case LensingVariable::KAPPA: m[i] = kappa(i); break;
+        case LensingVariable::GAMMA: m[i] = std::sqrt(gamma1(i) * gamma1(i) + gamma2(i) * gamma2(i)); break;
+        case LensingVariable::GAMMA1: m[i] = gamma1(i); break;
+        case LensingVariable::GAMMA2: m[i] = gamma2(i); break;
+        case LensingVariable::GAMMA3: m[i] = gamma3(i); break;
+        case LensingVariable::INVMAG: m[i] = invmag(i); break;
+        default:
+          throw std::runtime_error("GridMap::writePixelMap() does not work for the input LensingVariable");
+      }
+    }
+    return m;
+  }
+  // The same map computed on the GPU from a fresh grid (no per-point arrays
+  // on the host): glb_gridmap_pixelmap.
+  static std::vector<double> writePixelMapOnDevice(Lens *lens, unsigned long N1d, const double center[2],
+                                                   double range, LensingVariable lensvar,
+                                                   Precision prec = Precision::FP64) {
+    std::vector<double> m(N1d * N1d);
+    check(glb_gridmap_pixelmap(lens->handle(), N1d, center, range, (int)lensvar, m.data(), (int)prec));
+    return m;
+  }
 
  private:
   size_t n_;

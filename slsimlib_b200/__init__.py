@@ -57,7 +57,7 @@ EXPORTED = [
     "glb_halo_params", "glb_halo_destroy", "glb_halo_field_plane",
     "glb_lens_create", "glb_lens_destroy", "glb_lens_insert_halo", "glb_lens_insert_field_plane",
     "glb_lens_nplanes", "glb_lens_planes",
-    "glb_lens_reset_source", "glb_lens_rayshoot", "glb_lens_rayshoot_device", "glb_gridmap",
+    "glb_lens_reset_source", "glb_lens_rayshoot", "glb_lens_rayshoot_device", "glb_gridmap", "glb_gridmap_pixelmap",
     "glb_lens_last_timing", "glb_lens_count_interactions", "glb_lens_rayshoot_noalloc",
     "glb_batch_create_grids", "glb_batch_run", "glb_batch_autotune", "glb_batch_set_block", "glb_batch_info",
     "glb_batch_result", "glb_batch_destroy",
@@ -115,6 +115,7 @@ def load_library():
     L.glb_lens_rayshoot.argtypes = [_vp, C.c_size_t, _vp, _vp, _vp, _vp, C.c_int]
     L.glb_lens_rayshoot_device.argtypes = [_vp, C.c_size_t, _vp, _vp, _vp, _vp, C.c_int, _vp]
     L.glb_gridmap.argtypes = [_vp, C.c_size_t, _vp, C.c_double, _vp, _vp, C.c_int]
+    L.glb_gridmap_pixelmap.argtypes = [_vp, C.c_size_t, _vp, C.c_double, C.c_int, _vp, C.c_int]
     L.glb_lens_last_timing.argtypes = [_vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.glb_lens_count_interactions.argtypes = [_vp, C.c_size_t, _vp, _vp, _vp]
     L.glb_lens_rayshoot_noalloc.argtypes = [_vp, C.c_size_t, _vp, _vp, _vp, _vp, C.c_int, _vp]
@@ -446,6 +447,22 @@ class GridMap:
 
     def alpha(self):
         return self.positions() - self.y
+
+
+# LensingVariable, include/standard.h:89-102
+DELAYT, ALPHA, ALPHA1, ALPHA2, KAPPA, GAMMA, GAMMA1, GAMMA2, GAMMA3, INVMAG, PHI, SURF_BRIGHTNESS = range(12)
+
+
+def writePixelMap(lens: Lens, N1d: int, center: Sequence[float], range_: float, lensvar: int,
+                  precision=PREC_FP64) -> np.ndarray:
+    """GridMap(lens, N1d, center, range).writePixelMap(lensvar)
+    (include/gridmap.h:529-598) computed on the GPU: an (N1d, N1d) map, rows
+    of constant y; only the map comes back to the host."""
+    c = np.ascontiguousarray(center, dtype=np.float64)
+    out = np.zeros(int(N1d) * int(N1d))
+    _check(load_library().glb_gridmap_pixelmap(lens._h, int(N1d), _p(c), float(range_), int(lensvar), _p(out),
+                                               precision))
+    return out.reshape(int(N1d), int(N1d))
 
 
 def direct_sum_device(n: int, particles_ptr: int, inv_area: float, nrays: int, rays_ptr: int, out_ptr: int,

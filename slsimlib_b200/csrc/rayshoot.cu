@@ -616,6 +616,37 @@ __global__ void __launch_bounds__(256) k_direct_sum(const glb_particle_rec *p, s
     for (int c = 0; c < 5; ++c) out[5 * k + c] = acc[c];
 }
 
+// GridMap::writePixelMap (include/gridmap.h:529-598): one map pixel per grid
+// point, the quantity selected by LensingVariable (include/standard.h:89-102):
+// 0 DELAYT (0 on this path), 1 ALPHA = |x - y|, 2 ALPHA1, 3 ALPHA2,
+// 4 KAPPA = 1 - (a0 + a3)/2, 5 GAMMA = |(gamma1, gamma2)|, 6 GAMMA1 = (a0 - a3)/2,
+// 7 GAMMA2 = (a1 + a2)/2, 8 GAMMA3 = (a2 - a1)/2, 9 INVMAG = a0 a3 - a1 a2
+// (include/point.h:377-381, 446-448).
+__global__ void k_pixelmap(const double *x, const double *y, const double *A, size_t n, int var, double *map) {
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double a0 = A[4 * i], a1 = A[4 * i + 1], a2 = A[4 * i + 2], a3 = A[4 * i + 3];
+  const double d0 = x[2 * i] - y[2 * i], d1 = x[2 * i + 1] - y[2 * i + 1];
+  double v = 0;
+  switch (var) {
+    case 1: v = sqrt(d0 * d0 + d1 * d1); break;
+    case 2: v = d0; break;
+    case 3: v = d1; break;
+    case 4: v = 1 - (a0 + a3) / 2; break;
+    case 5: {
+      const double g1 = (a0 - a3) / 2, g2 = (a1 + a2) / 2;
+      v = sqrt(g1 * g1 + g2 * g2);
+      break;
+    }
+    case 6: v = (a0 - a3) / 2; break;
+    case 7: v = (a1 + a2) / 2; break;
+    case 8: v = (a2 - a1) / 2; break;
+    case 9: v = a0 * a3 - a1 * a2; break;
+    default: v = 0; break;  // DELAYT: dt = 0
+  }
+  map[i] = v;
+}
+
 inline int nblk(size_t n, int t) { return (int)((n + t - 1) / t); }
 
 }  // namespace
@@ -1470,6 +1501,32 @@ int glb_gridmap(glb_lens *l, size_t n1d, const double *center, double range, dou
   int rc = rayshoot_host(l, n, dx.p, nullptr, y, A, precision, true);
   CKR(cudaStreamSynchronize(l->stream));
   return rc;
+}
+
+int glb_gridmap_pixelmap(glb_lens *l, size_t n1d, const double *center, double range, int lensvar, double *map,
+                         int precision) {
+  if (!l || !center || !map) return fail(GLB_ERR_ARG, "null argument");
+  if (n1d < 1) return fail(GLB_ERR_ARG, "GridMap size is < 1!");  // gridmap.cpp:102
+  if (range <= 0) return fail(GLB_ERR_ARG, "GridMap range is <= 0!");
+  if (precision != GLB_PREC_FP64 && precision != GLB_PREC_SPLIT) return fail(GLB_ERR_ARG, "unknown precision");
+  if (lensvar == 10 || lensvar == 11)  // PHI, SurfBrightness (gridmap.h:588-594)
+    return fail(GLB_ERR_UNSUPPORTED, "GridMap::writePixelMap() does not work for the input LensingVariable");
+  if (lensvar < 0 || lensvar > 11) return fail(GLB_ERR_ARG, "unknown LensingVariable");
+  if (int rc = set_dev(l->device)) return rc;
+  const size_t n = n1d * n1d;
+  DBuf<double> dx, dy, dA, dm;
+  CKR(dx.alloc(2 * n));
+  CKR(dy.alloc(2 * n));
+  CKR(dA.alloc(4 * n));
+  CKR(dm.alloc(n));
+  k_grid<<<nblk(n, 256), 256, 0, l->stream>>>(n1d, center[0], center[1], range, dx.p);
+  CKR(cudaGetLastError());
+  if (int rc = rayshoot_device(l, n, dx.p, nullptr, dy.p, dA.p, precision, l->stream)) return rc;
+  k_pixelmap<<<nblk(n, 256), 256, 0, l->stream>>>(dx.p, dy.p, dA.p, n, lensvar, dm.p);
+  CKR(cudaGetLastError());
+  CKR(cudaMemcpyAsync(map, dm.p, n * sizeof(double), cudaMemcpyDeviceToHost, l->stream));
+  CKR(cudaStreamSynchronize(l->stream));
+  return 0;
 }
 
 int glb_lens_count_interactions(glb_lens *l, size_t n, const double *x, const double *zs,

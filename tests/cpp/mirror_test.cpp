@@ -145,6 +145,13 @@ int main(int argc, char **argv) {
     std::memcpy(&gy[2 * i], gm.source(i), 2 * sizeof(double));
     std::memcpy(&gA[4 * i], gm.A(i), 4 * sizeof(double));
   }
+  for (g::LensingVariable v : {g::LensingVariable::ALPHA, g::LensingVariable::KAPPA, g::LensingVariable::GAMMA,
+                               g::LensingVariable::INVMAG, g::LensingVariable::GAMMA3}) {
+    const std::vector<double> host = gm.writePixelMap(v);
+    const std::vector<double> dev = g::GridMap::writePixelMapOnDevice(&lens, n1d, center, range, v);
+    for (size_t i = 0; i < host.size(); ++i)
+      REQUIRE(std::fabs(host[i] - dev[i]) <= 1e-12 * std::fabs(host[i]) + 1e-300);
+  }
   write(out + "/grid_y.bin", gy.data(), gy.size() * sizeof(double));
   write(out + "/grid_A.bin", gA.data(), gA.size() * sizeof(double));
 

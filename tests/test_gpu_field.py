@@ -126,3 +126,27 @@ def test_field_plane_errors_and_edges():
     f = pack(*glb.halo_from_spec(one).force_halo(xx))
     m, cols = force_err(f, H.oracle_halo_force(one, xx)[0])
     assert m < RTOL64, cols
+
+
+def test_pixelmap_matches_gridmap_and_oracle():
+    """writePixelMap on the device: every LensingVariable equals the value
+    derived from the GridMap's y and A, which equal the oracle's."""
+    spec = mixed_spec(seed=13)
+    L = glb.lens_from_spec(spec)
+    n1d, c, rng = 31, (1e-6, -2e-6), 50 * synth.ARCSEC
+    gm = glb.GridMap(L, n1d, c, rng)
+    x = gm.positions()
+    yo, Ao = H.OracleLens(spec).rayshoot(x)
+    assert np.max(rel_err(gm.y, yo)) < RTOL64
+    a = x - gm.y
+    g1, g2 = gm.gamma1(), gm.gamma2()
+    expect = {glb.DELAYT: np.zeros(len(x)), glb.ALPHA: np.hypot(a[:, 0], a[:, 1]), glb.ALPHA1: a[:, 0],
+              glb.ALPHA2: a[:, 1], glb.KAPPA: gm.kappa(), glb.GAMMA: np.hypot(g1, g2), glb.GAMMA1: g1,
+              glb.GAMMA2: g2, glb.GAMMA3: gm.gamma3(), glb.INVMAG: gm.invmag()}
+    for var, e in expect.items():
+        m = glb.writePixelMap(L, n1d, c, rng, var).ravel()
+        np.testing.assert_allclose(m, e, rtol=1e-12, atol=1e-15 * np.abs(e).max(), err_msg=str(var))
+    for var in (glb.PHI, glb.SURF_BRIGHTNESS):
+        with pytest.raises(glb.GlamerError) as ex:
+            glb.writePixelMap(L, n1d, c, rng, var)
+        assert ex.value.code == glb.GLB_ERR_UNSUPPORTED
