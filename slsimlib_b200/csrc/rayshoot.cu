@@ -508,8 +508,9 @@ __device__ __forceinline__ void plane_step(const StepArgs &a) {
 }
 
 // The FP64 form keeps the compiler's own register choice; the split form is
-// latency-bound (dependent node loads), and capping it at 80 registers
-// (6 blocks of 128 per SM) buys the occupancy that hides them.
+// latency-bound (dependent node loads and short arithmetic chains), and
+// capping it at 64 registers (8 blocks of 128 per SM, half the warp slots)
+// buys the occupancy that hides them, spills included.
 // Planes holding a field plane (HALO_FIELD) use the FIELD instances, so that
 // the halo-tree walk adds no code to the kernels of particle planes.
 template <int PREC, bool COUNT = false, bool FIELD = false>
@@ -517,7 +518,7 @@ __global__ void __launch_bounds__(128) k_plane_step(StepArgs a) {
   plane_step<PREC, COUNT, FIELD>(a);
 }
 template <bool FIELD = false>
-__global__ void __launch_bounds__(128, 6) k_plane_step_split(StepArgs a) {
+__global__ void __launch_bounds__(128, 8) k_plane_step_split(StepArgs a) {
   plane_step<GLB_PREC_SPLIT, false, FIELD>(a);
 }
 

@@ -445,6 +445,16 @@ __global__ void k_gather_bigs(const float4 *parts, const unsigned *bval, int nb,
 
 // out[0..3]: mass and quadrupole of the last branch of the moments walk (the
 // far-field potential's); out[4..7]: the root's mass, |mass| sum and centre.
+// Every walk moves forward through the preorder array: a node's skip must lie
+// in (i, nnodes].  The split walk relies on it without a per-node guard, so
+// the build checks it once; *bad counts the nodes that break it.
+__global__ void k_check_skips(const GNodeS *sn, int nnodes, int *bad) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nnodes) return;
+  const int k = sn[i].skip;
+  if (k <= i || k > nnodes) atomicAdd(bad, 1);
+}
+
 __global__ void k_phi_node(const Slot *s, double *out) {
   out[4] = s[0].count > 0 ? s[0].mass : 0.0;
   out[5] = s[0].count > 0 ? s[0].absm : 0.0;
@@ -663,6 +673,12 @@ Status build_tree(const glb_particle_rec *hp, size_t n, const TreeParams &prm, b
   CK(T->nodes.alloc(nnodes));
   CK(T->snodes.alloc(nnodes));
   k_emit_nodes<<<nblk(nslots, 256), 256, 0, st>>>(slots.p, nslots, prm.theta, T->nodes.p, T->snodes.p);
+  DBuf<int> dbad;
+  CK(dbad.alloc(1));
+  CK(cudaMemsetAsync(dbad.p, 0, sizeof(int), st));
+  if (nnodes > 0) k_check_skips<<<nblk(nnodes, 256), 256, 0, st>>>(T->snodes.p, nnodes, dbad.p);
+  int hbad = 0;
+  CK(cudaMemcpyAsync(&hbad, dbad.p, sizeof(int), cudaMemcpyDeviceToHost, st));
   DBuf<double> phin;
   CK(phin.alloc(8));
   k_phi_node<<<1, 1, 0, st>>>(slots.p, phin.p);
@@ -679,6 +695,7 @@ Status build_tree(const glb_particle_rec *hp, size_t n, const TreeParams &prm, b
   CK(cudaEventRecord(e1, st));
   CK(cudaStreamSynchronize(st));
   CK(cudaGetLastError());
+  if (hbad != 0) return Status::err(-2, "tree build produced a node array that does not move forward");
   cudaEventElapsedTime(&T->build_ms, e0, e1);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);

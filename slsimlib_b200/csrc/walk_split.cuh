@@ -208,7 +208,7 @@ __device__ __forceinline__ void walk_split(const TreeDev &T, double rx, double r
     const float4 *sp = reinterpret_cast<const float4 *>(T.snodes + node);
     const float4 c0 = __ldg(sp), c1 = __ldg(sp + 1);  // centre; open2, near2, mass/pi, open band
     const int4 c3 = __ldg(reinterpret_cast<const int4 *>(sp + 3));  // skip, leaf, start, count
-    const int skip = max(c3.x, node + 1);  // forward progress even on a malformed array
+    const int skip = c3.x;  // > node: checked once per tree by the build (k_check_skips)
     const bool act = node >= resume;
     const float2 d = PURE ? __fadd2_rn(make_float2(c0.x, c0.y), nrh)
                           : __fadd2_rn(__fadd2_rn(make_float2(c0.x, c0.y), nrh), __fadd2_rn(make_float2(c0.z, c0.w), nrl));
