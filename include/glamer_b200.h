@@ -197,6 +197,24 @@ int glb_gridmap(glb_lens *l, size_t n1d, const double *center, double range, dou
 int glb_gridmap_pixelmap(glb_lens *l, size_t n1d, const double *center, double range, int lensvar, double *map,
                          int precision);
 
+/* GridMap(lens, N1d, center, range).RefreshSurfaceBrightnesses(&source)
+ * (TreeCode_link/gridmap.cpp:174-187): the grid shot on the GPU and the
+ * source's surface brightness evaluated there at every ray's source-plane
+ * position; sb gets N1d^2 values (GridMap order) and *total (optional) the
+ * reference's flux sum, sum of sb x resolution^2 in point order
+ * (resolution = range / (N1d - 1), N1d >= 2).  source_kind and
+ * source_params = {x, y (source position, radians), ...}:
+ *   0 SourceUniform(position, z, radius) (AnalyticNSIE/source.cpp:207-209):
+ *     {x, y, radius (radians)};
+ *   1 SourceGaussian(position, r_size, z, SBlimit, zero_point)
+ *     (source.cpp:211-213): {x, y, r_size (radians)};
+ *   2 SourceSersic(mag, Reff, PA, index, q, z, band) (Source/sersic.cpp:116-135):
+ *     {x, y, total flux (SourceColored::mag_to_flux of the magnitude),
+ *      Reff (arcsec), PA (radians), index, q, sb_limit}.
+ * Other kinds: GLB_ERR_UNSUPPORTED. */
+int glb_gridmap_surface_brightness(glb_lens *l, size_t n1d, const double *center, double range, int source_kind,
+                                   const double *source_params, double *sb, double *total, int precision);
+
 /* No counterpart in the reference.  glb_lens_rayshoot_device for callers that
  * cannot allocate device memory while they shoot rays: cudaMalloc / cudaFree
  * synchronise the whole device and can fail under a memory cap, which grid

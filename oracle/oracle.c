@@ -891,6 +891,35 @@ void orc_halo_force(orc_halo *h, size_t n, const double *xcm, double *alpha, dou
   }
 }
 
+/* ===================== source surface brightness ======================== */
+/* SourceUniform::SurfaceBrightness (AnalyticNSIE/source.cpp:207-209),
+ * SourceGaussian::SurfaceBrightness (source.cpp:211-213) and
+ * SourceSersic::SurfaceBrightness (Source/sersic.cpp:116-135, constants from
+ * ReSet / setReff / setSersicIndex / setAxesRatio, include/sersic_source.h). */
+void orc_source_sb(int kind, const double *p, size_t n, const double *y, double *out) {
+  for (size_t i = 0; i < n; ++i) {
+    const double d0 = y[2 * i] - p[0], d1 = y[2 * i + 1] - p[1];
+    if (kind == 0) {
+      out[i] = (double)((pow(d0, 2) + pow(d1, 2)) < p[2] * p[2]);
+    } else if (kind == 1) {
+      out[i] = exp(-(pow(d0, 2) + pow(d1, 2)) / (p[2] * p[2]));
+    } else {
+      const double flux = p[2], Reff = p[3] * 4.848136811e-6, PA = p[4], index = p[5], sb_limit = p[7];
+      double q = p[6];
+      if (q > 1) q = 1 / q;
+      const double bn = 1.9992 * index - 0.3271;
+      const double I_n = 1. / index * pow(bn, 2 * index) / tgamma(2 * index);
+      const double I_q = 1. / q, I_r = 1. / 2. / ORC_PI / Reff / Reff;
+      const double cosPA = cos(PA), sinPA = sin(PA);
+      const double x0 = d0 * cosPA + d1 * sinPA, x1 = d0 * sinPA - d1 * cosPA;
+      double r = sqrt(x0 * x0 + x1 * x1 / q / q);
+      if (r < 4.848136811e-9) r = 4.848136811e-9;
+      double sb = flux * I_n * I_q * I_r * exp(-bn * pow(r / Reff, 1. / index));
+      out[i] = sb < sb_limit ? 0. : sb;
+    }
+  }
+}
+
 /* =================== TreeQuadHalos / LensPlaneTree ===================== */
 /* A quadtree over analytic haloes (include/quadTreeHalos.h:35-130) as built by
  * LensPlaneTree (MultiPlane/planes.cpp:13-18). */

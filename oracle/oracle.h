@@ -99,6 +99,12 @@ orc_halo *orc_halo_field_plane(orc_halo **halos, int n, double z,
                                double sigma_back, double inv_screening,
                                int *err);
 
+/* Source::SurfaceBrightness at n source-plane positions y (2n, radians).
+ * p = {x, y, ...}: kind 0 SourceUniform {radius}; 1 SourceGaussian {r_size};
+ * 2 SourceSersic {flux, Reff (arcsec), PA, index, q, sb_limit}. */
+void orc_source_sb(int kind, const double *p, size_t n, const double *y,
+                   double *out);
+
 /* ---------------- Lens (MultiPlane/lens.cpp, include/lens.h) ---------- */
 typedef struct orc_lens orc_lens;
 orc_lens *orc_lens_create(double zsource);

@@ -25,6 +25,11 @@
  *                                                    TIMEFILE gets the ctor wall seconds
  *   rays XFILE N ZFILE OUT TIMEFILE                  rayshooterInternal(N, RAY*) with per-ray z
  *   points XFILE N OUT TIMEFILE                      rayshooterInternal(N, Point*)
+ *   sourcesb KIND A B C D E F G YFILE N OUT
+ *        Source::SurfaceBrightness at N source-plane positions -> OUT: N values
+ *        and the source's total flux.  KIND 0 SourceUniform(Point_2d(A,B), 1, C);
+ *        1 SourceGaussian(Point_2d(A,B), C, 1, -1, 0); 2 SourceSersic(mag C,
+ *        Reff D arcsec, PA E, index F, q G, z 1, zeropoint 0) at (A, B).
  *   fieldplane HFILE NH Z SIGMA_BACK INV_SCREEN XFILE N OUT
  *        LensPlaneTree(Z, haloes, NH, SIGMA_BACK, INV_SCREEN)::force at N plane
  *        positions -> per position alpha[2] kappa gamma[3] phi.  HFILE: 8
@@ -35,6 +40,7 @@
  */
 #include "slsimlib.h"
 #include "particle_halo.h"
+#include "sersic_source.h"
 #include "gridmap.h"
 #include "oracle.h"
 
@@ -271,6 +277,26 @@ int main() {
       }
       write_arr(out, o);
       write_time(tf, secs);
+    } else if (cmd == "sourcesb") {
+      int kind;
+      double p[7];
+      std::string yf, out;
+      size_t n;
+      in >> kind >> p[0] >> p[1] >> p[2] >> p[3] >> p[4] >> p[5] >> p[6] >> yf >> n >> out;
+      std::unique_ptr<Source> src;
+      if (kind == 0) {
+        src.reset(new SourceUniform(Point_2d(p[0], p[1]), 1.0, p[2]));
+      } else if (kind == 1) {
+        src.reset(new SourceGaussian(Point_2d(p[0], p[1]), p[2], 1.0, -1, 0));
+      } else {
+        SourceSersic *ss = new SourceSersic(p[2], p[3], p[4], p[5], p[6], 1.0, 0.0, Band::NoBand);
+        ss->setTheta(p[0], p[1]);
+        src.reset(ss);
+      }
+      std::vector<double> y = read_arr<double>(yf, 2 * n), o(n + 1);
+      for (size_t i = 0; i < n; ++i) o[i] = src->SurfaceBrightness(&y[2 * i]);
+      o[n] = src->getTotalFlux();
+      write_arr(out, o);
     } else if (cmd == "fieldplane") {
       std::string hf, xf, out;
       size_t nh, n;

@@ -1,2 +1,6 @@
-/* Empty stand-in for an absent third-party header (oracle build only). */
+/* Stand-in for an absent third-party header (oracle build only): the NR
+   factorial that the reference's shapelet source names (never evaluated by the
+   oracle's commands). */
 #pragma once
+#include <cmath>
+inline double factrl(int n) { return std::tgamma(n + 1.0); }

@@ -58,6 +58,7 @@ EXPORTED = [
     "glb_lens_create", "glb_lens_destroy", "glb_lens_insert_halo", "glb_lens_insert_field_plane",
     "glb_lens_nplanes", "glb_lens_planes",
     "glb_lens_reset_source", "glb_lens_rayshoot", "glb_lens_rayshoot_device", "glb_gridmap", "glb_gridmap_pixelmap",
+    "glb_gridmap_surface_brightness",
     "glb_lens_last_timing", "glb_lens_count_interactions", "glb_lens_rayshoot_noalloc",
     "glb_batch_create_grids", "glb_batch_run", "glb_batch_autotune", "glb_batch_set_block", "glb_batch_info",
     "glb_batch_result", "glb_batch_destroy",
@@ -116,6 +117,8 @@ def load_library():
     L.glb_lens_rayshoot_device.argtypes = [_vp, C.c_size_t, _vp, _vp, _vp, _vp, C.c_int, _vp]
     L.glb_gridmap.argtypes = [_vp, C.c_size_t, _vp, C.c_double, _vp, _vp, C.c_int]
     L.glb_gridmap_pixelmap.argtypes = [_vp, C.c_size_t, _vp, C.c_double, C.c_int, _vp, C.c_int]
+    L.glb_gridmap_surface_brightness.argtypes = [_vp, C.c_size_t, _vp, C.c_double, C.c_int, _vp, _vp,
+                                                 C.POINTER(C.c_double), C.c_int]
     L.glb_lens_last_timing.argtypes = [_vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.glb_lens_count_interactions.argtypes = [_vp, C.c_size_t, _vp, _vp, _vp]
     L.glb_lens_rayshoot_noalloc.argtypes = [_vp, C.c_size_t, _vp, _vp, _vp, _vp, C.c_int, _vp]
@@ -463,6 +466,25 @@ def writePixelMap(lens: Lens, N1d: int, center: Sequence[float], range_: float, 
     _check(load_library().glb_gridmap_pixelmap(lens._h, int(N1d), _p(c), float(range_), int(lensvar), _p(out),
                                                precision))
     return out.reshape(int(N1d), int(N1d))
+
+
+SOURCE_UNIFORM, SOURCE_GAUSSIAN, SOURCE_SERSIC = 0, 1, 2
+
+
+def refreshSurfaceBrightnesses(lens: Lens, N1d: int, center: Sequence[float], range_: float, kind: int,
+                               params: Sequence[float], precision=PREC_FP64):
+    """GridMap(lens, N1d, center, range).RefreshSurfaceBrightnesses(&source)
+    (TreeCode_link/gridmap.cpp:174-187) on the GPU: (sb as an (N1d, N1d) map,
+    total flux).  params per kind as glb_gridmap_surface_brightness documents:
+    SOURCE_UNIFORM (x, y, radius), SOURCE_GAUSSIAN (x, y, r_size),
+    SOURCE_SERSIC (x, y, flux, Reff_arcsec, PA, index, q, sb_limit)."""
+    c = np.ascontiguousarray(center, dtype=np.float64)
+    prm = np.ascontiguousarray(params, dtype=np.float64)
+    sb = np.zeros(int(N1d) * int(N1d))
+    tot = C.c_double()
+    _check(load_library().glb_gridmap_surface_brightness(lens._h, int(N1d), _p(c), float(range_), int(kind), _p(prm),
+                                                         _p(sb), C.byref(tot), precision))
+    return sb.reshape(int(N1d), int(N1d)), tot.value
 
 
 def direct_sum_device(n: int, particles_ptr: int, inv_area: float, nrays: int, rays_ptr: int, out_ptr: int,

@@ -648,6 +648,35 @@ __global__ void k_pixelmap(const double *x, const double *y, const double *A, si
   map[i] = v;
 }
 
+// Source::SurfaceBrightness at the source-plane positions y:
+// kind 0 SourceUniform (AnalyticNSIE/source.cpp:207-209): 1 inside radius q[0];
+// kind 1 SourceGaussian (source.cpp:211-213): exp(-|y - x|^2 / q[0]) (q[0] = r^2);
+// kind 2 SourceSersic (Source/sersic.cpp:116-135) with the host-derived
+// constants q = {cosPA, sinPA, 1/q^2, flux I_n I_q I_r, bn, 1/Reff, 1/index, sb_limit}.
+struct SourceDev {
+  int kind;
+  double x, y;
+  double q[8];
+};
+__global__ void k_surface_brightness(const double *y, size_t n, SourceDev S, double *sb) {
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double d0 = y[2 * i] - S.x, d1 = y[2 * i + 1] - S.y;
+  double v;
+  if (S.kind == 0) {
+    v = (d0 * d0 + d1 * d1) < S.q[0] * S.q[0] ? 1.0 : 0.0;
+  } else if (S.kind == 1) {
+    v = exp(-(d0 * d0 + d1 * d1) / S.q[0]);
+  } else {
+    const double x0 = d0 * S.q[0] + d1 * S.q[1], x1 = d0 * S.q[1] - d1 * S.q[0];
+    double r = sqrt(x0 * x0 + x1 * x1 * S.q[2]);
+    if (r < 4.848136811e-9) r = 4.848136811e-9;
+    v = S.q[3] * exp(-S.q[4] * pow(r * S.q[5], S.q[6]));
+    if (v < S.q[7]) v = 0.0;
+  }
+  sb[i] = v;
+}
+
 inline int nblk(size_t n, int t) { return (int)((n + t - 1) / t); }
 
 }  // namespace
@@ -1527,6 +1556,66 @@ int glb_gridmap_pixelmap(glb_lens *l, size_t n1d, const double *center, double r
   CKR(cudaGetLastError());
   CKR(cudaMemcpyAsync(map, dm.p, n * sizeof(double), cudaMemcpyDeviceToHost, l->stream));
   CKR(cudaStreamSynchronize(l->stream));
+  return 0;
+}
+
+int glb_gridmap_surface_brightness(glb_lens *l, size_t n1d, const double *center, double range, int source_kind,
+                                   const double *source_params, double *sb, double *total, int precision) {
+  if (!l || !center || !source_params || !sb) return fail(GLB_ERR_ARG, "null argument");
+  if (n1d < 2) return fail(GLB_ERR_ARG, "GridMap size must be > 1 for a resolution");
+  if (range <= 0) return fail(GLB_ERR_ARG, "GridMap range is <= 0!");
+  if (precision != GLB_PREC_FP64 && precision != GLB_PREC_SPLIT) return fail(GLB_ERR_ARG, "unknown precision");
+  SourceDev S;
+  memset(&S, 0, sizeof(S));
+  S.kind = source_kind;
+  S.x = source_params[0];
+  S.y = source_params[1];
+  const double *p = source_params + 2;
+  if (source_kind == 0) {
+    S.q[0] = p[0];  // radius (radians)
+  } else if (source_kind == 1) {
+    S.q[0] = p[0] * p[0];  // source_gauss_r2 = r_size^2
+  } else if (source_kind == 2) {
+    // SourceSersic::ReSet / setReff / setSersicIndex / setAxesRatio
+    // (Source/sersic.cpp:87-113, include/sersic_source.h:62-92)
+    const double flux = p[0], reff = p[1] * 4.848136811e-6, pa = p[2], index = p[3];
+    double q = p[4];
+    if (q > 1) q = 1 / q;
+    if (!(reff > 0) || !(index > 0) || !(q > 0)) return fail(GLB_ERR_ARG, "Sersic Reff, index and q must be positive");
+    const double bn = 1.9992 * index - 0.3271;
+    const double I_n = 1. / index * pow(bn, 2 * index) / tgamma(2 * index);
+    const double I_q = 1. / q, I_r = 1. / 2. / kPi / reff / reff;
+    S.q[0] = cos(pa);
+    S.q[1] = sin(pa);
+    S.q[2] = 1. / q / q;
+    S.q[3] = flux * I_n * I_q * I_r;
+    S.q[4] = bn;
+    S.q[5] = 1. / reff;
+    S.q[6] = 1. / index;
+    S.q[7] = p[5];  // sb_limit
+  } else {
+    return fail(GLB_ERR_UNSUPPORTED, "source kind outside this library (0 uniform, 1 Gaussian, 2 Sersic)");
+  }
+  if (int rc = set_dev(l->device)) return rc;
+  const size_t n = n1d * n1d;
+  DBuf<double> dx, dy, dA, dsb;
+  CKR(dx.alloc(2 * n));
+  CKR(dy.alloc(2 * n));
+  CKR(dA.alloc(4 * n));
+  CKR(dsb.alloc(n));
+  k_grid<<<nblk(n, 256), 256, 0, l->stream>>>(n1d, center[0], center[1], range, dx.p);
+  CKR(cudaGetLastError());
+  if (int rc = rayshoot_device(l, n, dx.p, nullptr, dy.p, dA.p, precision, l->stream)) return rc;
+  k_surface_brightness<<<nblk(n, 256), 256, 0, l->stream>>>(dy.p, n, S, dsb.p);
+  CKR(cudaGetLastError());
+  CKR(cudaMemcpyAsync(sb, dsb.p, n * sizeof(double), cudaMemcpyDeviceToHost, l->stream));
+  CKR(cudaStreamSynchronize(l->stream));
+  if (total) {  // GridMap::RefreshSurfaceBrightnesses: sum in point order times resolution^2
+    const double res = range / (double)(n1d - 1), res2 = pow(res, 2);
+    double t = 0;
+    for (size_t i = 0; i < n; ++i) t += sb[i] * res2;
+    *total = t;
+  }
   return 0;
 }
 

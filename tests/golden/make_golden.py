@@ -118,6 +118,35 @@ def field_fixture():
     np.savez_compressed(os.path.join(OUT, "field_plane.npz"), **arrays)
 
 
+# (kind, the reference driver's seven numbers, glb / oracle params)
+SOURCE_CASES = (
+    (0, (1e-5, -2e-5, 2e-5, 0, 0, 0, 0), (1e-5, -2e-5, 2e-5)),
+    (1, (1e-5, -2e-5, 1.5e-5, 0, 0, 0, 0), (1e-5, -2e-5, 1.5e-5)),
+    (2, (1e-5, -2e-5, 22.0, 0.8, 0.4, 2.5, 0.7), None),  # params get the reference's total flux
+    (2, (-3e-6, 4e-6, 23.5, 0.3, -0.7, 1.0, 1.4), None),
+)
+
+
+def source_fixture():
+    """Source::SurfaceBrightness of uniform, Gaussian and two Sersic sources."""
+    y = np.random.default_rng(18).normal(0, 3e-5, (400, 2))
+    y[:3] = [[1e-5, -2e-5], [-3e-6, 4e-6], [1e-5 + 1e-9, -2e-5]]  # centres: the r clamp
+    R = H.RefDriver()
+    arrays = {"y": y}
+    for c, (kind, p7, _) in enumerate(SOURCE_CASES):
+        sb, flux = R.source_sb(kind, p7, y)
+        arrays[f"sb_{c}"] = sb
+        arrays[f"flux_{c}"] = flux
+    np.savez_compressed(os.path.join(OUT, "sources.npz"), **arrays)
+
+
+def source_params(c, flux):
+    kind, p7, prm = SOURCE_CASES[c]
+    if prm is not None:
+        return kind, prm
+    return kind, (p7[0], p7[1], flux, p7[3], p7[4], p7[5], p7[6], -1.0)  # sb_limit -1: no cut
+
+
 def lens_spec_from_fixture(d) -> synth.LensSpec:
     """Rebuilds the LensSpec of lens_small.npz (insertion order as generated)."""
     halos = []
@@ -139,4 +168,5 @@ if __name__ == "__main__":
     halo_fixture()
     lens_fixture()
     field_fixture()
+    source_fixture()
     print("golden fixtures written to", OUT)

@@ -77,6 +77,7 @@ def oracle_lib():
     L.orc_halo_field_plane.restype = _vp
     L.orc_halo_field_plane.argtypes = [_vp, C.c_int, C.c_double, C.c_double, C.c_double, C.POINTER(C.c_int)]
     L.orc_lens_add_field_plane.argtypes = [_vp, _vp]
+    L.orc_source_sb.argtypes = [C.c_int, _vp, C.c_size_t, _vp, _vp]
     _lib = L
     return L
 
@@ -223,6 +224,15 @@ class OracleLens:
             pass
 
 
+def oracle_source_sb(kind, params, y):
+    """orc_source_sb: params = {x, y, ...} as glb_gridmap_surface_brightness takes them."""
+    y = np.ascontiguousarray(y, dtype=np.float64).reshape(-1, 2)
+    p = np.ascontiguousarray(params, dtype=np.float64)
+    out = np.zeros(len(y))
+    oracle_lib().orc_source_sb(int(kind), _ptr(p), len(y), _ptr(y), _ptr(out))
+    return out
+
+
 # ------------------------------------------------------- reference driver
 def ref_available() -> bool:
     return os.path.exists(REF_BIN)
@@ -291,6 +301,16 @@ class RefDriver:
         of = self._file()
         self.run([f"fieldplane {hf} {len(rows)} {fp.z!r} {fp.sigma_back!r} {fp.inv_screening!r} {xf} {len(xx)} {of}"])
         return np.fromfile(of).reshape(-1, 7)
+
+    def source_sb(self, kind, p7, y):
+        """The reference's Source::SurfaceBrightness at source positions y ->
+        (values, total flux); p7 as the driver's sourcesb command reads them."""
+        y = np.ascontiguousarray(y, dtype=np.float64).reshape(-1, 2)
+        yf = self._file(y)
+        of = self._file()
+        self.run([f"sourcesb {kind} " + " ".join(repr(float(v)) for v in p7) + f" {yf} {len(y)} {of}"])
+        o = np.fromfile(of)
+        return o[:-1], float(o[-1])
 
     def lens_lines(self, spec: synth.LensSpec):
         lines = [f"lens {spec.zsource!r}"]

@@ -150,3 +150,32 @@ def test_pixelmap_matches_gridmap_and_oracle():
         with pytest.raises(glb.GlamerError) as ex:
             glb.writePixelMap(L, n1d, c, rng, var)
         assert ex.value.code == glb.GLB_ERR_UNSUPPORTED
+
+
+def test_surface_brightness_matches_oracle(golden):
+    """RefreshSurfaceBrightnesses on the device: each source's surface
+    brightness at the GridMap's source positions equals the oracle's (itself
+    pinned to the reference's Source::SurfaceBrightness), and the total is the
+    reference's sum of sb x resolution^2."""
+    from tests.golden.make_golden import SOURCE_CASES, source_params
+    d = golden("sources.npz")
+    spec = mixed_spec(seed=17)
+    L = glb.lens_from_spec(spec)
+    n1d, c, rng = 41, (0.0, 0.0), 50 * synth.ARCSEC
+    gm = glb.GridMap(L, n1d, c, rng)
+    for k in range(len(SOURCE_CASES)):
+        kind, prm = source_params(k, float(d[f"flux_{k}"]))
+        # put each source where the lens maps a grid point, so that it lights up
+        prm = (gm.y[n1d * n1d // 2, 0], gm.y[n1d * n1d // 2, 1]) + tuple(prm[2:])
+        sb, total = glb.refreshSurfaceBrightnesses(L, n1d, c, rng, kind, prm)
+        ref = H.oracle_source_sb(kind, prm, gm.y)
+        assert ref.max() > 0
+        np.testing.assert_allclose(sb.ravel(), ref, rtol=1e-12, atol=1e-15 * ref.max(), err_msg=str(k))
+        res2 = (rng / (n1d - 1)) ** 2
+        expect = 0.0
+        for v in sb.ravel():
+            expect += v * res2
+        assert total == expect
+    with pytest.raises(glb.GlamerError) as ex:
+        glb.refreshSurfaceBrightnesses(L, n1d, c, rng, 7, (0.0, 0.0, 1.0))
+    assert ex.value.code == glb.GLB_ERR_UNSUPPORTED

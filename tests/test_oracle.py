@@ -126,3 +126,14 @@ def test_field_plane_matches_golden(golden):
             scale = np.abs(ref).max(axis=0)
             err = np.abs(f - ref).max(axis=0) / np.where(scale > 0, scale, 1)
             assert err.max() < tol, (name, c, err)
+
+
+def test_source_surface_brightness_matches_golden(golden):
+    """Uniform, Gaussian and Sersic surface brightness against the reference's
+    Source::SurfaceBrightness (the Sersic's total flux from its magnitude)."""
+    from tests.golden.make_golden import SOURCE_CASES, source_params
+    d = golden("sources.npz")
+    for c in range(len(SOURCE_CASES)):
+        kind, prm = source_params(c, float(d[f"flux_{c}"]))
+        sb = H.oracle_source_sb(kind, prm, d["y"])
+        np.testing.assert_allclose(sb, d[f"sb_{c}"], rtol=1e-13, atol=0, err_msg=str(c))
