@@ -440,6 +440,58 @@ class Lens {
   std::unique_ptr<glb_lens, Del> l_;
 };
 
+// ------------------------------------------------------------- sources
+// The analytic sources of GridMap::RefreshSurfaceBrightnesses that the library
+// evaluates on the GPU (glb_gridmap_surface_brightness).  Constructors take
+// the reference's arguments (AnalyticNSIE/source.cpp, Source/sersic.cpp);
+// Point_2d-like positions are anything indexable by [0], [1].
+class Source {
+ public:
+  virtual ~Source() = default;
+  void setTheta(PosType x, PosType y) {
+    prm_[0] = x;
+    prm_[1] = y;
+  }
+  int kind() const { return kind_; }
+  const std::vector<double> &params() const { return prm_; }
+
+ protected:
+  int kind_ = 0;
+  std::vector<double> prm_;
+};
+
+class SourceUniform : public Source {
+ public:
+  template <class P2>
+  SourceUniform(const P2 &position, PosType /*z*/, PosType radius_in_radians) {
+    kind_ = 0;
+    prm_ = {position[0], position[1], radius_in_radians};
+  }
+};
+
+class SourceGaussian : public Source {
+ public:
+  template <class P2>
+  SourceGaussian(const P2 &position, double r_size, double /*z*/, double /*SBlimit*/, double /*zero_point*/) {
+    kind_ = 1;
+    prm_ = {position[0], position[1], r_size};
+  }
+};
+
+class SourceSersic : public Source {
+ public:
+  // SourceSersic(mag, Reff [arcsec], PA, index, q, z, zeropoint, band): the total
+  // flux is mag_to_flux(mag, zeropoint) = 10^(-0.4 (mag - zeropoint))
+  // (include/source.h:31-34); the source sits at (0, 0) until setTheta.
+  template <class BandT>
+  SourceSersic(double my_mag, double my_Reff, double my_PA, double my_index, double my_q, double /*my_z*/,
+               double my_zeropoint, BandT /*band*/) {
+    kind_ = 2;
+    const double flux = my_mag == 100 ? 0.0 : std::pow(10, -0.4 * (my_mag - my_zeropoint));
+    prm_ = {0.0, 0.0, flux, my_Reff, my_PA, my_index, my_q, -1.0};
+  }
+};
+
 // LensingVariable (include/standard.h:89-102)
 enum class LensingVariable { DELAYT, ALPHA, ALPHA1, ALPHA2, KAPPA, GAMMA, GAMMA1, GAMMA2, GAMMA3, INVMAG, PHI,
                              SurfBrightness };
@@ -508,6 +560,19 @@ class GridMap {
       }
     }
     return m;
+  }
+  // GridMap::RefreshSurfaceBrightnesses (gridmap.cpp:174-187) on the GPU for
+  // this grid's lens: per-point surface brightness into `sb` (optional) and
+  // the reference's total (sum of sb x resolution^2 in point order).
+  static double RefreshSurfaceBrightnesses(Lens *lens, unsigned long N1d, const double center[2], double range,
+                                           const Source &source, std::vector<double> *sb = nullptr,
+                                           Precision prec = Precision::FP64) {
+    std::vector<double> tmp(N1d * N1d);
+    double total = 0;
+    check(glb_gridmap_surface_brightness(lens->handle(), N1d, center, range, source.kind(), source.params().data(),
+                                         tmp.data(), &total, (int)prec));
+    if (sb) sb->swap(tmp);
+    return total;
   }
   // The same map computed on the GPU from a fresh grid (no per-point arrays
   // on the host): glb_gridmap_pixelmap.

@@ -82,7 +82,7 @@ __device__ __forceinline__ void plane_force(const PlaneDev &P, const HaloDev *ha
 }
 
 template <int PREC>
-// capped at 80 registers (3 blocks of 256 per SM) for occupancy, as k_plane_step_split
+// capped at 80 registers (3 blocks of 256 per SM) for occupancy (64 registers measured slower here)
 __global__ void __launch_bounds__(256, 3) k_batch(const Chunk *chunks, int nchunks, const LensDev *lenses,
                                                NFWTables tab, const double *xs, const unsigned *outidx,
                                                double *y, double *A, int *counter) {

@@ -569,7 +569,7 @@ __device__ __forceinline__ void tree_force(const TreeDev &T, size_t n, const dou
 __global__ void __launch_bounds__(128) k_tree_force(TreeDev T, size_t n, const double *x, double *out) {
   tree_force<GLB_PREC_FP64>(T, n, x, out);
 }
-// the FP32-arithmetic forms, capped at 80 registers as k_plane_step_split
+// the FP32-arithmetic forms, capped at 80 registers (6 blocks of 128 per SM) for occupancy
 template <int PREC>
 __global__ void __launch_bounds__(128, 6) k_tree_force_lo(TreeDev T, size_t n, const double *x, double *out) {
   tree_force<PREC>(T, n, x, out);

@@ -152,6 +152,17 @@ int main(int argc, char **argv) {
     for (size_t i = 0; i < host.size(); ++i)
       REQUIRE(std::fabs(host[i] - dev[i]) <= 1e-12 * std::fabs(host[i]) + 1e-300);
   }
+  {  // surface brightness of a Sersic source placed where the lens maps the grid centre
+    g::SourceSersic src(22.0, 0.5, 0.3, 2.0, 0.8, 2.0, 0.0, 0);
+    const size_t mid = n1d * n1d / 2;
+    src.setTheta(gm.source(mid)[0], gm.source(mid)[1]);
+    std::vector<double> sb;
+    const double total = g::GridMap::RefreshSurfaceBrightnesses(&lens, n1d, center, range, src, &sb);
+    const double res2 = std::pow(range / (n1d - 1), 2);
+    double expect = 0;
+    for (double v : sb) expect += v * res2;
+    REQUIRE(sb.size() == n1d * n1d && sb[mid] > 0 && total == expect);
+  }
   write(out + "/grid_y.bin", gy.data(), gy.size() * sizeof(double));
   write(out + "/grid_A.bin", gA.data(), gA.size() * sizeof(double));
 
