@@ -215,6 +215,22 @@ int glb_gridmap_pixelmap(glb_lens *l, size_t n1d, const double *center, double r
 int glb_gridmap_surface_brightness(glb_lens *l, size_t n1d, const double *center, double range, int source_kind,
                                    const double *source_params, double *sb, double *total, int precision);
 
+/* GridMap::AdaptiveRefreshSurfaceBrightnesses(lens, source)
+ * (TreeCode_link/gridmap.cpp:189-258), the reference's grid-refinement client
+ * that shoots one ray per rayshooterInternal call: pixels whose surface
+ * brightness differs from a neighbour's by more than 1e-4 of the total are
+ * resampled on n x n sub-grids (n = 3, 9, 27, ...) until the mean changes by
+ * less than 1e-3.  Here every pixel that refines is resampled level by level
+ * in batched GPU calls; the pass over the pixels that decides, in the
+ * reference's order, which refine and updates the running total stays on the
+ * host.  As in the reference the sub-grids are laid around each pixel's
+ * source-plane position and pixels of the first row and column never refine.
+ * At most 6 levels (n = 729) per pixel.  sb: N1d^2 refined values; *total:
+ * the returned flux.  Sources as glb_gridmap_surface_brightness. */
+int glb_gridmap_adaptive_surface_brightness(glb_lens *l, size_t n1d, const double *center, double range,
+                                            int source_kind, const double *source_params, double *sb,
+                                            double *total, int precision);
+
 /* No counterpart in the reference.  glb_lens_rayshoot_device for callers that
  * cannot allocate device memory while they shoot rays: cudaMalloc / cudaFree
  * synchronise the whole device and can fail under a memory cap, which grid

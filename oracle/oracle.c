@@ -1564,6 +1564,85 @@ void orc_lens_rayshoot(orc_lens *l, size_t n, const double *x, const double *zs,
   free(jobs);
 }
 
+/* GridMap::to_refine (TreeCode_link/gridmap.cpp:248-258).  The neighbour
+ * range is MAX<size_t>(i-1, 0) .. MIN<size_t>(i+2, N): for i = 0 (or j = 0)
+ * i - 1 wraps to the largest size_t, so pixels of the first row and column
+ * never refine. */
+static int to_refine(const double *sb, long i, long j, long N, double total, double f) {
+  double flux = sb[i + j * N];
+  size_t i0 = (size_t)(i - 1), j0 = (size_t)(j - 1); /* MAX<size_t>(., 0) is the identity */
+  size_t i1 = (size_t)(i + 2) < (size_t)N ? (size_t)(i + 2) : (size_t)N;
+  size_t j1 = (size_t)(j + 2) < (size_t)N ? (size_t)(j + 2) : (size_t)N;
+  for (size_t ii = i0; ii < i1; ++ii)
+    for (size_t jj = j0; jj < j1; ++jj)
+      if (fabs(flux - sb[ii + jj * N]) / total > f) return 1;
+  return 0;
+}
+
+/* The refinement of one pixel (gridmap.cpp:205-234): rays on an n x n
+ * sub-grid of the pixel, n = 3, 9, 27, ..., until the mean surface brightness
+ * changes by less than 1e-3; at most ORC_MAX_REFINE levels.  The sub-grid is
+ * laid around the pixel's SOURCE position (`*(i_points[k].image)`), as the
+ * reference does. */
+#define ORC_MAX_REFINE 6
+double orc_refine_pixel(orc_lens *l, const double *ysrc, double resolution, double sb0, int kind, const double *p) {
+  double ll[2] = {ysrc[0] - resolution / 2, ysrc[1] - resolution / 2};
+  double new_flux = sb0, old_flux = 0;
+  int n = 1;
+  for (int level = 0; level < ORC_MAX_REFINE && fabs(old_flux - new_flux) > 1.0e-3 * new_flux; ++level) {
+    old_flux = new_flux;
+    n *= 3;
+    double res = resolution / n;
+    size_t m = (size_t)n * n;
+    double *x = (double *)malloc(2 * m * sizeof(double)), *y = (double *)malloc(2 * m * sizeof(double));
+    double *A = (double *)malloc(4 * m * sizeof(double)), *sb = (double *)malloc(m * sizeof(double));
+    for (int u = 0; u < n; ++u)
+      for (int v = 0; v < n; ++v) {
+        x[2 * ((size_t)u * n + v)] = ll[0] + (0.5 + u) * res;
+        x[2 * ((size_t)u * n + v) + 1] = ll[1] + (0.5 + v) * res;
+      }
+    orc_lens_rayshoot(l, m, x, NULL, y, A, 0);
+    orc_source_sb(kind, p, m, y, sb);
+    new_flux = 0;
+    for (size_t k = 0; k < m; ++k) new_flux += sb[k];
+    new_flux /= n * n;
+    free(x); free(y); free(A); free(sb);
+  }
+  return new_flux;
+}
+
+/* GridMap::AdaptiveRefreshSurfaceBrightnesses (gridmap.cpp:189-246) for a grid
+ * of N1d x N1d rays: sb gets the final per-pixel surface brightness (GridMap
+ * order); returns the total flux (sum x resolution^2). */
+double orc_gridmap_adaptive_sb(orc_lens *l, size_t N1d, const double *center, double range, int kind,
+                               const double *p, double *sb) {
+  const double f = 1.0e-4;
+  size_t n = N1d * N1d;
+  double resolution = range / (N1d - 1);
+  double *x = (double *)malloc(2 * n * sizeof(double)), *y = (double *)malloc(2 * n * sizeof(double));
+  double *A = (double *)malloc(4 * n * sizeof(double));
+  orc_grid_positions(N1d, center, range, x);
+  orc_lens_rayshoot(l, n, x, NULL, y, A, 0);
+  orc_source_sb(kind, p, n, y, sb);
+  double total = 0, res2 = pow(resolution, 2);
+  for (size_t i = 0; i < n; ++i) total += sb[i] * res2; /* RefreshSurfaceBrightnesses */
+  double total_flux = total / resolution / resolution;
+  if (total_flux == 0) { free(x); free(y); free(A); return 0; }
+  for (long j = 0; j < (long)N1d; ++j) {
+    size_t k = j * N1d;
+    for (long i = 0; i < (long)N1d; ++i, ++k) {
+      if (to_refine(sb, i, j, (long)N1d, total_flux, f)) {
+        double new_flux = orc_refine_pixel(l, &y[2 * k], resolution, sb[k], kind, p);
+        total_flux -= sb[k];
+        sb[k] = new_flux;
+        total_flux += new_flux;
+      }
+    }
+  }
+  free(x); free(y); free(A);
+  return total_flux * resolution * resolution;
+}
+
 void orc_grid_positions(size_t N1d, const double *center, double range, double *x) {
   for (size_t i = 0; i < N1d * N1d; ++i) {
     if (N1d == 1) {

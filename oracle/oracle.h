@@ -131,6 +131,16 @@ void orc_lens_plane_force(orc_lens *l, int j, size_t n, const double *xx,
                           double *alpha, double *kappa, double *gamma,
                           double *phi);
 
+/* GridMap::AdaptiveRefreshSurfaceBrightnesses (gridmap.cpp:189-258): sb
+ * (N1d^2) the refined per-pixel surface brightness; returns the total flux.
+ * Refinement levels are capped at 6 (n = 729). */
+double orc_gridmap_adaptive_sb(orc_lens *l, size_t N1d, const double *center,
+                               double range, int kind, const double *p,
+                               double *sb);
+/* One pixel's refinement (sub-grid around its source position ysrc). */
+double orc_refine_pixel(orc_lens *l, const double *ysrc, double resolution,
+                        double sb0, int kind, const double *p);
+
 /* ---------------- GridMap (TreeCode_link/gridmap.cpp:93-120) ----------- */
 /* xygridpoints + PositionFromIndex (gridmap.cpp:293-321, utilities.cpp:149-158) */
 void orc_grid_positions(size_t N1d, const double *center, double range,

@@ -30,6 +30,9 @@
  *        and the source's total flux.  KIND 0 SourceUniform(Point_2d(A,B), 1, C);
  *        1 SourceGaussian(Point_2d(A,B), C, 1, -1, 0); 2 SourceSersic(mag C,
  *        Reff D arcsec, PA E, index F, q G, z 1, zeropoint 0) at (A, B).
+ *   adaptive N CX CY RANGE KIND A B C D E F G OUT
+ *        GridMap ctor + AdaptiveRefreshSurfaceBrightnesses(lens, source) with
+ *        the source of sourcesb -> OUT: the returned total flux.
  *   fieldplane HFILE NH Z SIGMA_BACK INV_SCREEN XFILE N OUT
  *        LensPlaneTree(Z, haloes, NH, SIGMA_BACK, INV_SCREEN)::force at N plane
  *        positions -> per position alpha[2] kappa gamma[3] phi.  HFILE: 8
@@ -297,6 +300,25 @@ int main() {
       for (size_t i = 0; i < n; ++i) o[i] = src->SurfaceBrightness(&y[2 * i]);
       o[n] = src->getTotalFlux();
       write_arr(out, o);
+    } else if (cmd == "adaptive") {
+      size_t N;
+      double c[2], range, p[7];
+      int kind;
+      std::string out;
+      in >> N >> c[0] >> c[1] >> range >> kind >> p[0] >> p[1] >> p[2] >> p[3] >> p[4] >> p[5] >> p[6] >> out;
+      std::unique_ptr<Source> src;
+      if (kind == 0) {
+        src.reset(new SourceUniform(Point_2d(p[0], p[1]), 1.0, p[2]));
+      } else if (kind == 1) {
+        src.reset(new SourceGaussian(Point_2d(p[0], p[1]), p[2], 1.0, -1, 0));
+      } else {
+        SourceSersic *ss = new SourceSersic(p[2], p[3], p[4], p[5], p[6], 1.0, 0.0, Band::NoBand);
+        ss->setTheta(p[0], p[1]);
+        src.reset(ss);
+      }
+      GridMap gm(lens.get(), N, c, range);
+      double total = gm.AdaptiveRefreshSurfaceBrightnesses(*lens, *src);
+      write_arr(out, std::vector<double>(1, total));
     } else if (cmd == "fieldplane") {
       std::string hf, xf, out;
       size_t nh, n;

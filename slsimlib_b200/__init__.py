@@ -58,7 +58,7 @@ EXPORTED = [
     "glb_lens_create", "glb_lens_destroy", "glb_lens_insert_halo", "glb_lens_insert_field_plane",
     "glb_lens_nplanes", "glb_lens_planes",
     "glb_lens_reset_source", "glb_lens_rayshoot", "glb_lens_rayshoot_device", "glb_gridmap", "glb_gridmap_pixelmap",
-    "glb_gridmap_surface_brightness",
+    "glb_gridmap_surface_brightness", "glb_gridmap_adaptive_surface_brightness",
     "glb_lens_last_timing", "glb_lens_count_interactions", "glb_lens_rayshoot_noalloc",
     "glb_batch_create_grids", "glb_batch_run", "glb_batch_autotune", "glb_batch_set_block", "glb_batch_info",
     "glb_batch_result", "glb_batch_destroy",
@@ -119,6 +119,8 @@ def load_library():
     L.glb_gridmap_pixelmap.argtypes = [_vp, C.c_size_t, _vp, C.c_double, C.c_int, _vp, C.c_int]
     L.glb_gridmap_surface_brightness.argtypes = [_vp, C.c_size_t, _vp, C.c_double, C.c_int, _vp, _vp,
                                                  C.POINTER(C.c_double), C.c_int]
+    L.glb_gridmap_adaptive_surface_brightness.argtypes = [_vp, C.c_size_t, _vp, C.c_double, C.c_int, _vp, _vp,
+                                                          C.POINTER(C.c_double), C.c_int]
     L.glb_lens_last_timing.argtypes = [_vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.glb_lens_count_interactions.argtypes = [_vp, C.c_size_t, _vp, _vp, _vp]
     L.glb_lens_rayshoot_noalloc.argtypes = [_vp, C.c_size_t, _vp, _vp, _vp, _vp, C.c_int, _vp]
@@ -484,6 +486,20 @@ def refreshSurfaceBrightnesses(lens: Lens, N1d: int, center: Sequence[float], ra
     tot = C.c_double()
     _check(load_library().glb_gridmap_surface_brightness(lens._h, int(N1d), _p(c), float(range_), int(kind), _p(prm),
                                                          _p(sb), C.byref(tot), precision))
+    return sb.reshape(int(N1d), int(N1d)), tot.value
+
+
+def adaptiveRefreshSurfaceBrightnesses(lens: Lens, N1d: int, center: Sequence[float], range_: float, kind: int,
+                                       params: Sequence[float], precision=PREC_FP64):
+    """GridMap(lens, N1d, center, range).AdaptiveRefreshSurfaceBrightnesses(lens,
+    source) (TreeCode_link/gridmap.cpp:189-258) with the refinement rays shot
+    in batches on the GPU: (refined sb as an (N1d, N1d) map, total flux)."""
+    c = np.ascontiguousarray(center, dtype=np.float64)
+    prm = np.ascontiguousarray(params, dtype=np.float64)
+    sb = np.zeros(int(N1d) * int(N1d))
+    tot = C.c_double()
+    _check(load_library().glb_gridmap_adaptive_surface_brightness(lens._h, int(N1d), _p(c), float(range_), int(kind),
+                                                                  _p(prm), _p(sb), C.byref(tot), precision))
     return sb.reshape(int(N1d), int(N1d)), tot.value
 
 

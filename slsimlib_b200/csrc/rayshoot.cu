@@ -1559,13 +1559,8 @@ int glb_gridmap_pixelmap(glb_lens *l, size_t n1d, const double *center, double r
   return 0;
 }
 
-int glb_gridmap_surface_brightness(glb_lens *l, size_t n1d, const double *center, double range, int source_kind,
-                                   const double *source_params, double *sb, double *total, int precision) {
-  if (!l || !center || !source_params || !sb) return fail(GLB_ERR_ARG, "null argument");
-  if (n1d < 2) return fail(GLB_ERR_ARG, "GridMap size must be > 1 for a resolution");
-  if (range <= 0) return fail(GLB_ERR_ARG, "GridMap range is <= 0!");
-  if (precision != GLB_PREC_FP64 && precision != GLB_PREC_SPLIT) return fail(GLB_ERR_ARG, "unknown precision");
-  SourceDev S;
+// The device descriptor of a Source (kind, position, derived constants).
+static int make_source_dev(int source_kind, const double *source_params, SourceDev &S) {
   memset(&S, 0, sizeof(S));
   S.kind = source_kind;
   S.x = source_params[0];
@@ -1596,6 +1591,17 @@ int glb_gridmap_surface_brightness(glb_lens *l, size_t n1d, const double *center
   } else {
     return fail(GLB_ERR_UNSUPPORTED, "source kind outside this library (0 uniform, 1 Gaussian, 2 Sersic)");
   }
+  return 0;
+}
+
+int glb_gridmap_surface_brightness(glb_lens *l, size_t n1d, const double *center, double range, int source_kind,
+                                   const double *source_params, double *sb, double *total, int precision) {
+  if (!l || !center || !source_params || !sb) return fail(GLB_ERR_ARG, "null argument");
+  if (n1d < 2) return fail(GLB_ERR_ARG, "GridMap size must be > 1 for a resolution");
+  if (range <= 0) return fail(GLB_ERR_ARG, "GridMap range is <= 0!");
+  if (precision != GLB_PREC_FP64 && precision != GLB_PREC_SPLIT) return fail(GLB_ERR_ARG, "unknown precision");
+  SourceDev S;
+  if (int rc = make_source_dev(source_kind, source_params, S)) return rc;
   if (int rc = set_dev(l->device)) return rc;
   const size_t n = n1d * n1d;
   DBuf<double> dx, dy, dA, dsb;
@@ -1616,6 +1622,143 @@ int glb_gridmap_surface_brightness(glb_lens *l, size_t n1d, const double *center
     for (size_t i = 0; i < n; ++i) t += sb[i] * res2;
     *total = t;
   }
+  return 0;
+}
+
+// GridMap::to_refine (TreeCode_link/gridmap.cpp:248-258).  The neighbour range
+// MAX<size_t>(i-1, 0) .. MIN<size_t>(i+2, N) wraps to nothing for i = 0 (and
+// j = 0): pixels of the first row and column never refine.
+static bool to_refine(const std::vector<double> &sb, long i, long j, long N, double total, double f) {
+  const double flux = sb[i + j * N];
+  const size_t i0 = (size_t)(i - 1), j0 = (size_t)(j - 1);
+  const size_t i1 = std::min<size_t>((size_t)(i + 2), (size_t)N), j1 = std::min<size_t>((size_t)(j + 2), (size_t)N);
+  for (size_t ii = i0; ii < i1; ++ii)
+    for (size_t jj = j0; jj < j1; ++jj)
+      if (std::fabs(flux - sb[ii + jj * N]) / total > f) return true;
+  return false;
+}
+
+constexpr int kMaxRefine = 6;                 // n = 3 ... 729 sub-rays per side
+constexpr size_t kRefineChunk = 4u << 20;     // sub-rays per launch
+
+// The refinement loop of gridmap.cpp:205-234 for many pixels at once, level by
+// level: every pixel still changing shoots its n x n sub-grid (laid around its
+// source position, as the reference does) in one batched call; the sub-rays'
+// surface brightness is summed per pixel on the host in the reference's (u, v)
+// order.  out[k] = refined flux of pixel P[k].
+static int refine_pixels(glb_lens *l, const std::vector<size_t> &P, const std::vector<double> &ysrc,
+                         const std::vector<double> &sb0, double resolution, const SourceDev &S, int precision,
+                         std::vector<double> &out) {
+  const size_t np = P.size();
+  std::vector<double> nf(np), of(np, 0.0);
+  for (size_t k = 0; k < np; ++k) nf[k] = sb0[P[k]];
+  int n = 1;
+  for (int level = 0; level < kMaxRefine; ++level) {
+    std::vector<size_t> act;
+    for (size_t k = 0; k < np; ++k)
+      if (std::fabs(of[k] - nf[k]) > 1.0e-3 * nf[k]) act.push_back(k);
+    if (act.empty()) break;
+    n *= 3;
+    const double res = resolution / n;
+    const size_t m = (size_t)n * n;
+    const size_t per = std::max<size_t>(1, kRefineChunk / m);  // pixels per launch
+    DBuf<double> dx, dy, dA, dsb;
+    const size_t cap = std::min(per, act.size()) * m;
+    CKR(dx.alloc(2 * cap));
+    CKR(dy.alloc(2 * cap));
+    CKR(dA.alloc(4 * cap));
+    CKR(dsb.alloc(cap));
+    std::vector<double> hx(2 * cap), hsb(cap);
+    for (size_t a0 = 0; a0 < act.size(); a0 += per) {
+      const size_t a1 = std::min(act.size(), a0 + per), cnt = (a1 - a0) * m;
+      for (size_t a = a0; a < a1; ++a) {
+        const size_t k = act[a];
+        const double ll0 = ysrc[2 * P[k]] - resolution / 2, ll1 = ysrc[2 * P[k] + 1] - resolution / 2;
+        double *x = hx.data() + 2 * (a - a0) * m;
+        for (int u = 0; u < n; ++u)
+          for (int v = 0; v < n; ++v) {
+            x[2 * ((size_t)u * n + v)] = ll0 + (0.5 + u) * res;
+            x[2 * ((size_t)u * n + v) + 1] = ll1 + (0.5 + v) * res;
+          }
+      }
+      CKR(cudaMemcpyAsync(dx.p, hx.data(), 2 * cnt * sizeof(double), cudaMemcpyHostToDevice, l->stream));
+      if (int rc = rayshoot_device(l, cnt, dx.p, nullptr, dy.p, dA.p, precision, l->stream)) return rc;
+      k_surface_brightness<<<nblk(cnt, 256), 256, 0, l->stream>>>(dy.p, cnt, S, dsb.p);
+      CKR(cudaGetLastError());
+      CKR(cudaMemcpyAsync(hsb.data(), dsb.p, cnt * sizeof(double), cudaMemcpyDeviceToHost, l->stream));
+      CKR(cudaStreamSynchronize(l->stream));
+      for (size_t a = a0; a < a1; ++a) {
+        const size_t k = act[a];
+        of[k] = nf[k];
+        double sum = 0;
+        const double *v = hsb.data() + (a - a0) * m;
+        for (size_t q = 0; q < m; ++q) sum += v[q];
+        nf[k] = sum / (n * n);
+      }
+    }
+  }
+  out = nf;
+  return 0;
+}
+
+int glb_gridmap_adaptive_surface_brightness(glb_lens *l, size_t n1d, const double *center, double range,
+                                            int source_kind, const double *source_params, double *sb_out,
+                                            double *total, int precision) {
+  if (!l || !center || !source_params || !sb_out || !total) return fail(GLB_ERR_ARG, "null argument");
+  const size_t n = n1d * n1d;
+  std::vector<double> sb(n);
+  double total0 = 0;
+  // the grid, its source positions and RefreshSurfaceBrightnesses
+  if (int rc = glb_gridmap_surface_brightness(l, n1d, center, range, source_kind, source_params, sb.data(), &total0,
+                                              precision))
+    return rc;
+  std::vector<double> ysrc(2 * n), A(4 * n);
+  if (int rc = glb_gridmap(l, n1d, center, range, ysrc.data(), A.data(), precision)) return rc;
+  SourceDev S;
+  if (int rc = make_source_dev(source_kind, source_params, S)) return rc;
+  const double resolution = range / (double)(n1d - 1);
+  double total_flux = total0 / resolution / resolution;  // gridmap.cpp:195
+  if (total_flux == 0) {
+    memcpy(sb_out, sb.data(), n * sizeof(double));
+    *total = 0;
+    return 0;
+  }
+  const double f = 1.0e-4;
+  const long N = (long)n1d;
+  // pixels that refine on the unrefined map (refined all at once on the GPU)
+  std::vector<size_t> cand;
+  for (long j = 0; j < N; ++j)
+    for (long i = 0; i < N; ++i)
+      if (to_refine(sb, i, j, N, total_flux, f)) cand.push_back((size_t)(i + j * N));
+  std::vector<double> refined;
+  if (int rc = refine_pixels(l, cand, ysrc, sb, resolution, S, precision, refined)) return rc;
+  std::vector<double> cache(n, 0.0);
+  std::vector<char> have(n, 0);
+  for (size_t k = 0; k < cand.size(); ++k) {
+    cache[cand[k]] = refined[k];
+    have[cand[k]] = 1;
+  }
+  // the reference's sequential pass: later pixels see earlier refinements
+  // and the running total (gridmap.cpp:199-239)
+  for (long j = 0; j < N; ++j) {
+    size_t k = (size_t)j * n1d;
+    for (long i = 0; i < N; ++i, ++k) {
+      if (!to_refine(sb, i, j, N, total_flux, f)) continue;
+      double nfl;
+      if (have[k]) {
+        nfl = cache[k];
+      } else {
+        std::vector<double> one;
+        if (int rc = refine_pixels(l, std::vector<size_t>{k}, ysrc, sb, resolution, S, precision, one)) return rc;
+        nfl = one[0];
+      }
+      total_flux -= sb[k];
+      sb[k] = nfl;
+      total_flux += nfl;
+    }
+  }
+  memcpy(sb_out, sb.data(), n * sizeof(double));
+  *total = total_flux * resolution * resolution;
   return 0;
 }
 

@@ -147,6 +147,37 @@ def source_params(c, flux):
     return kind, (p7[0], p7[1], flux, p7[3], p7[4], p7[5], p7[6], -1.0)  # sb_limit -1: no cut
 
 
+ADAPTIVE_N1D, ADAPTIVE_RANGE = 9, 30 * synth.ARCSEC
+
+
+def adaptive_spec():
+    return synth.LensSpec(zsource=2.0, halos=[synth.NFWHalo(3e14, 1.0, 0.4, 6.0),
+                                              synth.NSIEHalo(2e12, 0.4, 200.0, 1e-4, 0.8, 0.3, theta=(2e-6, -1e-6))])
+
+
+def adaptive_sources(ysrc):
+    """(kind, the reference driver's seven numbers, glb / oracle params) for a
+    Gaussian and an exponential Sersic source centred on a lensed grid point;
+    both are smooth on the pixel scale, so the refinement converges in a few
+    levels (the reference shoots its sub-rays one call each)."""
+    x, y = float(ysrc[0]), float(ysrc[1])
+    flux = 10 ** (-0.4 * 21.0)
+    return ((1, (x, y, 1e-4, 0, 0, 0, 0), (x, y, 1e-4)),
+            (2, (x, y, 21.0, 30.0, 0.5, 0.6, 0.8), (x, y, flux, 30.0, 0.5, 0.6, 0.8, -1.0)))
+
+
+def adaptive_fixture():
+    """GridMap::AdaptiveRefreshSurfaceBrightnesses totals from the reference."""
+    spec = adaptive_spec()
+    x = synth.grid_positions(ADAPTIVE_N1D, range_rad=ADAPTIVE_RANGE)
+    y, _ = H.OracleLens(spec).rayshoot(x)
+    ysrc = y[5 * ADAPTIVE_N1D + 4]
+    R = H.RefDriver()
+    totals = [R.adaptive(spec, ADAPTIVE_N1D, (0.0, 0.0), ADAPTIVE_RANGE, kind, p7)
+              for kind, p7, _ in adaptive_sources(ysrc)]
+    np.savez_compressed(os.path.join(OUT, "adaptive.npz"), ysrc=ysrc, totals=np.asarray(totals))
+
+
 def lens_spec_from_fixture(d) -> synth.LensSpec:
     """Rebuilds the LensSpec of lens_small.npz (insertion order as generated)."""
     halos = []
@@ -154,9 +185,9 @@ def lens_spec_from_fixture(d) -> synth.LensSpec:
     while f"plane{i}_particles" in d:
         halos.append(synth.ParticlePlane(d[f"plane{i}_particles"], float(d[f"plane{i}_z"])))
         i += 1
-    m, z, s, rc, f, pa = d["nsie"]
+    m, z, s, rc, f, pa = (float(v) for v in d["nsie"])
     halos.append(synth.NSIEHalo(m, z, s, rc, f, pa))
-    m, r, z, c, tx, ty = d["nfw"]
+    m, r, z, c, tx, ty = (float(v) for v in d["nfw"])
     halos.append(synth.NFWHalo(m, r, z, c, theta=(tx, ty)))
     return synth.LensSpec(zsource=float(d["zsource"]), halos=halos)
 
@@ -169,4 +200,5 @@ if __name__ == "__main__":
     lens_fixture()
     field_fixture()
     source_fixture()
+    adaptive_fixture()
     print("golden fixtures written to", OUT)

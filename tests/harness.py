@@ -78,6 +78,8 @@ def oracle_lib():
     L.orc_halo_field_plane.argtypes = [_vp, C.c_int, C.c_double, C.c_double, C.c_double, C.POINTER(C.c_int)]
     L.orc_lens_add_field_plane.argtypes = [_vp, _vp]
     L.orc_source_sb.argtypes = [C.c_int, _vp, C.c_size_t, _vp, _vp]
+    L.orc_gridmap_adaptive_sb.restype = C.c_double
+    L.orc_gridmap_adaptive_sb.argtypes = [_vp, C.c_size_t, _vp, C.c_double, C.c_int, _vp, _vp]
     _lib = L
     return L
 
@@ -209,6 +211,14 @@ class OracleLens:
         L.orc_lens_rayshoot(self.h, n, _ptr(x), zsp, _ptr(y), _ptr(A), threads)
         return y, A
 
+    def adaptive_sb(self, n1d, center, range_rad, kind, params):
+        """GridMap::AdaptiveRefreshSurfaceBrightnesses: (sb (n1d^2), total)."""
+        c = np.ascontiguousarray(center, dtype=np.float64)
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        sb = np.zeros(n1d * n1d)
+        tot = oracle_lib().orc_gridmap_adaptive_sb(self.h, n1d, _ptr(c), range_rad, int(kind), _ptr(p), _ptr(sb))
+        return sb, tot
+
     def plane_force(self, j: int, xx: np.ndarray) -> np.ndarray:
         L = oracle_lib()
         xx = np.ascontiguousarray(xx, dtype=np.float64).reshape(-1, 2)
@@ -311,6 +321,13 @@ class RefDriver:
         self.run([f"sourcesb {kind} " + " ".join(repr(float(v)) for v in p7) + f" {yf} {len(y)} {of}"])
         o = np.fromfile(of)
         return o[:-1], float(o[-1])
+
+    def adaptive(self, spec, n1d, center, range_rad, kind, p7):
+        """GridMap + AdaptiveRefreshSurfaceBrightnesses in the reference -> total."""
+        of = self._file()
+        self.run(self.lens_lines(spec) + [f"adaptive {n1d} {center[0]!r} {center[1]!r} {range_rad!r} {kind} " +
+                                          " ".join(repr(float(v)) for v in p7) + f" {of}"])
+        return float(np.fromfile(of)[0])
 
     def lens_lines(self, spec: synth.LensSpec):
         lines = [f"lens {spec.zsource!r}"]

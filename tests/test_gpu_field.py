@@ -179,3 +179,20 @@ def test_surface_brightness_matches_oracle(golden):
     with pytest.raises(glb.GlamerError) as ex:
         glb.refreshSurfaceBrightnesses(L, n1d, c, rng, 7, (0.0, 0.0, 1.0))
     assert ex.value.code == glb.GLB_ERR_UNSUPPORTED
+
+
+def test_adaptive_refresh_matches_oracle(golden):
+    """AdaptiveRefreshSurfaceBrightnesses with the refinement rays batched on
+    the GPU: per-pixel refined surface brightness and total against the
+    oracle's one-pixel-at-a-time restatement, on the reference-pinned case."""
+    from tests.golden.make_golden import (ADAPTIVE_N1D, ADAPTIVE_RANGE, adaptive_sources, adaptive_spec)
+    d = golden("adaptive.npz")
+    cases = [(adaptive_spec(), ADAPTIVE_N1D, ADAPTIVE_RANGE, adaptive_sources(d["ysrc"]))]
+    for spec, n1d, rng, sources in cases:
+        L = glb.lens_from_spec(spec)
+        O = H.OracleLens(spec)
+        for kind, _, prm in sources:
+            sb, tot = glb.adaptiveRefreshSurfaceBrightnesses(L, n1d, (0.0, 0.0), rng, kind, prm)
+            sbo, toto = O.adaptive_sb(n1d, (0.0, 0.0), rng, kind, prm)
+            np.testing.assert_allclose(sb.ravel(), sbo, rtol=1e-9, atol=1e-12 * np.abs(sbo).max())
+            assert abs(tot - toto) <= 1e-9 * abs(toto)

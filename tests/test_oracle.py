@@ -137,3 +137,18 @@ def test_source_surface_brightness_matches_golden(golden):
         kind, prm = source_params(c, float(d[f"flux_{c}"]))
         sb = H.oracle_source_sb(kind, prm, d["y"])
         np.testing.assert_allclose(sb, d[f"sb_{c}"], rtol=1e-13, atol=0, err_msg=str(c))
+
+
+def test_adaptive_refresh_matches_golden(golden):
+    """GridMap::AdaptiveRefreshSurfaceBrightnesses (the one-ray-per-call
+    refinement client) restated: the total flux against the reference's."""
+    from tests.golden.make_golden import (ADAPTIVE_N1D, ADAPTIVE_RANGE, adaptive_sources, adaptive_spec)
+    d = golden("adaptive.npz")
+    O = H.OracleLens(adaptive_spec())
+    for (kind, _, prm), tref in zip(adaptive_sources(d["ysrc"]), d["totals"]):
+        sb, tot = O.adaptive_sb(ADAPTIVE_N1D, (0.0, 0.0), ADAPTIVE_RANGE, kind, prm)
+        assert abs(tot - tref) <= 1e-8 * abs(tref), (kind, tot, tref)
+        # refinement happened: the refined map differs from the plain one
+        x = synth.grid_positions(ADAPTIVE_N1D, range_rad=ADAPTIVE_RANGE)
+        y, _ = O.rayshoot(x)
+        assert np.any(sb != H.oracle_source_sb(kind, prm, y))
