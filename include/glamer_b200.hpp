@@ -574,6 +574,19 @@ class GridMap {
     if (sb) sb->swap(tmp);
     return total;
   }
+  // GridMap::AdaptiveRefreshSurfaceBrightnesses (gridmap.cpp:189-258): the
+  // refinement sub-rays batched on the GPU (glb_gridmap_adaptive_surface_brightness).
+  static double AdaptiveRefreshSurfaceBrightnesses(Lens *lens, unsigned long N1d, const double center[2],
+                                                   double range, const Source &source,
+                                                   std::vector<double> *sb = nullptr,
+                                                   Precision prec = Precision::FP64) {
+    std::vector<double> tmp(N1d * N1d);
+    double total = 0;
+    check(glb_gridmap_adaptive_surface_brightness(lens->handle(), N1d, center, range, source.kind(),
+                                                  source.params().data(), tmp.data(), &total, (int)prec));
+    if (sb) sb->swap(tmp);
+    return total;
+  }
   // The same map computed on the GPU from a fresh grid (no per-point arrays
   // on the host): glb_gridmap_pixelmap.
   static std::vector<double> writePixelMapOnDevice(Lens *lens, unsigned long N1d, const double center[2],

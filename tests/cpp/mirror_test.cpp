@@ -162,6 +162,9 @@ int main(int argc, char **argv) {
     double expect = 0;
     for (double v : sb) expect += v * res2;
     REQUIRE(sb.size() == n1d * n1d && sb[mid] > 0 && total == expect);
+    std::vector<double> sba;
+    const double ta = g::GridMap::AdaptiveRefreshSurfaceBrightnesses(&lens, n1d, center, range, src, &sba);
+    REQUIRE(sba.size() == n1d * n1d && ta > 0);
   }
   write(out + "/grid_y.bin", gy.data(), gy.size() * sizeof(double));
   write(out + "/grid_A.bin", gA.data(), gA.size() * sizeof(double));
