@@ -1654,3 +1654,234 @@ void orc_grid_positions(size_t N1d, const double *center, double range, double *
     x[2 * i + 1] = center[1] + range * (1.0 * (i / N1d) / (N1d - 1) - 0.5);
   }
 }
+
+/* ================ adaptive kNN smoothing (calculate_smoothing) ========== */
+/* LensHaloParticles::calculate_smoothing (include/particle_halo.h:683-730)
+ * builds TreeSimple(pp, N, 2*Nsmooth, 3, median=true) and sets every
+ * particle's Size to NNDistance(x_i, Nsmooth+1).
+ *
+ * The tree (include/simpleTree.h:842-974, 1318-1364): a node holding more than
+ * `bucket` particles sorts them on coordinate level%3; child 1 takes the first
+ * n/2 and child 2 the rest; both inherit the parent's box except that child
+ * 1's upper and child 2's lower bound on that axis become the coordinate of
+ * the first particle of child 2.  brother links: child1 -> child2 ->
+ * parent's brother.
+ *
+ * NNDistance (simpleTree.h:483-618): descend by value to a leaf (_findleaf,
+ * :625-640: child 1 when its upper bound > x[d]); climb while the node holds
+ * fewer than Nneighbors particles (that node is `pass`); fill a max-heap with
+ * the Nneighbors smallest squared distances of pass's particles; then walk
+ * the whole tree in preorder from the top, skipping pass's subtree and any
+ * node whose box misses the interval x[dim] +- bestr on the axis its parent
+ * cut (dim = (level-1)%3), and push every leaf particle with r2 < bestr^2
+ * (bestr = sqrt(heap top) after every push/pop).  The result is the exact
+ * Nneighbors-th smallest distance, except when pass is the top node: then
+ * the walk visits leaves whose particles are already in the heap and counts
+ * them twice (happens only for N = 2*Nsmooth+1).  Squared distances are
+ * summed in double from float coordinate differences; the result is float.
+ * The reference sorts with std::sort; this restatement sorts stably, which
+ * matters only for particles with equal coordinates. */
+typedef struct {
+  size_t start, n;
+  double p1[3], p2[3];
+  int level, child1, child2, parent, brother;
+} knn_node;
+
+typedef struct {
+  knn_node *v;
+  int nn, cap;
+  unsigned *perm;
+  const orc_particle *p;
+  unsigned *tmp;
+  int bucket;
+} knn_tree;
+
+static void knn_stable_sort(knn_tree *t, size_t start, size_t n, int d) {
+  /* bottom-up merge sort of perm[start, start+n) by p[.].x[d] */
+  unsigned *a = t->perm + start, *b = t->tmp;
+  for (size_t w = 1; w < n; w *= 2) {
+    for (size_t lo = 0; lo < n; lo += 2 * w) {
+      size_t mid = lo + w < n ? lo + w : n, hi = lo + 2 * w < n ? lo + 2 * w : n;
+      size_t i = lo, j = mid, k = lo;
+      while (i < mid && j < hi)
+        b[k++] = (t->p[a[j]].x[d] < t->p[a[i]].x[d]) ? a[j++] : a[i++];
+      while (i < mid) b[k++] = a[i++];
+      while (j < hi) b[k++] = a[j++];
+    }
+    memcpy(a, b, n * sizeof(unsigned));
+  }
+}
+
+static int knn_new(knn_tree *t, size_t start, size_t n, int level, int parent,
+                   const double *p1, const double *p2) {
+  if (t->nn == t->cap) {
+    t->cap = t->cap ? 2 * t->cap : 1024;
+    t->v = (knn_node *)realloc(t->v, (size_t)t->cap * sizeof(knn_node));
+  }
+  int id = t->nn++;
+  knn_node *nd = &t->v[id];
+  nd->start = start;
+  nd->n = n;
+  nd->level = level;
+  nd->parent = parent;
+  nd->child1 = nd->child2 = nd->brother = -1;
+  memcpy(nd->p1, p1, sizeof nd->p1);
+  memcpy(nd->p2, p2, sizeof nd->p2);
+  return id;
+}
+
+/* _BuildTreeNB (simpleTree.h:882-974) */
+static void knn_build(knn_tree *t, int id) {
+  size_t start = t->v[id].start, n = t->v[id].n;
+  if (n <= (size_t)t->bucket) return;
+  int level = t->v[id].level, d = level % 3;
+  knn_stable_sort(t, start, n, d);
+  size_t cut = n / 2;
+  double xc = t->p[t->perm[start + cut]].x[d];
+  double a1[3], a2[3], b1[3], b2[3];
+  memcpy(a1, t->v[id].p1, sizeof a1);
+  memcpy(a2, t->v[id].p2, sizeof a2);
+  memcpy(b1, t->v[id].p1, sizeof b1);
+  memcpy(b2, t->v[id].p2, sizeof b2);
+  a2[d] = xc;
+  b1[d] = xc;
+  int c1 = knn_new(t, start, cut, level + 1, id, a1, a2);
+  int c2 = knn_new(t, start + cut, n - cut, level + 1, id, b1, b2);
+  t->v[id].child1 = c1;
+  t->v[id].child2 = c2;
+  t->v[c1].brother = c2;
+  t->v[c2].brother = t->v[id].brother;
+  knn_build(t, c1);
+  knn_build(t, c2);
+}
+
+/* std::priority_queue<double> (a max-heap): the walk only ever reads the top */
+typedef struct {
+  double *h;
+  size_t n;
+} knn_heap;
+
+static void heap_push(knn_heap *q, double v) {
+  size_t i = q->n++;
+  while (i > 0) {
+    size_t up = (i - 1) / 2;
+    if (q->h[up] >= v) break;
+    q->h[i] = q->h[up];
+    i = up;
+  }
+  q->h[i] = v;
+}
+
+static void heap_pop(knn_heap *q) {
+  double v = q->h[--q->n];
+  size_t i = 0;
+  for (;;) {
+    size_t c = 2 * i + 1;
+    if (c >= q->n) break;
+    if (c + 1 < q->n && q->h[c + 1] > q->h[c]) ++c;
+    if (q->h[c] <= v) break;
+    q->h[i] = q->h[c];
+    i = c;
+  }
+  if (q->n) q->h[i] = v;
+}
+
+static double knn_r2(const float *a, const float *ray) {
+  double s = 0.0;
+  for (int k = 0; k < 3; ++k) {
+    float dx = a[k] - ray[k];
+    s += (double)dx * (double)dx;
+  }
+  return s;
+}
+
+/* TreeSimple::iterator::walk (simpleTree.h:131-146); top's brother is -1 */
+static int knn_walk(const knn_tree *t, int *cur, int decend) {
+  const knn_node *c = &t->v[*cur];
+  if (decend && c->child1 >= 0) { *cur = c->child1; return 1; }
+  if (decend && c->child2 >= 0) { *cur = c->child2; return 1; }
+  if (c->brother == -1) return 0;
+  *cur = c->brother;
+  return 1;
+}
+
+static float knn_nndistance(const knn_tree *t, const float *ray, size_t K, knn_heap *q) {
+  int id = 0;
+  while (t->v[id].child1 >= 0 || t->v[id].child2 >= 0) {
+    int d = t->v[id].level % 3;
+    id = (t->v[t->v[id].child1].p2[d] > (double)ray[d]) ? t->v[id].child1 : t->v[id].child2;
+  }
+  while (t->v[id].n < K) id = t->v[id].parent;
+  const int pass = id;
+  const knn_node *pn = &t->v[pass];
+  q->n = 0;
+  size_t i = 0;
+  for (; i < K; ++i) heap_push(q, knn_r2(t->p[t->perm[pn->start + i]].x, ray));
+  for (; i < pn->n; ++i) {
+    double r2 = knn_r2(t->p[t->perm[pn->start + i]].x, ray);
+    if (r2 < q->h[0]) {
+      heap_push(q, r2);
+      heap_pop(q);
+    }
+  }
+  double bestr = sqrt(q->h[0]);
+  int cur = 0, decend = 1;
+  knn_walk(t, &cur, 1);
+  do {
+    if (cur == pass) {
+      decend = 0;
+    } else {
+      const knn_node *cb = &t->v[cur];
+      int dim = (cb->level - 1) % 3;
+      if ((ray[dim] + bestr) > cb->p1[dim] && (ray[dim] - bestr) < cb->p2[dim]) {
+        decend = 1;
+        if (cb->child1 < 0 && cb->child2 < 0) {
+          for (size_t j = 0; j < cb->n; ++j) {
+            double r2 = knn_r2(t->p[t->perm[cb->start + j]].x, ray);
+            if (r2 < bestr * bestr) {
+              heap_push(q, r2);
+              heap_pop(q);
+              bestr = sqrt(q->h[0]);
+            }
+          }
+        }
+      } else {
+        decend = 0;
+      }
+    }
+  } while (knn_walk(t, &cur, decend));
+  return (float)bestr;
+}
+
+int orc_calculate_smoothing(orc_particle *p, size_t n, int nsmooth) {
+  if (nsmooth < 1) return -1;
+  if (n <= (size_t)nsmooth + 1) return -1; /* simpleTree.h:488-492 */
+  knn_tree t;
+  memset(&t, 0, sizeof t);
+  t.p = p;
+  t.bucket = 2 * nsmooth;
+  t.perm = (unsigned *)malloc(n * sizeof(unsigned));
+  t.tmp = (unsigned *)malloc(n * sizeof(unsigned));
+  for (size_t i = 0; i < n; ++i) t.perm[i] = (unsigned)i;
+  double p1[3], p2[3];
+  for (int k = 0; k < 3; ++k) p1[k] = p2[k] = p[0].x[k];
+  for (size_t i = 0; i < n; ++i)
+    for (int k = 0; k < 3; ++k) {
+      if (p[i].x[k] < p1[k]) p1[k] = p[i].x[k];
+      if (p[i].x[k] > p2[k]) p2[k] = p[i].x[k];
+    }
+  knn_new(&t, 0, n, 0, -1, p1, p2);
+  knn_build(&t, 0);
+  const size_t K = (size_t)nsmooth + 1;
+  knn_heap q;
+  q.h = (double *)malloc((K + 1) * sizeof(double));
+  float *out = (float *)malloc(n * sizeof(float));
+  for (size_t i = 0; i < n; ++i) out[i] = knn_nndistance(&t, p[i].x, K, &q);
+  for (size_t i = 0; i < n; ++i) p[i].Size = out[i];
+  free(out);
+  free(q.h);
+  free(t.v);
+  free(t.perm);
+  free(t.tmp);
+  return 0;
+}

@@ -146,6 +146,12 @@ double orc_refine_pixel(orc_lens *l, const double *ysrc, double resolution,
 void orc_grid_positions(size_t N1d, const double *center, double range,
                         double *x);
 
+/* ---------- adaptive kNN smoothing (include/particle_halo.h:683-730) --- */
+/* Sets p[i].Size to TreeSimple::NNDistance(x_i, nsmooth+1) over a 3-d
+ * median-split tree with bucket 2*nsmooth.  Returns 0, or -1 when nsmooth < 1
+ * or n <= nsmooth+1. */
+int orc_calculate_smoothing(orc_particle *p, size_t n, int nsmooth);
+
 #ifdef __cplusplus
 }
 #endif

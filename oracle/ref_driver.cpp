@@ -40,6 +40,9 @@
  *        (a = Rsize, b = concentration), 1 = LensHaloRealNSIE (a = sigma,
  *        b = rcore, c = fratio, d = pa); each halo moved to Z with
  *        setZlensDist, as Lens::createFieldPlanes does.
+ *   smooth PFILE N NSMOOTH OUT TIMEFILE
+ *        LensHaloParticles<ParticleType<float>>::calculate_smoothing -> OUT: the
+ *        N particle sizes; TIMEFILE gets the wall seconds.
  */
 #include "slsimlib.h"
 #include "particle_halo.h"
@@ -352,6 +355,19 @@ int main() {
         std::copy(v, v + 7, &o[7 * k]);
       }
       write_arr(out, o);
+    } else if (cmd == "smooth") {
+      std::string pf, out, tf;
+      size_t n;
+      int nsmooth;
+      in >> pf >> n >> nsmooth >> out >> tf;
+      std::vector<PT> p = read_arr<PT>(pf, n);
+      auto t0 = std::chrono::steady_clock::now();
+      LensHaloParticles<PT>::calculate_smoothing(nsmooth, p.data(), n);
+      auto t1 = std::chrono::steady_clock::now();
+      std::vector<double> o(n);
+      for (size_t i = 0; i < n; ++i) o[i] = p[i].Size;
+      write_arr(out, o);
+      write_time(tf, std::chrono::duration<double>(t1 - t0).count());
     } else {
       fprintf(stderr, "glamer_ref: unknown command %s\n", cmd.c_str());
       return 2;

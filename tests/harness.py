@@ -80,6 +80,8 @@ def oracle_lib():
     L.orc_source_sb.argtypes = [C.c_int, _vp, C.c_size_t, _vp, _vp]
     L.orc_gridmap_adaptive_sb.restype = C.c_double
     L.orc_gridmap_adaptive_sb.argtypes = [_vp, C.c_size_t, _vp, C.c_double, C.c_int, _vp, _vp]
+    L.orc_calculate_smoothing.restype = C.c_int
+    L.orc_calculate_smoothing.argtypes = [_vp, C.c_size_t, C.c_int]
     _lib = L
     return L
 
@@ -243,6 +245,15 @@ def oracle_source_sb(kind, params, y):
     return out
 
 
+def oracle_smoothing(particles: np.ndarray, nsmooth: int) -> np.ndarray:
+    """orc_calculate_smoothing on a copy of the records -> the float32 sizes."""
+    p = np.array(particles, dtype=synth.PARTICLE_DTYPE, copy=True)
+    rc = oracle_lib().orc_calculate_smoothing(_ptr(p), len(p), int(nsmooth))
+    if rc != 0:
+        raise ValueError(f"orc_calculate_smoothing: {rc}")
+    return p["Size"].copy()
+
+
 # ------------------------------------------------------- reference driver
 def ref_available() -> bool:
     return os.path.exists(REF_BIN)
@@ -296,6 +307,13 @@ class RefDriver:
         self.run([cmd])
         o = np.fromfile(of)
         return o[:-3].reshape(-1, 7), tuple(o[-3:])
+
+    def smoothing(self, particles, nsmooth):
+        """LensHaloParticles::calculate_smoothing in the reference -> (sizes, seconds)."""
+        pf = self._file(np.ascontiguousarray(particles, dtype=synth.PARTICLE_DTYPE))
+        of, tf = self._file(), self._file()
+        self.run([f"smooth {pf} {len(particles)} {int(nsmooth)} {of} {tf}"])
+        return np.fromfile(of).astype(np.float32), float(np.fromfile(tf)[0])
 
     def field_plane(self, fp: "synth.FieldPlane", xx):
         """LensPlaneTree::force of a field plane at plane positions xx -> (n, 7)."""
