@@ -343,6 +343,80 @@ def run_sweep(args):
     print(json.dumps(line))
 
 
+def smoothing_particles(n, seed=31):
+    """A simulated cluster snapshot: a triaxial NFW halo (1e15 Msun, c = 4,
+    axes 1 / 0.8 / 0.6) sampled by 90 % of n particles plus 10 % uniform in its
+    bounding box (physical Mpc)."""
+    from slsimlib_b200 import synth
+    r = np.random.default_rng(seed)
+    nh = n - n // 10
+    p = synth.nfw_particles(r, nh, 1e15, 4.0, 0.3, 0.0, axis_ratios=(0.8, 0.6))
+    bg = np.zeros(n - nh, dtype=synth.PARTICLE_DTYPE)
+    lo, hi = p["x"].min(axis=0), p["x"].max(axis=0)
+    bg["x"] = r.uniform(lo, hi, size=(n - nh, 3)).astype(np.float32)
+    bg["Mass"] = p["Mass"][0]
+    return np.concatenate([p, bg])
+
+
+def run_smoothing(args):
+    """Adaptive kNN smoothing (LensHaloParticles::calculate_smoothing,
+    Nsmooth = 64) of a 4,194,304-particle cluster snapshot: particles/s with the
+    records resident in HBM (value), through the host C ABI with the records in
+    host memory (e2e), and the reference's threaded calculate_smoothing on a
+    524,288-particle snapshot of the same shape on the host cores."""
+    import torch
+    import slsimlib_b200 as glb
+    n = 4_194_304 if not args.small else 524_288
+    ns = 64
+    p = smoothing_particles(n)
+    st = torch.cuda.Stream()
+    torch.cuda.set_stream(st)
+    dev = torch.from_numpy(p.view(np.uint8).copy()).cuda()
+    out = torch.empty(n, dtype=torch.float32, device="cuda")
+    split = []
+    f = lambda: split.append(glb.calculate_smoothing_device(ns, n, dev.data_ptr(), out.data_ptr(), st.cuda_stream))
+    for _ in range(args.warmup):
+        f()
+    split.clear()
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        ms = _timed(f, st, args.steps)
+    clocks = clk.summary()
+    sort_ms = float(np.median([s[0] for s in split]))
+    search_ms = float(np.median([s[1] for s in split]))
+    # e2e: host records in, Size written back into them
+    q = p.copy()
+    glb.calculate_smoothing(ns, q)
+    t = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        glb.calculate_smoothing(ns, q)
+        t.append(time.perf_counter() - t0)
+    e2e_s = float(np.median(t))
+    assert np.array_equal(q["Size"], out.cpu().numpy())
+    line = _base_line(args, "particles/s, adaptive kNN smoothing (Nsmooth = 64)", "particles/s", n / (ms / 1e3), ms,
+                      "f32 coords, f64 distances",
+                      f"kNN smoothing of {n} particles (triaxial NFW cluster + 10% background), Nsmooth {ns}",
+                      clocks=clocks, kernels_ms={"morton_sort_and_boxes": sort_ms, "search": search_ms},
+                      # own kernels per call: bbox, Morton keys, gather, bucket boxes, log2(P) box levels, search
+                      # (the radix sort's kernels are the library's)
+                      gpu_launches=args.steps * (5 + int(np.ceil(np.log2(max(1, n // 128))))),
+                      e2e={"value": n / e2e_s, "unit": "particles/s", "h2d_bytes_per_step": 24 * n,
+                           "d2h_bytes_per_step": 4 * n})
+    if not args.no_cpu:
+        from tests import harness as H
+        if H.ref_available():
+            nc = 524_288 if not args.small else 65_536
+            pc = smoothing_particles(nc, seed=32)
+            R = H.RefDriver()
+            tf = R._file()
+            R.run([f"threads {tf}"])
+            _, secs = R.smoothing(pc, ns)
+            line["cpu_baseline"] = {"value": nc / secs, "unit": "particles/s", "cores": int(np.fromfile(tf)[0]),
+                                    "kind": "reference",
+                                    "sample": f"calculate_smoothing of a {nc}-particle snapshot of the same shape"}
+    print(json.dumps(line))
+
+
 def _random_lens_c4(seed):
     from slsimlib_b200 import synth
     r = np.random.default_rng(seed)
@@ -484,16 +558,16 @@ def main():
     ap.add_argument("--n1d", type=int, default=0,
                     help="rays per side of the light-cone grid (default 2048; a profiling size, not a bench line)")
     ap.add_argument("--workload", default="lightcone",
-                    choices=["lightcone", "single", "sweep", "batched", "served", "field"],
+                    choices=["lightcone", "single", "sweep", "batched", "served", "field", "smoothing"],
                     help="lightcone (default): the 10-plane light cone; the others are the single plane, the "
                          "precision sweep, batched uneven lenses, the served request stream and the light cone "
-                         "with field planes")
+                         "with field planes, and adaptive kNN smoothing of a particle snapshot")
     args = ap.parse_args()
     if args.impl == "ours" and args.workload != "lightcone":
         import torch
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
         return {"single": run_single, "sweep": run_sweep, "batched": run_batched, "served": run_served,
-                "field": run_field}[
+                "field": run_field, "smoothing": run_smoothing}[
             args.workload](args)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -316,6 +316,26 @@ int glb_server_destroy(glb_server *s);
  * per-plane kernels and of the whole call (CUDA events). */
 int glb_lens_last_timing(glb_lens *l, double *kernel_ms, double *total_ms);
 
+/* ---------------------------------------------- adaptive kNN smoothing */
+/* Replaces LensHaloParticles<ParticleType<float>>::calculate_smoothing(Nsmooth,
+ * pp, Npoints) (include/particle_halo.h:159-162, def :683-730): sets every
+ * particle's Size to the distance to its (nsmooth+1)-th nearest particle, the
+ * particle itself counted -- the value TreeSimple::NNDistance(x, Nsmooth+1)
+ * returns (include/simpleTree.h:483-618): squared distances summed in double
+ * from float coordinate differences, square root rounded to float.  For
+ * N = 2*nsmooth+1 the reference's walk counts some particles twice for the
+ * queries in its top node's first child; those values are reproduced too.
+ * Errors: nsmooth < 1 or n <= nsmooth+1 (the reference exits) GLB_ERR_ARG;
+ * nsmooth above about 700 GLB_ERR_UNSUPPORTED.  Synchronous; particles are
+ * host records, only their Size is written. */
+int glb_particles_smoothing(glb_particle *particles, size_t n, int nsmooth);
+/* The same on device buffers: n records at particles_dev, n floats written to
+ * size_dev, on `stream` (NULL: the legacy default stream).  Returns when the
+ * sizes are written.  ms_out (nullable, 2 floats): device milliseconds of the
+ * Morton sort and bucket boxes, and of the neighbour search. */
+int glb_particles_smoothing_device(const glb_particle *particles_dev, size_t n, int nsmooth, float *size_dev,
+                                   void *stream, float *ms_out);
+
 #ifdef __cplusplus
 }
 #endif

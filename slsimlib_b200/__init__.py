@@ -64,6 +64,7 @@ EXPORTED = [
     "glb_batch_result", "glb_batch_destroy",
     "glb_server_create", "glb_server_submit", "glb_server_wait", "glb_server_poll", "glb_server_stats",
     "glb_server_destroy",
+    "glb_particles_smoothing", "glb_particles_smoothing_device",
 ]
 
 
@@ -138,6 +139,8 @@ def load_library():
     L.glb_server_poll.argtypes = [_vp, C.c_longlong, C.POINTER(C.c_int)]
     L.glb_server_stats.argtypes = [_vp, _vp]
     L.glb_server_destroy.argtypes = [_vp]
+    L.glb_particles_smoothing.argtypes = [_vp, C.c_size_t, C.c_int]
+    L.glb_particles_smoothing_device.argtypes = [_vp, C.c_size_t, C.c_int, _vp, _vp, _vp]
     _lib = L
     return L
 
@@ -276,6 +279,30 @@ class LensHaloParticles(_Halo):
         _check(load_library().glb_halo_particles(_p(self.particles), len(self.particles), self.z, self.inv_area,
                                                  self.max_range, C.byref(h)))
         return h
+
+
+def calculate_smoothing(Nsmooth: int, pp: np.ndarray, Npoints: Optional[int] = None) -> None:
+    """LensHaloParticles<ParticleType<float>>::calculate_smoothing(Nsmooth, pp,
+    Npoints) (include/particle_halo.h:683-730) on the GPU: sets pp[i].Size, in
+    place, to the distance to the particle's Nsmooth-th nearest neighbour (the
+    (Nsmooth+1)-th nearest particle, itself counted), as
+    TreeSimple::NNDistance returns it.  Npoints (default len(pp)) smooths the
+    first Npoints records only, as the reference does for one particle type."""
+    if not isinstance(pp, np.ndarray) or pp.dtype != PARTICLE_DTYPE or not pp.flags.c_contiguous:
+        raise TypeError("pp must be a C-contiguous ParticleType<float> record array (slsimlib_b200.PARTICLE_DTYPE)")
+    n = len(pp) if Npoints is None else int(Npoints)
+    if n < 0 or n > len(pp):
+        raise ValueError("Npoints out of range")
+    _check(load_library().glb_particles_smoothing(_p(pp), n, int(Nsmooth)))
+
+
+def calculate_smoothing_device(Nsmooth: int, n: int, particles_ptr: int, size_ptr: int, stream: int = 0):
+    """glb_particles_smoothing_device on raw device pointers (n records in,
+    n floats out); returns the device milliseconds (sort + boxes, search)."""
+    ms = (C.c_float * 2)()
+    _check(load_library().glb_particles_smoothing_device(_vp(particles_ptr), int(n), int(Nsmooth), _vp(size_ptr),
+                                                         _vp(stream) if stream else None, ms))
+    return float(ms[0]), float(ms[1])
 
 
 class LensHaloNFW(_Halo):

@@ -95,6 +95,13 @@ struct HaloTreeHost {
 bool build_halo_tree(const std::vector<double> &xp, const std::vector<float> &rmax, const std::vector<float> &mass,
                      int bucket, double theta, double max_range, HaloTreeHost &out, std::string &err);
 
+// LensHaloParticles::calculate_smoothing on the device: Size of every record
+// of d_p (device, n records) written to d_size (device, n floats) as the
+// distance to the (nsmooth+1)-th nearest particle, the particle itself
+// counted.  ms_out (nullable): [0] sort and bucket boxes, [1] search, in ms.
+Status smooth_particles_device(const glb_particle_rec *d_p, size_t n, int nsmooth, float *d_size,
+                               cudaStream_t stream, float *ms_out);
+
 // Global options.
 extern int g_keep_tree_export;
 

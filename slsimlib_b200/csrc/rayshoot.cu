@@ -1865,6 +1865,39 @@ int noalloc_setup(int dev, unsigned char **out) {
 
 }  // namespace
 
+// ------------------------------------------------------ kNN smoothing
+extern "C" int glb_particles_smoothing_device(const glb_particle *particles_dev, size_t n, int nsmooth,
+                                              float *size_dev, void *stream, float *ms_out) {
+  if (n > 0 && (!particles_dev || !size_dev)) return fail(GLB_ERR_ARG, "null buffer");
+  if (int rc = need_device()) return rc;
+  Status s = smooth_particles_device(reinterpret_cast<const glb_particle_rec *>(particles_dev), n, nsmooth,
+                                     size_dev, (cudaStream_t)stream, ms_out);
+  return s.good() ? 0 : fail(s);
+}
+
+extern "C" int glb_particles_smoothing(glb_particle *particles, size_t n, int nsmooth) {
+  if (n > 0 && !particles) return fail(GLB_ERR_ARG, "null particles");
+  if (int rc = need_device()) return rc;
+  cudaStream_t st;
+  CKR(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  struct StreamGuard {
+    cudaStream_t s;
+    ~StreamGuard() { cudaStreamDestroy(s); }
+  } sg{st};
+  DBuf<glb_particle_rec> d_p;
+  DBuf<float> d_size;
+  CKR(d_p.alloc(n));
+  CKR(d_size.alloc(n));
+  if (n) CKR(cudaMemcpyAsync(d_p.p, particles, n * sizeof(glb_particle_rec), cudaMemcpyHostToDevice, st));
+  Status s = smooth_particles_device(d_p.p, n, nsmooth, d_size.p, st, nullptr);
+  if (!s.good()) return fail(s);
+  std::vector<float> sz(n);
+  CKR(cudaMemcpyAsync(sz.data(), d_size.p, n * sizeof(float), cudaMemcpyDeviceToHost, st));
+  CKR(cudaStreamSynchronize(st));
+  for (size_t i = 0; i < n; ++i) particles[i].Size = sz[i];
+  return 0;
+}
+
 extern "C" int glb_lens_rayshoot_noalloc(glb_lens *l, size_t n, const double *x_dev, const double *zs_dev,
                                          double *y_dev, double *A_dev, int precision, void *stream) {
   if (!l) return fail(GLB_ERR_ARG, "null lens");

@@ -1,0 +1,646 @@
+// Adaptive kNN smoothing of particles on the device
+// (LensHaloParticles::calculate_smoothing, include/particle_halo.h:683-730).
+//
+// The reference sets every particle's Size to TreeSimple::NNDistance(x, Nsmooth+1)
+// (include/simpleTree.h:483-618): the heap of the query's leaf (or its parent
+// when the leaf holds fewer than Nsmooth+1 particles) seeds a bound that a
+// full preorder walk of a median-split 3-d tree then tightens, so the value
+// returned is the exact (Nsmooth+1)-th smallest distance from the particle
+// (itself included), squared distances being summed in double from float
+// coordinate differences and the square root rounded to float.  One case is
+// not exact: when the node seeding the heap is the tree's top node (only
+// possible for N = 2*Nsmooth+1, for queries in the top node's first child) the
+// walk revisits the top node's two leaves and pushes their particles again.
+//
+// Here the answer is computed directly, without the reference's tree:
+//   1. particles are sorted along a 63-bit Morton curve of the bounding box
+//      and cut into buckets of S..2S-1 consecutive particles
+//      (S = 2*Nsmooth rounded up to 32);
+//   2. an implicit binary tree over the buckets carries float bounding boxes;
+//   3. one CTA per bucket: every query first takes the (Nsmooth+1)-th
+//      smallest squared distance within its own bucket as a bound; the CTA
+//      lists the buckets whose boxes lie within the largest bound of its
+//      queries; each warp then streams, per query, the listed buckets whose box
+//      lies within the query's current bound through a shared-memory buffer of
+//      squared distances below the bound, shrinking the buffer to exactly
+//      Nsmooth+1 entries (and the bound to their maximum) whenever it fills;
+//   4. the (Nsmooth+1)-th smallest entry, selected exactly on its 64-bit
+//      pattern, is the answer.
+// Box tests use the same float subtraction as the distances, so a box is
+// skipped only when every particle in it is at least the bound away in the
+// computed arithmetic.  The N = 2*Nsmooth+1 case replays the reference's walk
+// for the affected queries (k_knn_top_walk).
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+
+#include "glb_host.h"
+
+namespace glb {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kWarps = 4;         // warps per CTA in k_knn
+constexpr int kListCap = 2048;    // candidate buckets listed per CTA
+constexpr int kStack = 64;        // per-warp DFS stack (tree depth <= 31)
+
+#define CK(call)                                                                     \
+  do {                                                                               \
+    cudaError_t e_ = (call);                                                         \
+    if (e_ != cudaSuccess)                                                           \
+      return Status::err(-2, std::string("CUDA: ") + cudaGetErrorString(e_) + " at " \
+                                 + #call);                                           \
+  } while (0)
+
+__device__ __forceinline__ unsigned f2ord(float f) {
+  unsigned b = __float_as_uint(f);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__host__ __device__ inline float ord2f(unsigned u) {
+  unsigned b = (u & 0x80000000u) ? (u & 0x7fffffffu) : ~u;
+  float f;
+  memcpy(&f, &b, 4);
+  return f;
+}
+
+// Squared distance as NNDistance sums it: ((dx^2 + dy^2) + dz^2) in double
+// from float differences (each square is exact in double).
+__device__ __forceinline__ double knn_r2(float px, float py, float pz, float qx, float qy, float qz) {
+  const double dx = (double)__fsub_rn(px, qx);
+  const double dy = (double)__fsub_rn(py, qy);
+  const double dz = (double)__fsub_rn(pz, qz);
+  return __fma_rn(dz, dz, __fma_rn(dy, dy, __dmul_rn(dx, dx)));
+}
+
+// Lower bound of knn_r2 over a box: per axis the float gap, rounded like the
+// particle differences (rounding is monotone, so no particle in the box has a
+// smaller computed difference), squared and summed in the same order.
+__device__ __forceinline__ float gap1(float q, float lo, float hi) {
+  return q < lo ? __fsub_rn(lo, q) : (q > hi ? __fsub_rn(q, hi) : 0.f);
+}
+__device__ __forceinline__ double gap2_point(float qx, float qy, float qz, float4 lo, float4 hi) {
+  const double gx = gap1(qx, lo.x, hi.x), gy = gap1(qy, lo.y, hi.y), gz = gap1(qz, lo.z, hi.z);
+  return __fma_rn(gz, gz, __fma_rn(gy, gy, __dmul_rn(gx, gx)));
+}
+// Between any point of box a and any point of box b.
+__device__ __forceinline__ float gapbb(float alo, float ahi, float blo, float bhi) {
+  return ahi < blo ? __fsub_rn(blo, ahi) : (bhi < alo ? __fsub_rn(alo, bhi) : 0.f);
+}
+__device__ __forceinline__ double gap2_box(float4 alo, float4 ahi, float4 blo, float4 bhi) {
+  const double gx = gapbb(alo.x, ahi.x, blo.x, bhi.x), gy = gapbb(alo.y, ahi.y, blo.y, bhi.y),
+               gz = gapbb(alo.z, ahi.z, blo.z, bhi.z);
+  return __fma_rn(gz, gz, __fma_rn(gy, gy, __dmul_rn(gx, gx)));
+}
+
+__device__ __forceinline__ unsigned long long warp_min64(unsigned long long v) {
+  for (int o = 16; o; o >>= 1) {
+    unsigned long long w = __shfl_xor_sync(kFull, v, o);
+    v = w < v ? w : v;
+  }
+  return v;
+}
+__device__ __forceinline__ unsigned long long warp_max64(unsigned long long v) {
+  for (int o = 16; o; o >>= 1) {
+    unsigned long long w = __shfl_xor_sync(kFull, v, o);
+    v = w > v ? w : v;
+  }
+  return v;
+}
+
+// k-th smallest (1-based) of buf[0, cnt) (non-negative doubles, so the bit
+// patterns order like the values), by bitwise radix selection from the
+// highest bit in which the entries differ; stops as soon as one entry is left.
+__device__ double warp_select(const double *buf, int cnt, int k, int lane) {
+  unsigned long long lo = ~0ull, hi = 0ull;
+  for (int i = lane; i < cnt; i += 32) {
+    const unsigned long long u = __double_as_longlong(buf[i]);
+    lo = u < lo ? u : lo;
+    hi = u > hi ? u : hi;
+  }
+  lo = warp_min64(lo);
+  hi = warp_max64(hi);
+  if (lo == hi) return __longlong_as_double(lo);
+  const int top = 63 - __clzll(lo ^ hi);
+  unsigned long long above = top >= 63 ? 0ull : ~((2ull << top) - 1ull);
+  unsigned long long prefix = lo & above;
+  int act = cnt;
+  for (int b = top; b >= 0; --b) {
+    const unsigned long long bit = 1ull << b;
+    int c0 = 0;
+    for (int i = lane; i < cnt; i += 32) {
+      const unsigned long long u = __double_as_longlong(buf[i]);
+      c0 += ((u & above) == prefix) && !(u & bit);
+    }
+    c0 = (int)__reduce_add_sync(kFull, (unsigned)c0);
+    if (k <= c0) {
+      act = c0;
+    } else {
+      k -= c0;
+      prefix |= bit;
+      act -= c0;
+    }
+    above |= bit;
+    if (act == 1) {
+      unsigned long long f = 0ull;
+      for (int i = lane; i < cnt; i += 32) {
+        const unsigned long long u = __double_as_longlong(buf[i]);
+        if ((u & above) == prefix) f = u;
+      }
+      return __longlong_as_double(warp_max64(f));
+    }
+  }
+  return __longlong_as_double(prefix);
+}
+
+// Keeps exactly K entries of buf[0, cnt): all below beta (the K-th smallest)
+// and as many equal to beta as needed.  Returns K.
+__device__ int warp_compact(double *buf, int cnt, int K, double beta, int lane) {
+  int nless = 0;
+  for (int i = lane; i < cnt; i += 32) nless += buf[i] < beta;
+  nless = (int)__reduce_add_sync(kFull, (unsigned)nless);
+  const int need = K - nless;
+  int w = 0, eq = 0;
+  const unsigned lt_mask = (1u << lane) - 1u;
+  for (int base = 0; base < cnt; base += 32) {
+    const int i = base + lane;
+    const double v = i < cnt ? buf[i] : 0.0;
+    const bool less = i < cnt && v < beta, equal = i < cnt && v == beta;
+    const unsigned em = __ballot_sync(kFull, equal);
+    const bool keep = less || (equal && eq + __popc(em & lt_mask) < need);
+    const unsigned km = __ballot_sync(kFull, keep);
+    __syncwarp();
+    if (keep) buf[w + __popc(km & lt_mask)] = v;
+    __syncwarp();
+    w += __popc(km);
+    eq += __popc(em);
+  }
+  return w;
+}
+
+// ------------------------------------------------------------------ build
+__global__ void k_bbox3(const glb_particle_rec *p, size_t n, unsigned *mm) {
+  unsigned lo[3] = {kFull, kFull, kFull}, hi[3] = {0u, 0u, 0u};
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const unsigned o = f2ord(p[i].x[k]);
+      lo[k] = min(lo[k], o);
+      hi[k] = max(hi[k], o);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    lo[k] = __reduce_min_sync(kFull, lo[k]);
+    hi[k] = __reduce_max_sync(kFull, hi[k]);
+  }
+  if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      atomicMin(&mm[k], lo[k]);
+      atomicMax(&mm[3 + k], hi[k]);
+    }
+  }
+}
+
+// 21-bit integer -> every third bit of a 63-bit word.
+__device__ __forceinline__ unsigned long long spread3(unsigned v) {
+  unsigned long long x = v & 0x1fffffu;
+  x = (x | x << 32) & 0x1f00000000ffffull;
+  x = (x | x << 16) & 0x1f0000ff0000ffull;
+  x = (x | x << 8) & 0x100f00f00f00f00full;
+  x = (x | x << 4) & 0x10c30c30c30c30c3ull;
+  x = (x | x << 2) & 0x1249249249249249ull;
+  return x;
+}
+
+__global__ void k_morton3(const glb_particle_rec *p, size_t n, float3 lo, float3 scale, unsigned long long *key,
+                          unsigned *idx) {
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float c[3] = {(p[i].x[0] - lo.x) * scale.x, (p[i].x[1] - lo.y) * scale.y, (p[i].x[2] - lo.z) * scale.z};
+  unsigned q[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) q[k] = (unsigned)fminf(fmaxf(c[k], 0.f), 2097151.f);
+  key[i] = spread3(q[0]) | (spread3(q[1]) << 1) | (spread3(q[2]) << 2);
+  idx[i] = (unsigned)i;
+}
+
+__global__ void k_gather_pos(const glb_particle_rec *p, const unsigned *sidx, size_t n, float4 *pos) {
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const unsigned j = sidx[i];
+  pos[i] = make_float4(p[j].x[0], p[j].x[1], p[j].x[2], __uint_as_float(j));
+}
+
+__device__ __forceinline__ size_t bucket_start(int b, size_t n, int nb) { return (size_t)b * n / (size_t)nb; }
+
+// One warp per leaf slot of the implicit tree: the bucket's bounding box, or
+// an empty box for padding slots.
+__global__ void k_bucket_box(const float4 *pos, size_t n, int nb, int P, float4 *blo, float4 *bhi) {
+  const int b = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  if (b >= P) return;
+  float lx = INFINITY, ly = INFINITY, lz = INFINITY, hx = -INFINITY, hy = -INFINITY, hz = -INFINITY;
+  if (b < nb) {
+    const size_t s = bucket_start(b, n, nb), e = bucket_start(b + 1, n, nb);
+    for (size_t i = s + lane; i < e; i += 32) {
+      const float4 v = pos[i];
+      lx = fminf(lx, v.x);
+      ly = fminf(ly, v.y);
+      lz = fminf(lz, v.z);
+      hx = fmaxf(hx, v.x);
+      hy = fmaxf(hy, v.y);
+      hz = fmaxf(hz, v.z);
+    }
+  }
+  for (int o = 16; o; o >>= 1) {
+    lx = fminf(lx, __shfl_xor_sync(kFull, lx, o));
+    ly = fminf(ly, __shfl_xor_sync(kFull, ly, o));
+    lz = fminf(lz, __shfl_xor_sync(kFull, lz, o));
+    hx = fmaxf(hx, __shfl_xor_sync(kFull, hx, o));
+    hy = fmaxf(hy, __shfl_xor_sync(kFull, hy, o));
+    hz = fmaxf(hz, __shfl_xor_sync(kFull, hz, o));
+  }
+  if (lane == 0) {
+    blo[P + b] = make_float4(lx, ly, lz, 0.f);
+    bhi[P + b] = make_float4(hx, hy, hz, 0.f);
+  }
+}
+
+// Internal nodes [w, 2w) of the implicit tree from their children.
+__global__ void k_box_up(int w, float4 *blo, float4 *bhi) {
+  const int i = w + (int)(blockIdx.x * blockDim.x + threadIdx.x);
+  if (i >= 2 * w) return;
+  const float4 a = blo[2 * i], b = blo[2 * i + 1], c = bhi[2 * i], d = bhi[2 * i + 1];
+  blo[i] = make_float4(fminf(a.x, b.x), fminf(a.y, b.y), fminf(a.z, b.z), 0.f);
+  bhi[i] = make_float4(fmaxf(c.x, d.x), fmaxf(c.y, d.y), fmaxf(c.z, d.z), 0.f);
+}
+
+// ----------------------------------------------------------------- search
+struct KnnArgs {
+  const float4 *pos;  // Morton-sorted {x, y, z, original index}
+  const float4 *blo, *bhi;
+  size_t n;
+  int nb, P, K, cap;
+  float *size_out;    // indexed by original particle index
+  int *flags;         // [0]: CTAs whose candidate list overflowed
+};
+
+// Appends the squared distances below beta of bucket c's particles to the
+// warp's buffer, shrinking it to K entries whenever the next 32 might not fit.
+__device__ __forceinline__ void knn_visit(const KnnArgs &a, int c, float qx, float qy, float qz, double *buf,
+                                          int &cnt, double &beta, int lane) {
+  const size_t s = bucket_start(c, a.n, a.nb), e = bucket_start(c + 1, a.n, a.nb);
+  const unsigned lt_mask = (1u << lane) - 1u;
+  for (size_t base = s; base < e; base += 32) {
+    if (cnt + 32 > a.cap) {
+      beta = warp_select(buf, cnt, a.K, lane);
+      cnt = warp_compact(buf, cnt, a.K, beta, lane);
+    }
+    const size_t i = base + lane;
+    double r2 = 0.0;
+    bool keep = false;
+    if (i < e) {
+      const float4 v = a.pos[i];
+      r2 = knn_r2(v.x, v.y, v.z, qx, qy, qz);
+      keep = r2 < beta;
+    }
+    const unsigned m = __ballot_sync(kFull, keep);
+    if (keep) buf[cnt + __popc(m & lt_mask)] = r2;
+    cnt += __popc(m);
+    __syncwarp();
+  }
+}
+
+__global__ void __launch_bounds__(kWarps * 32) k_knn(KnnArgs a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int b = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const size_t s0 = bucket_start(b, a.n, a.nb);
+  const int m = (int)(bucket_start(b + 1, a.n, a.nb) - s0);
+  const int mmax = (int)((a.n + a.nb - 1) / a.nb);
+  float4 *own = reinterpret_cast<float4 *>(smem);
+  double *qbeta = reinterpret_cast<double *>(own + mmax);
+  double *buf = qbeta + mmax + (size_t)warp * a.cap;
+  int *list = reinterpret_cast<int *>(qbeta + mmax + (size_t)kWarps * a.cap);
+  int *stack = list + kListCap + warp * kStack;
+  __shared__ unsigned long long s_r2max;
+  __shared__ int s_nlist, s_overflow;
+
+  for (int i = tid; i < m; i += blockDim.x) own[i] = a.pos[s0 + i];
+  if (tid == 0) {
+    s_r2max = 0ull;
+    s_nlist = 0;
+    s_overflow = 0;
+  }
+  __syncthreads();
+
+  // 1. bound of every query from its own bucket (m >= K)
+  unsigned long long r2max = 0ull;
+  for (int q = warp; q < m; q += kWarps) {
+    const float4 x = own[q];
+    for (int i = lane; i < m; i += 32) buf[i] = knn_r2(own[i].x, own[i].y, own[i].z, x.x, x.y, x.z);
+    __syncwarp();
+    const double beta = warp_select(buf, m, a.K, lane);
+    if (lane == 0) qbeta[q] = beta;
+    const unsigned long long u = __double_as_longlong(beta);
+    r2max = u > r2max ? u : r2max;
+    __syncwarp();
+  }
+  if (lane == 0) atomicMax(&s_r2max, r2max);
+  __syncthreads();
+
+  // 2. buckets whose box lies within the largest bound of the box of this one
+  if (tid == 0) {
+    const double R2 = __longlong_as_double(s_r2max);
+    const float4 olo = a.blo[a.P + b], ohi = a.bhi[a.P + b];
+    int sp = 0, nl = 0, ovf = 0;
+    int stk[kStack];
+    stk[sp++] = 1;
+    while (sp > 0) {
+      const int node = stk[--sp];
+      if (node >= a.P) {
+        const int c = node - a.P;
+        if (c != b && c < a.nb) {
+          if (nl < kListCap) list[nl++] = c;
+          else ovf = 1;
+        }
+        continue;
+      }
+      const int c0 = 2 * node, c1 = 2 * node + 1;
+      const double g0 = gap2_box(olo, ohi, a.blo[c0], a.bhi[c0]);
+      const double g1 = gap2_box(olo, ohi, a.blo[c1], a.bhi[c1]);
+      // near child popped first
+      if (g0 <= g1) {
+        if (g1 < R2) stk[sp++] = c1;
+        if (g0 < R2) stk[sp++] = c0;
+      } else {
+        if (g0 < R2) stk[sp++] = c0;
+        if (g1 < R2) stk[sp++] = c1;
+      }
+    }
+    s_nlist = nl;
+    s_overflow = ovf;
+    if (ovf) atomicAdd(&a.flags[0], 1);
+  }
+  __syncthreads();
+  const int nlist = s_nlist;
+  const bool overflow = s_overflow != 0;
+
+  // 3. per query: own bucket below its bound, then the candidates
+  for (int q = warp; q < m; q += kWarps) {
+    const float4 x = own[q];
+    double beta = qbeta[q];
+    int cnt = 0;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    for (int base = 0; base < m; base += 32) {
+      const int i = base + lane;
+      double r2 = 0.0;
+      bool keep = false;
+      if (i < m) {
+        r2 = knn_r2(own[i].x, own[i].y, own[i].z, x.x, x.y, x.z);
+        keep = r2 <= beta;
+      }
+      const unsigned msk = __ballot_sync(kFull, keep);
+      if (keep) buf[cnt + __popc(msk & lt_mask)] = r2;
+      cnt += __popc(msk);
+    }
+    __syncwarp();
+    if (cnt > a.K) cnt = warp_compact(buf, cnt, a.K, beta, lane);
+    if (!overflow) {
+      for (int li = 0; li < nlist; ++li) {
+        const int c = list[li];
+        if (gap2_point(x.x, x.y, x.z, a.blo[a.P + c], a.bhi[a.P + c]) < beta)
+          knn_visit(a, c, x.x, x.y, x.z, buf, cnt, beta, lane);
+      }
+    } else {
+      // the list did not fit: walk the tree for this query
+      int sp = 0;
+      if (lane == 0) stack[0] = 1;
+      sp = 1;
+      __syncwarp();
+      while (sp > 0) {
+        const int node = stack[sp - 1];
+        __syncwarp();
+        --sp;
+        if (gap2_point(x.x, x.y, x.z, a.blo[node], a.bhi[node]) >= beta) continue;
+        if (node >= a.P) {
+          const int c = node - a.P;
+          if (c != b && c < a.nb) knn_visit(a, c, x.x, x.y, x.z, buf, cnt, beta, lane);
+          continue;
+        }
+        const int c0 = 2 * node, c1 = 2 * node + 1;
+        const double g0 = gap2_point(x.x, x.y, x.z, a.blo[c0], a.bhi[c0]);
+        const double g1 = gap2_point(x.x, x.y, x.z, a.blo[c1], a.bhi[c1]);
+        const int far = g0 <= g1 ? c1 : c0, near = g0 <= g1 ? c0 : c1;
+        if (lane == 0) {
+          stack[sp] = far;
+          stack[sp + 1] = near;
+        }
+        sp += 2;
+        __syncwarp();
+      }
+    }
+    const double kth = warp_select(buf, cnt, a.K, lane);
+    if (lane == 0) a.size_out[__float_as_uint(x.w)] = __double2float_rn(__dsqrt_rn(kth));
+    __syncwarp();
+  }
+}
+
+// ------------------------------------------- N = 2*Nsmooth+1: the reference's walk
+// Stable rank of every particle by x (the top node's sort order).
+__global__ void k_rank_x(const glb_particle_rec *p, int n, int *order) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float xi = p[i].x[0];
+  int r = 0;
+  for (int j = 0; j < n; ++j) {
+    const float xj = p[j].x[0];
+    r += (xj < xi) || (xj == xi && j < i);
+  }
+  order[r] = i;
+}
+
+__device__ void heap_push_d(double *h, int &n, double v) {
+  int i = n++;
+  while (i > 0) {
+    const int up = (i - 1) / 2;
+    if (h[up] >= v) break;
+    h[i] = h[up];
+    i = up;
+  }
+  h[i] = v;
+}
+__device__ void heap_pop_d(double *h, int &n) {
+  const double v = h[--n];
+  int i = 0;
+  for (;;) {
+    int c = 2 * i + 1;
+    if (c >= n) break;
+    if (c + 1 < n && h[c + 1] > h[c]) ++c;
+    if (h[c] <= v) break;
+    h[i] = h[c];
+    i = c;
+  }
+  if (n) h[i] = v;
+}
+
+// One CTA (one thread) per particle of the top node's first child: heap of
+// the top node's particles, then its two leaves pushed again in order
+// (simpleTree.h:561-615 with pass = top).
+__global__ void k_knn_top_walk(const glb_particle_rec *p, int n, int K, const int *order, float *size_out) {
+  extern __shared__ double heap[];
+  if (threadIdx.x != 0) return;
+  const int i = blockIdx.x;
+  const int cut = n / 2;
+  const float xcut = p[order[cut]].x[0], xmin = p[order[0]].x[0], xmax = p[order[n - 1]].x[0];
+  const float qx = p[i].x[0], qy = p[i].x[1], qz = p[i].x[2];
+  if (!((double)xcut > (double)qx)) return;  // _findleaf went to the second child
+  int hn = 0;
+  for (int j = 0; j < n; ++j) {
+    const glb_particle_rec &pj = p[order[j]];
+    const double r2 = knn_r2(pj.x[0], pj.x[1], pj.x[2], qx, qy, qz);
+    if (j < K) {
+      heap_push_d(heap, hn, r2);
+    } else if (r2 < heap[0]) {
+      heap_push_d(heap, hn, r2);
+      heap_pop_d(heap, hn);
+    }
+  }
+  double bestr = __dsqrt_rn(heap[0]);
+  for (int leaf = 0; leaf < 2; ++leaf) {
+    const double lo = leaf == 0 ? (double)xmin : (double)xcut, hi = leaf == 0 ? (double)xcut : (double)xmax;
+    if (!(((double)qx + bestr) > lo && ((double)qx - bestr) < hi)) continue;
+    const int s = leaf == 0 ? 0 : cut, e = leaf == 0 ? cut : n;
+    for (int j = s; j < e; ++j) {
+      const glb_particle_rec &pj = p[order[j]];
+      const double r2 = knn_r2(pj.x[0], pj.x[1], pj.x[2], qx, qy, qz);
+      if (r2 < bestr * bestr) {
+        heap_push_d(heap, hn, r2);
+        heap_pop_d(heap, hn);
+        bestr = __dsqrt_rn(heap[0]);
+      }
+    }
+  }
+  size_out[i] = __double2float_rn(bestr);
+}
+
+unsigned nblk(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
+
+}  // namespace
+
+size_t smoothing_smem_bytes(size_t n, int nsmooth) {
+  const int K = nsmooth + 1;
+  const int S = ((2 * nsmooth + 31) / 32) * 32;
+  const int nb = (int)std::max<size_t>(1, n / (size_t)S);
+  const int mmax = (int)((n + nb - 1) / nb);
+  int cap = std::max(512, std::max(mmax + 64, 2 * K + 64));
+  cap = (cap + 31) / 32 * 32;
+  return (size_t)mmax * (sizeof(float4) + sizeof(double)) + (size_t)kWarps * cap * sizeof(double) +
+         (size_t)(kListCap + kWarps * kStack) * sizeof(int);
+}
+
+Status smooth_particles_device(const glb_particle_rec *d_p, size_t n, int nsmooth, float *d_size,
+                               cudaStream_t st, float *ms_out) {
+  if (nsmooth < 1) return Status::err(-1, "Nsmooth must be >= 1");
+  if (n <= (size_t)nsmooth + 1)
+    return Status::err(-1, "number of neighbors >= total number of particles (TreeSimple::NNDistance)");
+  if (n >= (size_t)1 << 31) return Status::err(-1, "more than 2^31-1 particles");
+  const int K = nsmooth + 1;
+  const int S = ((2 * nsmooth + 31) / 32) * 32;
+  const int nb = (int)std::max<size_t>(1, n / (size_t)S);
+  int P = 1;
+  while (P < nb) P <<= 1;
+  const int mmax = (int)((n + nb - 1) / nb);
+  int cap = std::max(512, std::max(mmax + 64, 2 * K + 64));
+  cap = (cap + 31) / 32 * 32;
+  const size_t smem = smoothing_smem_bytes(n, nsmooth);
+  if (smem > 200 * 1024) return Status::err(-6, "Nsmooth too large for the shared-memory search");
+  const bool top_walk = n == 2 * (size_t)nsmooth + 1;
+  if (top_walk && (size_t)(K + 1) * sizeof(double) > 48 * 1024)
+    return Status::err(-6, "Nsmooth too large for the N = 2*Nsmooth+1 walk");
+
+  cudaEvent_t ev[3];
+  for (auto &e : ev) CK(cudaEventCreate(&e));
+  struct EvGuard {
+    cudaEvent_t *e;
+    ~EvGuard() {
+      for (int i = 0; i < 3; ++i) cudaEventDestroy(e[i]);
+    }
+  } evg{ev};
+  CK(cudaEventRecord(ev[0], st));
+
+  DBuf<unsigned> mm;
+  CK(mm.alloc(6));
+  const unsigned init[6] = {kFull, kFull, kFull, 0u, 0u, 0u};
+  CK(cudaMemcpyAsync(mm.p, init, sizeof init, cudaMemcpyHostToDevice, st));
+  k_bbox3<<<std::min<unsigned>(nblk(n, 256), 148 * 8), 256, 0, st>>>(d_p, n, mm.p);
+  unsigned hmm[6];
+  CK(cudaMemcpyAsync(hmm, mm.p, sizeof hmm, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  float3 lo, sc;
+  float l[3], sv[3];
+  for (int k = 0; k < 3; ++k) {
+    l[k] = ord2f(hmm[k]);
+    const float ext = ord2f(hmm[3 + k]) - l[k];
+    sv[k] = ext > 0.f && std::isfinite(ext) ? 2097151.f / ext : 0.f;
+  }
+  lo = make_float3(l[0], l[1], l[2]);
+  sc = make_float3(sv[0], sv[1], sv[2]);
+
+  DBuf<unsigned long long> key, key2;
+  DBuf<unsigned> idx, sidx;
+  DBuf<float4> pos, blo, bhi;
+  DBuf<int> flags;
+  CK(key.alloc(n));
+  CK(key2.alloc(n));
+  CK(idx.alloc(n));
+  CK(sidx.alloc(n));
+  CK(pos.alloc(n));
+  CK(blo.alloc(2 * (size_t)P));
+  CK(bhi.alloc(2 * (size_t)P));
+  CK(flags.alloc(1));
+  CK(cudaMemsetAsync(flags.p, 0, sizeof(int), st));
+  k_morton3<<<nblk(n, 256), 256, 0, st>>>(d_p, n, lo, sc, key.p, idx.p);
+  size_t tb = 0;
+  CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, key.p, key2.p, idx.p, sidx.p, (int)n, 0, 63, st));
+  DBuf<unsigned char> tmp;
+  CK(tmp.alloc(tb));
+  CK(cub::DeviceRadixSort::SortPairs(tmp.p, tb, key.p, key2.p, idx.p, sidx.p, (int)n, 0, 63, st));
+  k_gather_pos<<<nblk(n, 256), 256, 0, st>>>(d_p, sidx.p, n, pos.p);
+  k_bucket_box<<<nblk((size_t)P * 32, 256), 256, 0, st>>>(pos.p, n, nb, P, blo.p, bhi.p);
+  for (int w = P / 2; w >= 1; w /= 2) k_box_up<<<nblk(w, 256), 256, 0, st>>>(w, blo.p, bhi.p);
+  CK(cudaEventRecord(ev[1], st));
+
+  KnnArgs a;
+  a.pos = pos.p;
+  a.blo = blo.p;
+  a.bhi = bhi.p;
+  a.n = n;
+  a.nb = nb;
+  a.P = P;
+  a.K = K;
+  a.cap = cap;
+  a.size_out = d_size;
+  a.flags = flags.p;
+  CK(cudaFuncSetAttribute(k_knn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_knn<<<nb, kWarps * 32, smem, st>>>(a);
+  if (top_walk) {
+    DBuf<int> order;
+    CK(order.alloc(n));
+    k_rank_x<<<nblk(n, 128), 128, 0, st>>>(d_p, (int)n, order.p);
+    k_knn_top_walk<<<(unsigned)n, 32, (size_t)(K + 1) * sizeof(double), st>>>(d_p, (int)n, K, order.p, d_size);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(st));
+  }
+  CK(cudaEventRecord(ev[2], st));
+  CK(cudaGetLastError());
+  CK(cudaEventSynchronize(ev[2]));
+  if (ms_out) {
+    CK(cudaEventElapsedTime(&ms_out[0], ev[0], ev[1]));
+    CK(cudaEventElapsedTime(&ms_out[1], ev[1], ev[2]));
+  }
+  return Status::ok();
+}
+
+}  // namespace glb

@@ -6,7 +6,7 @@ oracle/Makefile from the SLsimLib tree).  Each fixture stores its inputs and
 the reference's outputs, so tests need neither the reference tree nor the
 generator at run time.
 
-    make -C oracle && python tests/golden/make_golden.py
+    make -C oracle && python tests/golden/make_golden.py [tree halos lens field sources adaptive smoothing]
 """
 from __future__ import annotations
 
@@ -178,6 +178,37 @@ def adaptive_fixture():
     np.savez_compressed(os.path.join(OUT, "adaptive.npz"), ysrc=ysrc, totals=np.asarray(totals))
 
 
+def smoothing_cases():
+    """(name, particles, Nsmooth) of the kNN smoothing fixture: clustered and
+    uniform sets, coincident particles, and N = 2*Nsmooth+1 (the reference's
+    walk counts some particles twice there)."""
+    rng = np.random.default_rng(41)
+    cases = []
+    cases.append(("nfw_500_8", synth.nfw_particles(rng, 500, 1e14, 5.0, 0.5, 0.0), 8))
+    cube = np.zeros(3000, dtype=synth.PARTICLE_DTYPE)
+    cube["x"] = rng.uniform(-1.0, 1.0, (3000, 3)).astype(np.float32)
+    cube["Mass"] = 1.0
+    cases.append(("cube_3000_16", cube, 16))
+    cases.append(("nfw_3000_64", synth.nfw_particles(rng, 3000, 1e14, 5.0, 0.5, 0.0), 64))
+    cases.append(("top_129_64", synth.nfw_particles(rng, 129, 1e14, 5.0, 0.5, 0.0), 64))
+    cases.append(("top_17_8", synth.nfw_particles(rng, 17, 1e14, 5.0, 0.5, 0.0), 8))
+    cases.append(("small_11_3", synth.nfw_particles(rng, 11, 1e14, 5.0, 0.5, 0.0), 3))
+    dup = synth.nfw_particles(rng, 200, 1e14, 5.0, 0.5, 0.0)
+    dup["x"][100:] = dup["x"][:100]
+    cases.append(("dup_200_4", dup, 4))
+    return cases
+
+
+def smoothing_fixture():
+    arrays = {}
+    for name, p, ns in smoothing_cases():
+        sizes, _ = H.RefDriver().smoothing(p, ns)
+        arrays[f"{name}_particles"] = p
+        arrays[f"{name}_sizes"] = sizes
+        arrays[f"{name}_nsmooth"] = np.int32(ns)
+    np.savez_compressed(os.path.join(OUT, "smoothing.npz"), **arrays)
+
+
 def lens_spec_from_fixture(d) -> synth.LensSpec:
     """Rebuilds the LensSpec of lens_small.npz (insertion order as generated)."""
     halos = []
@@ -195,10 +226,8 @@ def lens_spec_from_fixture(d) -> synth.LensSpec:
 if __name__ == "__main__":
     if not H.ref_available():
         sys.exit("oracle/_ref/glamer_ref missing: run `make -C oracle` where the reference tree exists")
-    tree_fixture()
-    halo_fixture()
-    lens_fixture()
-    field_fixture()
-    source_fixture()
-    adaptive_fixture()
+    fixtures = {"tree": tree_fixture, "halos": halo_fixture, "lens": lens_fixture, "field": field_fixture,
+                "sources": source_fixture, "adaptive": adaptive_fixture, "smoothing": smoothing_fixture}
+    for name in (sys.argv[1:] or fixtures):
+        fixtures[name]()
     print("golden fixtures written to", OUT)

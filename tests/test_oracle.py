@@ -152,3 +152,59 @@ def test_adaptive_refresh_matches_golden(golden):
         x = synth.grid_positions(ADAPTIVE_N1D, range_rad=ADAPTIVE_RANGE)
         y, _ = O.rayshoot(x)
         assert np.any(sb != H.oracle_source_sb(kind, prm, y))
+
+
+def smoothing_golden_cases(golden):
+    d = golden("smoothing.npz")
+    names = sorted({k[: -len("_particles")] for k in d.files if k.endswith("_particles")})
+    return [(nm, d[f"{nm}_particles"], int(d[f"{nm}_nsmooth"]), d[f"{nm}_sizes"]) for nm in names]
+
+
+def brute_kth(p, k):
+    """Distance to the k-th nearest particle (1-based, the particle itself
+    counted) with NNDistance's arithmetic: float differences, double sum."""
+    x = p["x"]
+    d2 = np.zeros((len(p), len(p)))
+    for j in range(3):
+        dx = (x[None, :, j] - x[:, None, j]).astype(np.float32).astype(np.float64)
+        d2 += dx * dx
+    return np.sqrt(np.sort(d2, axis=1)[:, k - 1]).astype(np.float32)
+
+
+def test_smoothing_matches_golden(golden):
+    """orc_calculate_smoothing reproduces calculate_smoothing bit for bit."""
+    for name, p, ns, sizes in smoothing_golden_cases(golden):
+        got = H.oracle_smoothing(p, ns)
+        assert np.array_equal(got, sizes), name
+
+
+def test_smoothing_golden_is_exact_knn_except_top_walk(golden):
+    """The reference's answer is the exact (Nsmooth+1)-th nearest distance,
+    except for N = 2*Nsmooth+1, where queries in the top node's first child
+    (x below the median) see some particles twice and get a smaller value."""
+    for name, p, ns, sizes in smoothing_golden_cases(golden):
+        exact = brute_kth(p, ns + 1)
+        if len(p) == 2 * ns + 1:
+            xs = np.sort(p["x"][:, 0])
+            first = p["x"][:, 0] < xs[len(p) // 2]
+            assert np.array_equal(sizes[~first], exact[~first]), name
+            assert np.all(sizes[first] <= exact[first]) and np.any(sizes[first] < exact[first]), name
+        else:
+            assert np.array_equal(sizes, exact), name
+
+
+def test_smoothing_oracle_errors():
+    p = synth.nfw_particles(np.random.default_rng(3), 10, 1e14, 5.0, 0.5, 0.0)
+    with pytest.raises(ValueError):
+        H.oracle_smoothing(p, 0)
+    with pytest.raises(ValueError):
+        H.oracle_smoothing(p, 9)  # N <= Nsmooth+1
+
+
+@pytest.mark.skipif(not H.ref_available(), reason="reference not compiled here")
+def test_smoothing_oracle_matches_reference_live():
+    rng = np.random.default_rng(77)
+    for n, ns in ((6000, 32), (65, 32), (2500, 1)):
+        p = synth.nfw_particles(rng, n, 3e14, 4.0, 0.3, 0.0)
+        ref, _ = H.RefDriver().smoothing(p, ns)
+        assert np.array_equal(H.oracle_smoothing(p, ns), ref), (n, ns)
