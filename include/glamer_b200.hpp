@@ -232,6 +232,24 @@ class LensHaloParticles : public LensHalo {
     return with_theta(h);
   }
 
+  // particle_halo.h:159-162 (def :683-730), on the GPU: pp[i].Size for
+  // i < Npoints becomes the distance to the (Nsmooth+1)-th nearest of the
+  // Npoints particles (itself counted), TreeSimple::NNDistance's value.
+  // Throws std::invalid_argument where the reference exits (Nsmooth < 1,
+  // Npoints <= Nsmooth+1).
+  template <class PType>
+  static void calculate_smoothing(int Nsmooth, PType *pp, size_t Npoints, bool /*verbose*/ = false) {
+    std::vector<glb_particle> v(Npoints);
+    for (size_t i = 0; i < Npoints; ++i) {
+      for (int k = 0; k < 3; ++k) v[i].x[k] = (float)pp[i].x[k];
+      v[i].Mass = (float)pp[i].Mass;
+      v[i].Size = (float)pp[i].Size;
+      v[i].type = 0;
+    }
+    check(glb_particles_smoothing(v.data(), Npoints, Nsmooth));
+    for (size_t i = 0; i < Npoints; ++i) pp[i].Size = v[i].Size;
+  }
+
  protected:
   bool overwrites() const override { return true; }
 

@@ -35,6 +35,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 
 #include "glb_host.h"
 
@@ -45,6 +46,8 @@ constexpr unsigned kFull = 0xffffffffu;
 constexpr int kWarps = 4;         // warps per CTA in k_knn
 constexpr int kListCap = 2048;    // candidate buckets listed per CTA
 constexpr int kStack = 64;        // per-warp DFS stack (tree depth <= 31)
+constexpr int kFront = 1024;      // breadth-first frontier of the candidate search
+constexpr int kSortMax = 1024;    // candidate lists up to this size are sorted near-first
 
 #define CK(call)                                                                     \
   do {                                                                               \
@@ -112,7 +115,7 @@ __device__ __forceinline__ unsigned long long warp_max64(unsigned long long v) {
 // k-th smallest (1-based) of buf[0, cnt) (non-negative doubles, so the bit
 // patterns order like the values), by bitwise radix selection from the
 // highest bit in which the entries differ; stops as soon as one entry is left.
-__device__ double warp_select(const double *buf, int cnt, int k, int lane) {
+__device__ __noinline__ double warp_select(const double *buf, int cnt, int k, int lane) {
   unsigned long long lo = ~0ull, hi = 0ull;
   for (int i = lane; i < cnt; i += 32) {
     const unsigned long long u = __double_as_longlong(buf[i]);
@@ -156,7 +159,7 @@ __device__ double warp_select(const double *buf, int cnt, int k, int lane) {
 
 // Keeps exactly K entries of buf[0, cnt): all below beta (the K-th smallest)
 // and as many equal to beta as needed.  Returns K.
-__device__ int warp_compact(double *buf, int cnt, int K, double beta, int lane) {
+__device__ __noinline__ int warp_compact(double *buf, int cnt, int K, double beta, int lane) {
   int nless = 0;
   for (int i = lane; i < cnt; i += 32) nless += buf[i] < beta;
   nless = (int)__reduce_add_sync(kFull, (unsigned)nless);
@@ -215,14 +218,17 @@ __device__ __forceinline__ unsigned long long spread3(unsigned v) {
   return x;
 }
 
-__global__ void k_morton3(const glb_particle_rec *p, size_t n, float3 lo, float3 scale, unsigned long long *key,
+__global__ void k_morton3(const glb_particle_rec *p, size_t n, const unsigned *mm, unsigned long long *key,
                           unsigned *idx) {
   const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const float c[3] = {(p[i].x[0] - lo.x) * scale.x, (p[i].x[1] - lo.y) * scale.y, (p[i].x[2] - lo.z) * scale.z};
   unsigned q[3];
 #pragma unroll
-  for (int k = 0; k < 3; ++k) q[k] = (unsigned)fminf(fmaxf(c[k], 0.f), 2097151.f);
+  for (int k = 0; k < 3; ++k) {
+    const float lo = ord2f(mm[k]), ext = ord2f(mm[3 + k]) - lo;
+    const float sc = ext > 0.f && isfinite(ext) ? 2097151.f / ext : 0.f;
+    q[k] = (unsigned)fminf(fmaxf((p[i].x[k] - lo) * sc, 0.f), 2097151.f);
+  }
   key[i] = spread3(q[0]) | (spread3(q[1]) << 1) | (spread3(q[2]) << 2);
   idx[i] = (unsigned)i;
 }
@@ -283,12 +289,15 @@ struct KnnArgs {
   const float4 *blo, *bhi;
   size_t n;
   int nb, P, K, cap;
+  int shrink_at;      // buffer size that triggers a shrink after a bucket
   float *size_out;    // indexed by original particle index
   int *flags;         // [0]: CTAs whose candidate list overflowed
 };
 
 // Appends the squared distances below beta of bucket c's particles to the
-// warp's buffer, shrinking it to K entries whenever the next 32 might not fit.
+// warp's buffer, shrinking it to K entries (and beta to their largest)
+// whenever the next 32 might not fit, and after the bucket once it holds
+// shrink_at entries, so that the bound tightens early.
 __device__ __forceinline__ void knn_visit(const KnnArgs &a, int c, float qx, float qy, float qz, double *buf,
                                           int &cnt, double &beta, int lane) {
   const size_t s = bucket_start(c, a.n, a.nb), e = bucket_start(c + 1, a.n, a.nb);
@@ -311,9 +320,16 @@ __device__ __forceinline__ void knn_visit(const KnnArgs &a, int c, float qx, flo
     cnt += __popc(m);
     __syncwarp();
   }
+  if (cnt >= a.shrink_at) {
+    beta = warp_select(buf, cnt, a.K, lane);
+    cnt = warp_compact(buf, cnt, a.K, beta, lane);
+  }
 }
 
-__global__ void __launch_bounds__(kWarps * 32) k_knn(KnnArgs a) {
+#ifndef GLB_KNN_MIN_BLOCKS
+#define GLB_KNN_MIN_BLOCKS 6
+#endif
+__global__ void __launch_bounds__(kWarps * 32, GLB_KNN_MIN_BLOCKS) k_knn(KnnArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int b = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const size_t s0 = bucket_start(b, a.n, a.nb);
@@ -324,8 +340,9 @@ __global__ void __launch_bounds__(kWarps * 32) k_knn(KnnArgs a) {
   double *buf = qbeta + mmax + (size_t)warp * a.cap;
   int *list = reinterpret_cast<int *>(qbeta + mmax + (size_t)kWarps * a.cap);
   int *stack = list + kListCap + warp * kStack;
+  int *front = list + kListCap + kWarps * kStack;
   __shared__ unsigned long long s_r2max;
-  __shared__ int s_nlist, s_overflow;
+  __shared__ int s_nlist, s_overflow, s_fn[2];
 
   for (int i = tid; i < m; i += blockDim.x) own[i] = a.pos[s0 + i];
   if (tid == 0) {
@@ -350,42 +367,77 @@ __global__ void __launch_bounds__(kWarps * 32) k_knn(KnnArgs a) {
   if (lane == 0) atomicMax(&s_r2max, r2max);
   __syncthreads();
 
-  // 2. buckets whose box lies within the largest bound of the box of this one
-  if (tid == 0) {
+  // 2. buckets whose box lies within the largest bound of the box of this one,
+  //    level by level over the implicit tree by all threads of the CTA
+  {
     const double R2 = __longlong_as_double(s_r2max);
     const float4 olo = a.blo[a.P + b], ohi = a.bhi[a.P + b];
-    int sp = 0, nl = 0, ovf = 0;
-    int stk[kStack];
-    stk[sp++] = 1;
-    while (sp > 0) {
-      const int node = stk[--sp];
-      if (node >= a.P) {
-        const int c = node - a.P;
-        if (c != b && c < a.nb) {
-          if (nl < kListCap) list[nl++] = c;
-          else ovf = 1;
-        }
-        continue;
-      }
-      const int c0 = 2 * node, c1 = 2 * node + 1;
-      const double g0 = gap2_box(olo, ohi, a.blo[c0], a.bhi[c0]);
-      const double g1 = gap2_box(olo, ohi, a.blo[c1], a.bhi[c1]);
-      // near child popped first
-      if (g0 <= g1) {
-        if (g1 < R2) stk[sp++] = c1;
-        if (g0 < R2) stk[sp++] = c0;
-      } else {
-        if (g0 < R2) stk[sp++] = c0;
-        if (g1 < R2) stk[sp++] = c1;
-      }
+    if (tid == 0) {
+      s_fn[0] = a.P > 1 ? 1 : 0;
+      s_fn[1] = 0;
+      front[0] = 1;
     }
-    s_nlist = nl;
-    s_overflow = ovf;
-    if (ovf) atomicAdd(&a.flags[0], 1);
+    __syncthreads();
+    int cur = 0;
+    for (;;) {
+      const int nf = min(s_fn[cur], kFront);
+      __syncthreads();
+      if (nf == 0) break;
+      for (int i = tid; i < nf; i += blockDim.x) {
+        const int node = front[cur * kFront + i];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int ch = 2 * node + h;
+          if (!(gap2_box(olo, ohi, a.blo[ch], a.bhi[ch]) < R2)) continue;
+          if (ch >= a.P) {
+            const int c = ch - a.P;
+            if (c == b || c >= a.nb) continue;
+            const int k = atomicAdd(&s_nlist, 1);
+            if (k < kListCap) list[k] = c;
+            else s_overflow = 1;
+          } else {
+            const int k = atomicAdd(&s_fn[cur ^ 1], 1);
+            if (k < kFront) front[(cur ^ 1) * kFront + k] = ch;
+            else s_overflow = 1;
+          }
+        }
+      }
+      if (tid == 0) s_fn[cur] = 0;
+      __syncthreads();
+      cur ^= 1;
+    }
   }
+  if (tid == 0 && s_overflow) atomicAdd(&a.flags[0], 1);
   __syncthreads();
-  const int nlist = s_nlist;
+  const int nlist = min(s_nlist, kListCap);
   const bool overflow = s_overflow != 0;
+  // near-first order (by the distance between box centres), so that the
+  // bound tightens on the first buckets visited; rank sort, ties by position
+  if (!overflow && nlist > 1 && nlist <= kSortMax) {
+    const float4 olo = a.blo[a.P + b], ohi = a.bhi[a.P + b];
+    const float ox = 0.5f * (olo.x + ohi.x), oy = 0.5f * (olo.y + ohi.y), oz = 0.5f * (olo.z + ohi.z);
+    float *key = reinterpret_cast<float *>(front);
+    int *sorted = front + kSortMax;
+    for (int i = tid; i < nlist; i += blockDim.x) {
+      const int c = list[i];
+      const float4 lo = a.blo[a.P + c], hi = a.bhi[a.P + c];
+      const float dx = 0.5f * (lo.x + hi.x) - ox, dy = 0.5f * (lo.y + hi.y) - oy, dz = 0.5f * (lo.z + hi.z) - oz;
+      key[i] = dx * dx + dy * dy + dz * dz;
+    }
+    __syncthreads();
+    for (int i = tid; i < nlist; i += blockDim.x) {
+      const float ki = key[i];
+      int r = 0;
+      for (int j = 0; j < nlist; ++j) {
+        const float kj = key[j];
+        r += (kj < ki) || (kj == ki && j < i);
+      }
+      sorted[r] = list[i];
+    }
+    __syncthreads();
+    for (int i = tid; i < nlist; i += blockDim.x) list[i] = sorted[i];
+    __syncthreads();
+  }
 
   // 3. per query: own bucket below its bound, then the candidates
   for (int q = warp; q < m; q += kWarps) {
@@ -408,10 +460,17 @@ __global__ void __launch_bounds__(kWarps * 32) k_knn(KnnArgs a) {
     __syncwarp();
     if (cnt > a.K) cnt = warp_compact(buf, cnt, a.K, beta, lane);
     if (!overflow) {
-      for (int li = 0; li < nlist; ++li) {
-        const int c = list[li];
-        if (gap2_point(x.x, x.y, x.z, a.blo[a.P + c], a.bhi[a.P + c]) < beta)
-          knn_visit(a, c, x.x, x.y, x.z, buf, cnt, beta, lane);
+      // 32 listed boxes tested at once against the current bound
+      for (int base = 0; base < nlist; base += 32) {
+        const int li = base + lane;
+        const int c = li < nlist ? list[li] : 0;
+        const bool near = li < nlist && gap2_point(x.x, x.y, x.z, a.blo[a.P + c], a.bhi[a.P + c]) < beta;
+        unsigned msk = __ballot_sync(kFull, near);
+        while (msk) {
+          const int l = __ffs(msk) - 1;
+          msk &= msk - 1;
+          knn_visit(a, __shfl_sync(kFull, c, l), x.x, x.y, x.z, buf, cnt, beta, lane);
+        }
       }
     } else {
       // the list did not fit: walk the tree for this query
@@ -537,7 +596,7 @@ size_t smoothing_smem_bytes(size_t n, int nsmooth) {
   int cap = std::max(512, std::max(mmax + 64, 2 * K + 64));
   cap = (cap + 31) / 32 * 32;
   return (size_t)mmax * (sizeof(float4) + sizeof(double)) + (size_t)kWarps * cap * sizeof(double) +
-         (size_t)(kListCap + kWarps * kStack) * sizeof(int);
+         (size_t)(kListCap + kWarps * kStack + 2 * kFront) * sizeof(int);
 }
 
 Status smooth_particles_device(const glb_particle_rec *d_p, size_t n, int nsmooth, float *d_size,
@@ -560,6 +619,39 @@ Status smooth_particles_device(const glb_particle_rec *d_p, size_t n, int nsmoot
   if (top_walk && (size_t)(K + 1) * sizeof(double) > 48 * 1024)
     return Status::err(-6, "Nsmooth too large for the N = 2*Nsmooth+1 walk");
 
+  // scratch kept between calls (grown on demand), one per device; calls on a
+  // device are serialised
+  struct Workspace {
+    std::mutex mu;
+    size_t n = 0;
+    int P = 0;
+    DBuf<unsigned long long> key, key2;
+    DBuf<unsigned> idx, sidx, mm;
+    DBuf<float4> pos, blo, bhi;
+    DBuf<int> flags;
+    DBuf<unsigned char> tmp;
+  };
+  static Workspace *wss = new Workspace[16];
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  Workspace &w = wss[dev & 15];
+  std::lock_guard<std::mutex> lock(w.mu);
+  if (w.n < n) {
+    CK(w.key.alloc(n));
+    CK(w.key2.alloc(n));
+    CK(w.idx.alloc(n));
+    CK(w.sidx.alloc(n));
+    CK(w.pos.alloc(n));
+    w.n = n;
+  }
+  if (w.P < P) {
+    CK(w.blo.alloc(2 * (size_t)P));
+    CK(w.bhi.alloc(2 * (size_t)P));
+    w.P = P;
+  }
+  if (!w.mm.p) CK(w.mm.alloc(6));
+  if (!w.flags.p) CK(w.flags.alloc(1));
+
   cudaEvent_t ev[3];
   for (auto &e : ev) CK(cudaEventCreate(&e));
   struct EvGuard {
@@ -570,59 +662,32 @@ Status smooth_particles_device(const glb_particle_rec *d_p, size_t n, int nsmoot
   } evg{ev};
   CK(cudaEventRecord(ev[0], st));
 
-  DBuf<unsigned> mm;
-  CK(mm.alloc(6));
-  const unsigned init[6] = {kFull, kFull, kFull, 0u, 0u, 0u};
-  CK(cudaMemcpyAsync(mm.p, init, sizeof init, cudaMemcpyHostToDevice, st));
-  k_bbox3<<<std::min<unsigned>(nblk(n, 256), 148 * 8), 256, 0, st>>>(d_p, n, mm.p);
-  unsigned hmm[6];
-  CK(cudaMemcpyAsync(hmm, mm.p, sizeof hmm, cudaMemcpyDeviceToHost, st));
-  CK(cudaStreamSynchronize(st));
-  float3 lo, sc;
-  float l[3], sv[3];
-  for (int k = 0; k < 3; ++k) {
-    l[k] = ord2f(hmm[k]);
-    const float ext = ord2f(hmm[3 + k]) - l[k];
-    sv[k] = ext > 0.f && std::isfinite(ext) ? 2097151.f / ext : 0.f;
-  }
-  lo = make_float3(l[0], l[1], l[2]);
-  sc = make_float3(sv[0], sv[1], sv[2]);
-
-  DBuf<unsigned long long> key, key2;
-  DBuf<unsigned> idx, sidx;
-  DBuf<float4> pos, blo, bhi;
-  DBuf<int> flags;
-  CK(key.alloc(n));
-  CK(key2.alloc(n));
-  CK(idx.alloc(n));
-  CK(sidx.alloc(n));
-  CK(pos.alloc(n));
-  CK(blo.alloc(2 * (size_t)P));
-  CK(bhi.alloc(2 * (size_t)P));
-  CK(flags.alloc(1));
-  CK(cudaMemsetAsync(flags.p, 0, sizeof(int), st));
-  k_morton3<<<nblk(n, 256), 256, 0, st>>>(d_p, n, lo, sc, key.p, idx.p);
+  static const unsigned init[6] = {kFull, kFull, kFull, 0u, 0u, 0u};
+  CK(cudaMemcpyAsync(w.mm.p, init, sizeof init, cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(w.flags.p, 0, sizeof(int), st));
+  k_bbox3<<<std::min<unsigned>(nblk(n, 256), 148 * 8), 256, 0, st>>>(d_p, n, w.mm.p);
+  k_morton3<<<nblk(n, 256), 256, 0, st>>>(d_p, n, w.mm.p, w.key.p, w.idx.p);
   size_t tb = 0;
-  CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, key.p, key2.p, idx.p, sidx.p, (int)n, 0, 63, st));
-  DBuf<unsigned char> tmp;
-  CK(tmp.alloc(tb));
-  CK(cub::DeviceRadixSort::SortPairs(tmp.p, tb, key.p, key2.p, idx.p, sidx.p, (int)n, 0, 63, st));
-  k_gather_pos<<<nblk(n, 256), 256, 0, st>>>(d_p, sidx.p, n, pos.p);
-  k_bucket_box<<<nblk((size_t)P * 32, 256), 256, 0, st>>>(pos.p, n, nb, P, blo.p, bhi.p);
-  for (int w = P / 2; w >= 1; w /= 2) k_box_up<<<nblk(w, 256), 256, 0, st>>>(w, blo.p, bhi.p);
+  CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, w.key.p, w.key2.p, w.idx.p, w.sidx.p, (int)n, 0, 63, st));
+  if (w.tmp.n < tb) CK(w.tmp.alloc(tb));
+  CK(cub::DeviceRadixSort::SortPairs(w.tmp.p, tb, w.key.p, w.key2.p, w.idx.p, w.sidx.p, (int)n, 0, 63, st));
+  k_gather_pos<<<nblk(n, 256), 256, 0, st>>>(d_p, w.sidx.p, n, w.pos.p);
+  k_bucket_box<<<nblk((size_t)P * 32, 256), 256, 0, st>>>(w.pos.p, n, nb, P, w.blo.p, w.bhi.p);
+  for (int l = P / 2; l >= 1; l /= 2) k_box_up<<<nblk(l, 256), 256, 0, st>>>(l, w.blo.p, w.bhi.p);
   CK(cudaEventRecord(ev[1], st));
 
   KnnArgs a;
-  a.pos = pos.p;
-  a.blo = blo.p;
-  a.bhi = bhi.p;
+  a.pos = w.pos.p;
+  a.blo = w.blo.p;
+  a.bhi = w.bhi.p;
   a.n = n;
   a.nb = nb;
   a.P = P;
   a.K = K;
   a.cap = cap;
+  a.shrink_at = std::min(cap - 32, 2 * K);
   a.size_out = d_size;
-  a.flags = flags.p;
+  a.flags = w.flags.p;
   CK(cudaFuncSetAttribute(k_knn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_knn<<<nb, kWarps * 32, smem, st>>>(a);
   if (top_walk) {

@@ -301,6 +301,31 @@ int main(int argc, char **argv) {
       REQUIRE(std::hypot(dx, dy) <= 1e-4 * std::hypot(ax, ay) + 1e-300);
     }
   }
+  // adaptive kNN smoothing: the static helper on the reference's particle
+  // struct writes Size only; the sizes go to the oracle comparison
+  {
+    std::vector<ref::ParticleType> sp(3000);
+    for (auto &q : sp) {
+      for (int k = 0; k < 3; ++k) q.x[k] = (float)(0.1 * grand());
+      q.Mass = 1.0f;
+      q.Size = -1.0f;
+      q.type = 7;
+    }
+    const std::vector<ref::ParticleType> before = sp;
+    g::LensHaloParticles::calculate_smoothing(16, sp.data(), sp.size());
+    for (size_t i = 0; i < sp.size(); ++i) {
+      REQUIRE(sp[i].Size > 0 && sp[i].type == 7 && sp[i].x[2] == before[i].x[2]);
+    }
+    write(out + "/smooth_in.bin", before.data(), before.size() * sizeof(ref::ParticleType));
+    write(out + "/smooth_out.bin", sp.data(), sp.size() * sizeof(ref::ParticleType));
+    bool threw = false;
+    try {
+      g::LensHaloParticles::calculate_smoothing(16, sp.data(), 17);
+    } catch (const std::invalid_argument &) {
+      threw = true;
+    }
+    REQUIRE(threw);
+  }
   std::printf("OK\n");
   return 0;
 }

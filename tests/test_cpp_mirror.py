@@ -57,3 +57,6 @@ def test_mirror_program_matches_capi_and_oracle(tmp_path):
     yo, Ao = H.OracleLens(spec).rayshoot(x)
     assert np.max(rel_err(y, yo)) < 1e-9
     assert np.max(np.abs(A - Ao)) < 1e-9
+    s_in = np.fromfile(out / "smooth_in.bin", dtype=synth.PARTICLE_DTYPE)
+    s_out = np.fromfile(out / "smooth_out.bin", dtype=synth.PARTICLE_DTYPE)
+    assert np.array_equal(s_out["Size"], H.oracle_smoothing(s_in, 16))
