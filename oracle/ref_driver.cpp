@@ -40,6 +40,15 @@
  *        (a = Rsize, b = concentration), 1 = LensHaloRealNSIE (a = sigma,
  *        b = rcore, c = fratio, d = pa); each halo moved to Z with
  *        setZlensDist, as Lens::createFieldPlanes does.
+ *   makeparticles FILE FMT NSMOOTH RECENTER OUT
+ *        MakeParticleLenses from a glmb file (FMT 0) or a csv file (FMT 3-6,
+ *        SimFileFormat::csvFMT; writes FILE_S<NSMOOTH>.glmb beside it) -> OUT: the
+ *        particle records; OUT.meta: {1, cm[3], bbox_ll[3], bbox_ur[3],
+ *        z_original, nparticles[6]}, or {0} when the constructor throws.
+ *   writesizes PFILE N NSMOOTH OUT     LensHaloParticles::writeSizes
+ *   readsizes FILE N NSMOOTH MIN_SIZE OUT
+ *        LensHaloParticles::readSizesFile -> OUT: {found, sizes[N]}, or {-1}
+ *        when it throws.
  *   smooth PFILE N NSMOOTH OUT TIMEFILE
  *        LensHaloParticles<ParticleType<float>>::calculate_smoothing -> OUT: the
  *        N particle sizes; TIMEFILE gets the wall seconds.
@@ -368,6 +377,52 @@ int main() {
       for (size_t i = 0; i < n; ++i) o[i] = p[i].Size;
       write_arr(out, o);
       write_time(tf, std::chrono::duration<double>(t1 - t0).count());
+    } else if (cmd == "makeparticles") {
+      std::string file, out;
+      int fmt, nsmooth, recenter;
+      in >> file >> fmt >> nsmooth >> recenter >> out;
+      const SimFileFormat f = fmt == 0 ? SimFileFormat::glmb
+                              : fmt == 3 ? SimFileFormat::csv3
+                              : fmt == 4 ? SimFileFormat::csv4
+                              : fmt == 5 ? SimFileFormat::csv5 : SimFileFormat::csv6;
+      std::vector<double> meta;
+      try {
+        std::unique_ptr<MakeParticleLenses> m(fmt == 0 ? new MakeParticleLenses(file, recenter != 0)
+                                                       : new MakeParticleLenses(file, f, nsmooth, recenter != 0));
+        FILE *fp = fopen(out.c_str(), "wb");
+        fwrite(m->data.data(), sizeof(PT), m->data.size(), fp);
+        fclose(fp);
+        Point_3d<> cm = m->getCenterOfMass(), lo, hi;
+        m->getBoundingBox(lo, hi);
+        meta = {1.0, cm[0], cm[1], cm[2], lo[0], lo[1], lo[2], hi[0], hi[1], hi[2], m->getZoriginal()};
+        for (size_t k : m->getnp()) meta.push_back((double)k);
+      } catch (const std::exception &e) {
+        meta = {0.0};
+      }
+      write_arr(out + ".meta", meta);
+    } else if (cmd == "writesizes") {
+      std::string pf, out;
+      size_t n;
+      int nsmooth;
+      in >> pf >> n >> nsmooth >> out;
+      std::vector<PT> p = read_arr<PT>(pf, n);
+      LensHaloParticles<PT>::writeSizes(out, nsmooth, p.data(), n);
+    } else if (cmd == "readsizes") {
+      std::string file, out;
+      size_t n;
+      int nsmooth;
+      double min_size;
+      in >> file >> n >> nsmooth >> min_size >> out;
+      std::vector<PT> p(n);
+      std::vector<double> o;
+      try {
+        const bool ok = LensHaloParticles<PT>::readSizesFile(file, p.data(), n, nsmooth, min_size);
+        o.push_back(ok ? 1.0 : 0.0);
+        for (auto &q : p) o.push_back(q.Size);
+      } catch (const std::exception &e) {
+        o = {-1.0};
+      }
+      write_arr(out, o);
     } else {
       fprintf(stderr, "glamer_ref: unknown command %s\n", cmd.c_str());
       return 2;

@@ -315,6 +315,30 @@ class RefDriver:
         self.run([f"smooth {pf} {len(particles)} {int(nsmooth)} {of} {tf}"])
         return np.fromfile(of).astype(np.float32), float(np.fromfile(tf)[0])
 
+    def make_particles(self, filename, fmt, nsmooth, recenter=False):
+        """MakeParticleLenses in the reference -> (records, meta) or (None, None)
+        when it throws; meta = {cm[3], bbox_ll[3], bbox_ur[3], z_original,
+        nparticles[6]}."""
+        of = self._file()
+        self.run([f"makeparticles {filename} {int(fmt)} {int(nsmooth)} {int(recenter)} {of}"])
+        meta = np.fromfile(of + ".meta")
+        if meta[0] == 0:
+            return None, None
+        return np.fromfile(of, dtype=synth.PARTICLE_DTYPE), meta[1:]
+
+    def write_sizes(self, particles, nsmooth, filename):
+        pf = self._file(np.ascontiguousarray(particles, dtype=synth.PARTICLE_DTYPE))
+        self.run([f"writesizes {pf} {len(particles)} {int(nsmooth)} {filename}"])
+
+    def read_sizes(self, filename, n, nsmooth, min_size):
+        """readSizesFile -> sizes, None (not found / other Nsmooth) or 'throw'."""
+        of = self._file()
+        self.run([f"readsizes {filename} {int(n)} {int(nsmooth)} {float(min_size)!r} {of}"])
+        o = np.fromfile(of)
+        if o[0] < 0:
+            return "throw"
+        return o[1:].astype(np.float32) if o[0] == 1 else None
+
     def field_plane(self, fp: "synth.FieldPlane", xx):
         """LensPlaneTree::force of a field plane at plane positions xx -> (n, 7)."""
         rows = []
