@@ -23,9 +23,13 @@
 #ifndef GLAMER_B200_HPP
 #define GLAMER_B200_HPP
 
+#include <array>
 #include <cmath>
 #include <cstddef>
+#include <cstdio>
+#include <fstream>
 #include <memory>
+#include <sstream>
 #include <stdexcept>
 #include <string>
 #include <type_traits>
@@ -237,6 +241,63 @@ class LensHaloParticles : public LensHalo {
   // Npoints particles (itself counted), TreeSimple::NNDistance's value.
   // Throws std::invalid_argument where the reference exits (Nsmooth < 1,
   // Npoints <= Nsmooth+1).
+  // particle_halo.h:734-762: "# nparticles N", "# nsmooth NS", one Size per
+  // line as std::ostream prints a float.
+  template <class PType>
+  static void writeSizes(const std::string &filename, int Nsmooth, const PType *pp, size_t Npoints) {
+    std::ofstream f(filename);
+    if (!f.is_open()) throw std::runtime_error("file writing error");
+    f << "# nparticles " << Npoints << std::endl;
+    f << "# nsmooth " << Nsmooth << std::endl;
+    for (size_t i = 0; i < Npoints; ++i) {
+      f << pp[i].Size << std::endl;
+      if (!f) throw std::runtime_error("file writing error");
+    }
+  }
+  // particle_halo.h:557-632: false when the file is missing or was made with
+  // another Nsmooth; sizes below min_size are raised to it.
+  template <class PType>
+  static bool readSizesFile(const std::string &filename, PType *pp, size_t Npoints, int Nsmooth, double min_size) {
+    std::ifstream f(filename);
+    if (!f.is_open()) return false;
+    std::string str, label;
+    int count = 0;
+    while (std::getline(f, str)) {
+      std::stringstream ss(str);
+      ss >> label;
+      if (label == "#") {
+        ss >> label;
+        if (label == "nparticles") {
+          size_t n = 0;
+          ss >> n;
+          if (n != Npoints) throw std::runtime_error("file reading error");
+          ++count;
+        }
+        if (label == "nsmooth") {
+          int ns = 0;
+          ss >> ns;
+          if (ns != Nsmooth) return false;
+          ++count;
+        }
+      } else {
+        break;
+      }
+      if (count == 2) break;
+    }
+    if (count != 2) throw std::runtime_error("file reading error");
+    size_t row = 0;
+    while (std::getline(f, str)) {
+      if (str[0] == '#') continue;
+      if (row >= Npoints) throw std::runtime_error("file reading error");
+      std::stringstream ss(str);
+      ss >> pp[row].Size;
+      if (min_size > pp[row].Size) pp[row].Size = (float)min_size;
+      ++row;
+    }
+    if (row != Npoints) throw std::runtime_error("file reading error");
+    return true;
+  }
+
   template <class PType>
   static void calculate_smoothing(int Nsmooth, PType *pp, size_t Npoints, bool /*verbose*/ = false) {
     std::vector<glb_particle> v(Npoints);
@@ -256,6 +317,179 @@ class LensHaloParticles : public LensHalo {
  private:
   std::vector<glb_particle> parts_;
   double inv_area_, max_range_;
+};
+
+// MakeParticleLenses (particle_halo.h:975-1073, particle_lens.cpp:22-341) for
+// glmb and csv3 / csv4 / csv5 files; the smoothing runs on the GPU.  Records are
+// glb_particle, the layout of ParticleType<float>.
+enum class SimFileFormat { csv3, csv4, csv5, csv6, gadget2, ascii, glmb };
+
+class MakeParticleLenses {
+ public:
+  std::vector<glb_particle> data;
+  std::vector<LensHaloParticles *> halos;
+
+  // particle_lens.cpp:22-107: glmb reads the file; csvN reads
+  // <filename>_S<Nsmooth>.glmb when it exists, else the csv file, and writes
+  // that glmb file.  csv6 and the other formats throw std::invalid_argument
+  // (the reference's switch falls through to its error branch for csv6).
+  MakeParticleLenses(const std::string &filename, SimFileFormat format, int Nsmooth, bool recenter)
+      : filename_(filename), Nsmooth_(Nsmooth) {
+    if (format == SimFileFormat::glmb) {
+      if (!readSizesB(filename, data, Nsmooth_, nparticles_, z_original_))
+        throw std::invalid_argument("Can't find file.");
+    } else {
+      const std::string sizefile = filename + "_S" + std::to_string(Nsmooth) + ".glmb";
+      std::ifstream probe(sizefile);
+      if (probe.good()) {
+        readSizesB(sizefile, data, Nsmooth_, nparticles_, z_original_);
+      } else {
+        if (format == SimFileFormat::csv3) readCSV(3);
+        else if (format == SimFileFormat::csv4) readCSV(4);
+        else if (format == SimFileFormat::csv5) readCSV(5);
+        else throw std::invalid_argument("missing format");
+        writeSizesB(sizefile, data, Nsmooth_, nparticles_, z_original_);
+      }
+    }
+    moments(false);
+    if (recenter) shift(cm_);
+  }
+  // particle_lens.cpp:109-137 (its bounding box starts at the origin)
+  MakeParticleLenses(const std::string &filename, bool recenter) : filename_(filename), Nsmooth_(0) {
+    readSizesB(filename, data, Nsmooth_, nparticles_, z_original_);
+    moments(true);
+    if (recenter) Recenter(cm_);
+  }
+  ~MakeParticleLenses() {
+    for (auto *h : halos) delete h;
+  }
+  MakeParticleLenses(const MakeParticleLenses &) = delete;
+  MakeParticleLenses &operator=(const MakeParticleLenses &) = delete;
+
+  std::vector<size_t> getnp() const { return nparticles_; }
+  std::array<double, 3> getCenterOfMass() const { return cm_; }
+  void getBoundingBox(std::array<double, 3> &Xmin, std::array<double, 3> &Xmax) const {
+    Xmin = ll_;
+    Xmax = ur_;
+  }
+  double getZoriginal() const { return z_original_; }
+
+  // particle_lens.cpp:139-151
+  void Recenter(std::array<double, 3> x) {
+    shift(x);
+    for (auto *h : halos) delete h;
+    halos.clear();
+  }
+
+  // particle_lens.cpp:153-209: records to comoving Mpc / Msun (divided by h),
+  // one LensHaloParticles per particle type present
+  void CreateHalos(const COSMOLOGY &cosmo, double redshift, double inv_area) {
+    const float h = (float)cosmo.gethubble();
+    const double unit = 1.0 / h;
+    for (auto &p : data) {
+      for (int k = 0; k < 3; ++k) p.x[k] = (float)(p.x[k] * unit);
+      p.Size = (float)(p.Size * unit);
+      p.Mass = (float)(p.Mass * unit);
+    }
+    for (auto *hh : halos) delete hh;
+    halos.clear();
+    size_t skip = 0;
+    struct Zero {
+      double operator[](int) const { return 0.0; }
+    };
+    for (int i = 0; i < 6; ++i) {
+      if (nparticles_[i] > 0)
+        halos.push_back(new LensHaloParticles(data.data() + skip, nparticles_[i], (float)redshift, cosmo, Zero(),
+                                              false, inv_area));
+      skip += nparticles_[i];
+    }
+  }
+
+  // particle_halo.h:1036-1053
+  static void writeSizesB(const std::string &filename, const std::vector<glb_particle> &pv, int Nsmooth,
+                          const std::vector<size_t> &numbytype, double redshift) {
+    if (numbytype.size() != 6) throw std::invalid_argument("numbytype must have 6 entries");
+    std::ofstream f(filename, std::ios::out | std::ios::binary);
+    if (!f.write((const char *)&Nsmooth, sizeof(int))) throw std::runtime_error("file writing error");
+    const size_t ntot = pv.size();
+    f.write((const char *)&ntot, sizeof(size_t));
+    f.write((const char *)numbytype.data(), sizeof(size_t) * 6);
+    f.write((const char *)&redshift, sizeof(double));
+    f.write((const char *)pv.data(), sizeof(glb_particle) * ntot);
+  }
+  // particle_halo.h:1056-1073
+  static bool readSizesB(const std::string &filename, std::vector<glb_particle> &pv, int &Nsmooth,
+                         std::vector<size_t> &numbytype, double &redshift) {
+    numbytype.assign(6, 0);
+    std::ifstream f(filename, std::ios::in | std::ios::binary);
+    if (!f.read((char *)&Nsmooth, sizeof(int))) return false;
+    size_t ntot = 0;
+    f.read((char *)&ntot, sizeof(size_t));
+    f.read((char *)numbytype.data(), sizeof(size_t) * 6);
+    f.read((char *)&redshift, sizeof(double));
+    pv.assign(ntot, glb_particle{});
+    f.read((char *)pv.data(), sizeof(glb_particle) * ntot);
+    return true;
+  }
+
+ private:
+  std::string filename_;
+  int Nsmooth_;
+  std::vector<size_t> nparticles_ = std::vector<size_t>(6, 0);
+  double z_original_ = -1;
+  std::array<double, 3> cm_{}, ll_{}, ur_{};
+
+  // particle_lens.cpp:211-341 for 3, 4 and 5 columns
+  void readCSV(int columns_used) {
+    std::ifstream file(filename_);
+    std::string line;
+    while (std::getline(file, line) && line[0] == '#') {
+    }
+    auto split = [](const std::string &l) {
+      std::vector<std::string> v;
+      std::stringstream ss(l);
+      std::string c;
+      while (std::getline(ss, c, ',')) v.push_back(c);
+      return v;
+    };
+    if ((int)split(line).size() < columns_used) throw std::invalid_argument("bad file");
+    data.clear();
+    do {
+      const std::vector<std::string> v = split(line);
+      glb_particle p{};
+      p.x[0] = std::stof(v[0]);
+      p.x[1] = std::stof(v[1]);
+      p.x[2] = std::stof(v[2]);
+      p.Mass = columns_used == 3 ? 1.0f : std::stof(v[3]);
+      if (columns_used == 5) p.Size = std::stof(v[4]);
+      data.push_back(p);
+    } while (std::getline(file, line));
+    nparticles_ = {data.size(), 0, 0, 0, 0, 0};
+    if (columns_used < 5) LensHaloParticles::calculate_smoothing(Nsmooth_, data.data(), data.size());
+  }
+  void moments(bool from_origin) {
+    double m = 0;
+    cm_ = {0, 0, 0};
+    for (int k = 0; k < 3; ++k) ll_[k] = ur_[k] = (from_origin || data.empty()) ? 0.0 : data[0].x[k];
+    for (const auto &p : data) {
+      for (int k = 0; k < 3; ++k) {
+        cm_[k] += p.x[k] * p.Mass;
+        if (ll_[k] > p.x[k]) ll_[k] = p.x[k];
+        if (ur_[k] < p.x[k]) ur_[k] = p.x[k];
+      }
+      m += p.Mass;
+    }
+    for (int k = 0; k < 3; ++k) cm_[k] /= m;
+  }
+  void shift(std::array<double, 3> x) {
+    for (auto &p : data)
+      for (int k = 0; k < 3; ++k) p.x[k] = (float)(p.x[k] - x[k]);
+    for (int k = 0; k < 3; ++k) {
+      ll_[k] -= x[k];
+      ur_[k] -= x[k];
+      cm_[k] -= x[k];
+    }
+  }
 };
 
 class LensHaloNFW : public LensHalo {

@@ -164,3 +164,38 @@ def test_csv_with_smoothing_matches_reference(tmp_path, columns):
             == open(tmp_path / "our" / "sim.csv_S32.glmb", "rb").read())
     halos = m.CreateHalos(0.7, 0.4, 0.0)
     assert len(halos) == 1
+
+
+@needs_ref
+@pytest.mark.parametrize("recenter", [False, True])
+def test_cpp_mirror_particle_files_match_reference(tmp_path, recenter):
+    """The C++ mirror's MakeParticleLenses (csv5) and sizes-file helpers
+    against the reference on the same csv file."""
+    import subprocess
+    gxx = shutil.which("g++")
+    lib = os.path.join(H.ROOT, "slsimlib_b200")
+    if gxx is None or not os.path.exists(os.path.join(lib, "libglamer_b200.so")):
+        pytest.skip("no g++ or library")
+    exe = str(tmp_path / "pio")
+    r = subprocess.run([gxx, "-std=c++17", "-O2", "-Wall", "-Wextra", "-Werror", "-I",
+                        os.path.join(H.ROOT, "include"), os.path.join(H.ROOT, "tests", "cpp", "particle_io_test.cpp"),
+                        "-o", exe, "-L", lib, "-lglamer_b200", f"-Wl,-rpath,{lib}", "-Wl,--allow-shlib-undefined"],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    p = particles(600, 9)
+    for who in ("ref", "cpp"):
+        os.makedirs(tmp_path / who)
+        write_csv(tmp_path / who / "sim.csv", p, 5)
+    ref, meta = H.RefDriver().make_particles(str(tmp_path / "ref" / "sim.csv"), 5, 16, recenter)
+    out = str(tmp_path / "cpp" / "o")
+    r = subprocess.run([exe, str(tmp_path / "cpp" / "sim.csv"), "16", str(int(recenter)), out],
+                       capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0 and r.stdout.strip() == "OK", r.stdout + r.stderr
+    got = np.fromfile(out + ".bin", dtype=synth.PARTICLE_DTYPE)
+    assert np.array_equal(got.view(np.uint8), ref.view(np.uint8))
+    assert np.array_equal(np.fromfile(out + ".meta"), meta)
+    assert (open(tmp_path / "ref" / "sim.csv_S16.glmb", "rb").read()
+            == open(tmp_path / "cpp" / "sim.csv_S16.glmb", "rb").read())
+    R = H.RefDriver()
+    R.write_sizes(ref, 64, str(tmp_path / "ref.sizes"))
+    assert open(tmp_path / "ref.sizes", "rb").read() == open(out + ".sizes", "rb").read()
