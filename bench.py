@@ -397,9 +397,9 @@ def run_smoothing(args):
                       "f32 coords, f64 distances",
                       f"kNN smoothing of {n} particles (triaxial NFW cluster + 10% background), Nsmooth {ns}",
                       clocks=clocks, kernels_ms={"morton_sort_and_boxes": sort_ms, "search": search_ms},
-                      # own kernels per call: bbox, Morton keys, gather, bucket boxes, log2(P) box levels, search
-                      # (the radix sort's kernels are the library's)
-                      gpu_launches=args.steps * (5 + int(np.ceil(np.log2(max(1, n // 128))))),
+                      # own kernels per call: bbox, Morton keys, gather, bucket boxes, chunk boxes, log2(P) box
+                      # levels, search (the radix sort's kernels are the library's)
+                      gpu_launches=args.steps * (6 + int(np.ceil(np.log2(max(1, n // 128))))),
                       e2e={"value": n / e2e_s, "unit": "particles/s", "h2d_bytes_per_step": 24 * n,
                            "d2h_bytes_per_step": 4 * n})
     if not args.no_cpu:

@@ -44,10 +44,9 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kWarps = 4;         // warps per CTA in k_knn
-constexpr int kListCap = 2048;    // candidate buckets listed per CTA
+constexpr int kListCap = 1024;    // candidate buckets listed per CTA
 constexpr int kStack = 64;        // per-warp DFS stack (tree depth <= 31)
-constexpr int kFront = 1024;      // breadth-first frontier of the candidate search
-constexpr int kSortMax = 1024;    // candidate lists up to this size are sorted near-first
+constexpr int kFront = 512;       // breadth-first frontier of the candidate search
 
 #define CK(call)                                                                     \
   do {                                                                               \
@@ -97,13 +96,6 @@ __device__ __forceinline__ double gap2_box(float4 alo, float4 ahi, float4 blo, f
   return __fma_rn(gz, gz, __fma_rn(gy, gy, __dmul_rn(gx, gx)));
 }
 
-__device__ __forceinline__ unsigned long long warp_min64(unsigned long long v) {
-  for (int o = 16; o; o >>= 1) {
-    unsigned long long w = __shfl_xor_sync(kFull, v, o);
-    v = w < v ? w : v;
-  }
-  return v;
-}
 __device__ __forceinline__ unsigned long long warp_max64(unsigned long long v) {
   for (int o = 16; o; o >>= 1) {
     unsigned long long w = __shfl_xor_sync(kFull, v, o);
@@ -114,27 +106,73 @@ __device__ __forceinline__ unsigned long long warp_max64(unsigned long long v) {
 
 // k-th smallest (1-based) of buf[0, cnt) (non-negative doubles, so the bit
 // patterns order like the values), by bitwise radix selection from the
-// highest bit in which the entries differ; stops as soon as one entry is left.
+// highest bit in which the entries differ, first on the high 32-bit words and
+// then, among the entries sharing the selected high word, on the low words;
+// stops as soon as one entry is left.
 __device__ __noinline__ double warp_select(const double *buf, int cnt, int k, int lane) {
-  unsigned long long lo = ~0ull, hi = 0ull;
+  unsigned lo = kFull, hi = 0u;
+  for (int i = lane; i < cnt; i += 32) {
+    const unsigned h = (unsigned)__double2hiint(buf[i]);
+    lo = min(lo, h);
+    hi = max(hi, h);
+  }
+  lo = __reduce_min_sync(kFull, lo);
+  hi = __reduce_max_sync(kFull, hi);
+  unsigned hword = lo;
+  int act = cnt;
+  if (lo != hi) {
+    const int top = 31 - __clz(lo ^ hi);
+    unsigned above = top >= 31 ? 0u : ~((2u << top) - 1u);
+    unsigned prefix = lo & above;
+    for (int b = top; b >= 0; --b) {
+      const unsigned bit = 1u << b;
+      int c0 = 0;
+      for (int i = lane; i < cnt; i += 32) {
+        const unsigned h = (unsigned)__double2hiint(buf[i]);
+        c0 += ((h & above) == prefix) && !(h & bit);
+      }
+      c0 = (int)__reduce_add_sync(kFull, (unsigned)c0);
+      if (k <= c0) {
+        act = c0;
+      } else {
+        k -= c0;
+        prefix |= bit;
+        act -= c0;
+      }
+      above |= bit;
+      if (act == 1) {
+        unsigned long long f = 0ull;
+        for (int i = lane; i < cnt; i += 32) {
+          const unsigned long long u = __double_as_longlong(buf[i]);
+          if (((unsigned)(u >> 32) & above) == prefix) f = u;
+        }
+        return __longlong_as_double(warp_max64(f));
+      }
+    }
+    hword = prefix;
+  }
+  // act entries share the high word `hword`; rank k among their low words
+  unsigned llo = kFull, lhi = 0u;
   for (int i = lane; i < cnt; i += 32) {
     const unsigned long long u = __double_as_longlong(buf[i]);
-    lo = u < lo ? u : lo;
-    hi = u > hi ? u : hi;
+    if ((unsigned)(u >> 32) == hword) {
+      llo = min(llo, (unsigned)u);
+      lhi = max(lhi, (unsigned)u);
+    }
   }
-  lo = warp_min64(lo);
-  hi = warp_max64(hi);
-  if (lo == hi) return __longlong_as_double(lo);
-  const int top = 63 - __clzll(lo ^ hi);
-  unsigned long long above = top >= 63 ? 0ull : ~((2ull << top) - 1ull);
-  unsigned long long prefix = lo & above;
-  int act = cnt;
+  llo = __reduce_min_sync(kFull, llo);
+  lhi = __reduce_max_sync(kFull, lhi);
+  if (llo == lhi) return __hiloint2double((int)hword, (int)llo);
+  const int top = 31 - __clz(llo ^ lhi);
+  unsigned above = top >= 31 ? 0u : ~((2u << top) - 1u);
+  unsigned prefix = llo & above;
   for (int b = top; b >= 0; --b) {
-    const unsigned long long bit = 1ull << b;
+    const unsigned bit = 1u << b;
     int c0 = 0;
     for (int i = lane; i < cnt; i += 32) {
       const unsigned long long u = __double_as_longlong(buf[i]);
-      c0 += ((u & above) == prefix) && !(u & bit);
+      const unsigned l = (unsigned)u;
+      c0 += ((unsigned)(u >> 32) == hword) && ((l & above) == prefix) && !(l & bit);
     }
     c0 = (int)__reduce_add_sync(kFull, (unsigned)c0);
     if (k <= c0) {
@@ -145,16 +183,17 @@ __device__ __noinline__ double warp_select(const double *buf, int cnt, int k, in
       act -= c0;
     }
     above |= bit;
-    if (act == 1) {
-      unsigned long long f = 0ull;
-      for (int i = lane; i < cnt; i += 32) {
-        const unsigned long long u = __double_as_longlong(buf[i]);
-        if ((u & above) == prefix) f = u;
-      }
-      return __longlong_as_double(warp_max64(f));
-    }
+    if (act == 1) break;
   }
-  return __longlong_as_double(prefix);
+  if (act == 1) {
+    unsigned f = 0u;
+    for (int i = lane; i < cnt; i += 32) {
+      const unsigned long long u = __double_as_longlong(buf[i]);
+      if ((unsigned)(u >> 32) == hword && ((unsigned)u & above) == prefix) f = (unsigned)u;
+    }
+    return __hiloint2double((int)hword, (int)__reduce_max_sync(kFull, f));
+  }
+  return __hiloint2double((int)hword, (int)prefix);
 }
 
 // Keeps exactly K entries of buf[0, cnt): all below beta (the K-th smallest)
@@ -274,6 +313,28 @@ __global__ void k_bucket_box(const float4 *pos, size_t n, int nb, int P, float4 
   }
 }
 
+// One warp per aligned 32-particle chunk of the sorted array: its box.
+__global__ void k_chunk_box(const float4 *pos, size_t n, float4 *clo, float4 *chi) {
+  const size_t c = (blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (c >= (n + 31) / 32) return;
+  const size_t i = (c << 5) + lane;
+  float4 v = pos[i < n ? i : c << 5];
+  float lx = v.x, ly = v.y, lz = v.z, hx = v.x, hy = v.y, hz = v.z;
+  for (int o = 16; o; o >>= 1) {
+    lx = fminf(lx, __shfl_xor_sync(kFull, lx, o));
+    ly = fminf(ly, __shfl_xor_sync(kFull, ly, o));
+    lz = fminf(lz, __shfl_xor_sync(kFull, lz, o));
+    hx = fmaxf(hx, __shfl_xor_sync(kFull, hx, o));
+    hy = fmaxf(hy, __shfl_xor_sync(kFull, hy, o));
+    hz = fmaxf(hz, __shfl_xor_sync(kFull, hz, o));
+  }
+  if (lane == 0) {
+    clo[c] = make_float4(lx, ly, lz, 0.f);
+    chi[c] = make_float4(hx, hy, hz, 0.f);
+  }
+}
+
 // Internal nodes [w, 2w) of the implicit tree from their children.
 __global__ void k_box_up(int w, float4 *blo, float4 *bhi) {
   const int i = w + (int)(blockIdx.x * blockDim.x + threadIdx.x);
@@ -287,6 +348,7 @@ __global__ void k_box_up(int w, float4 *blo, float4 *bhi) {
 struct KnnArgs {
   const float4 *pos;  // Morton-sorted {x, y, z, original index}
   const float4 *blo, *bhi;
+  const float4 *clo, *chi;  // boxes of the aligned 32-particle chunks of pos
   size_t n;
   int nb, P, K, cap;
   int shrink_at;      // buffer size that triggers a shrink after a bucket
@@ -295,30 +357,40 @@ struct KnnArgs {
 };
 
 // Appends the squared distances below beta of bucket c's particles to the
-// warp's buffer, shrinking it to K entries (and beta to their largest)
-// whenever the next 32 might not fit, and after the bucket once it holds
-// shrink_at entries, so that the bound tightens early.
+// warp's buffer.  The bucket's aligned 32-particle chunks are tested against
+// beta first (one chunk box per lane); only chunks within it are read.  The
+// buffer is cut back to K entries (and beta to their largest) whenever the
+// next 32 might not fit, and after the bucket once it holds shrink_at entries,
+// so that the bound tightens early.
 __device__ __forceinline__ void knn_visit(const KnnArgs &a, int c, float qx, float qy, float qz, double *buf,
                                           int &cnt, double &beta, int lane) {
   const size_t s = bucket_start(c, a.n, a.nb), e = bucket_start(c + 1, a.n, a.nb);
   const unsigned lt_mask = (1u << lane) - 1u;
-  for (size_t base = s; base < e; base += 32) {
-    if (cnt + 32 > a.cap) {
-      beta = warp_select(buf, cnt, a.K, lane);
-      cnt = warp_compact(buf, cnt, a.K, beta, lane);
+  const size_t ch0 = s >> 5, nch = ((e - 1) >> 5) - ch0 + 1;
+  for (size_t cg = 0; cg < nch; cg += 32) {
+    const size_t ch = ch0 + cg + lane;
+    const bool near = cg + lane < nch && gap2_point(qx, qy, qz, a.clo[ch], a.chi[ch]) < beta;
+    unsigned cm = __ballot_sync(kFull, near);
+    while (cm) {
+      const int l = __ffs(cm) - 1;
+      cm &= cm - 1;
+      if (cnt + 32 > a.cap) {
+        beta = warp_select(buf, cnt, a.K, lane);
+        cnt = warp_compact(buf, cnt, a.K, beta, lane);
+      }
+      const size_t i = ((ch0 + cg + l) << 5) + lane;
+      double r2 = 0.0;
+      bool keep = false;
+      if (i >= s && i < e) {
+        const float4 v = a.pos[i];
+        r2 = knn_r2(v.x, v.y, v.z, qx, qy, qz);
+        keep = r2 < beta;
+      }
+      const unsigned m = __ballot_sync(kFull, keep);
+      if (keep) buf[cnt + __popc(m & lt_mask)] = r2;
+      cnt += __popc(m);
+      __syncwarp();
     }
-    const size_t i = base + lane;
-    double r2 = 0.0;
-    bool keep = false;
-    if (i < e) {
-      const float4 v = a.pos[i];
-      r2 = knn_r2(v.x, v.y, v.z, qx, qy, qz);
-      keep = r2 < beta;
-    }
-    const unsigned m = __ballot_sync(kFull, keep);
-    if (keep) buf[cnt + __popc(m & lt_mask)] = r2;
-    cnt += __popc(m);
-    __syncwarp();
   }
   if (cnt >= a.shrink_at) {
     beta = warp_select(buf, cnt, a.K, lane);
@@ -327,7 +399,7 @@ __device__ __forceinline__ void knn_visit(const KnnArgs &a, int c, float qx, flo
 }
 
 #ifndef GLB_KNN_MIN_BLOCKS
-#define GLB_KNN_MIN_BLOCKS 6
+#define GLB_KNN_MIN_BLOCKS 8
 #endif
 __global__ void __launch_bounds__(kWarps * 32, GLB_KNN_MIN_BLOCKS) k_knn(KnnArgs a) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -411,31 +483,36 @@ __global__ void __launch_bounds__(kWarps * 32, GLB_KNN_MIN_BLOCKS) k_knn(KnnArgs
   __syncthreads();
   const int nlist = min(s_nlist, kListCap);
   const bool overflow = s_overflow != 0;
-  // near-first order (by the distance between box centres), so that the
-  // bound tightens on the first buckets visited; rank sort, ties by position
-  if (!overflow && nlist > 1 && nlist <= kSortMax) {
-    const float4 olo = a.blo[a.P + b], ohi = a.bhi[a.P + b];
+  // near-first order: by a lower bound (rounded down to float) of the gap
+  // between this bucket's box and the candidate's, then by the distance
+  // between box centres; rank sort in the (still unused) warp buffers.  The
+  // gap order lets a query stop at the first entry whose bound is beyond it.
+  const float4 olo = a.blo[a.P + b], ohi = a.bhi[a.P + b];
+  const bool sorted = !overflow && nlist > 1 && (size_t)nlist * 12 <= (size_t)kWarps * a.cap * sizeof(double);
+  if (sorted) {
     const float ox = 0.5f * (olo.x + ohi.x), oy = 0.5f * (olo.y + ohi.y), oz = 0.5f * (olo.z + ohi.z);
-    float *key = reinterpret_cast<float *>(front);
-    int *sorted = front + kSortMax;
+    float *k1 = reinterpret_cast<float *>(qbeta + mmax);
+    float *k2 = k1 + nlist;
+    int *ids = reinterpret_cast<int *>(k2 + nlist);
     for (int i = tid; i < nlist; i += blockDim.x) {
       const int c = list[i];
       const float4 lo = a.blo[a.P + c], hi = a.bhi[a.P + c];
+      k1[i] = __double2float_rd(gap2_box(olo, ohi, lo, hi));
       const float dx = 0.5f * (lo.x + hi.x) - ox, dy = 0.5f * (lo.y + hi.y) - oy, dz = 0.5f * (lo.z + hi.z) - oz;
-      key[i] = dx * dx + dy * dy + dz * dz;
+      k2[i] = dx * dx + dy * dy + dz * dz;
     }
     __syncthreads();
     for (int i = tid; i < nlist; i += blockDim.x) {
-      const float ki = key[i];
+      const float g = k1[i], d = k2[i];
       int r = 0;
       for (int j = 0; j < nlist; ++j) {
-        const float kj = key[j];
-        r += (kj < ki) || (kj == ki && j < i);
+        const float gj = k1[j], dj = k2[j];
+        r += (gj < g) || (gj == g && (dj < d || (dj == d && j < i)));
       }
-      sorted[r] = list[i];
+      ids[r] = list[i];
     }
     __syncthreads();
-    for (int i = tid; i < nlist; i += blockDim.x) list[i] = sorted[i];
+    for (int i = tid; i < nlist; i += blockDim.x) list[i] = ids[i];
     __syncthreads();
   }
 
@@ -462,6 +539,11 @@ __global__ void __launch_bounds__(kWarps * 32, GLB_KNN_MIN_BLOCKS) k_knn(KnnArgs
     if (!overflow) {
       // 32 listed boxes tested at once against the current bound
       for (int base = 0; base < nlist; base += 32) {
+        if (sorted) {
+          // every later entry is at least as far from this bucket's box
+          const int c0 = list[base];
+          if ((double)__double2float_rd(gap2_box(olo, ohi, a.blo[a.P + c0], a.bhi[a.P + c0])) >= beta) break;
+        }
         const int li = base + lane;
         const int c = li < nlist ? list[li] : 0;
         const bool near = li < nlist && gap2_point(x.x, x.y, x.z, a.blo[a.P + c], a.bhi[a.P + c]) < beta;
@@ -593,7 +675,7 @@ size_t smoothing_smem_bytes(size_t n, int nsmooth) {
   const int S = ((2 * nsmooth + 31) / 32) * 32;
   const int nb = (int)std::max<size_t>(1, n / (size_t)S);
   const int mmax = (int)((n + nb - 1) / nb);
-  int cap = std::max(512, std::max(mmax + 64, 2 * K + 64));
+  int cap = std::max(mmax + 64, 2 * K + 64);
   cap = (cap + 31) / 32 * 32;
   return (size_t)mmax * (sizeof(float4) + sizeof(double)) + (size_t)kWarps * cap * sizeof(double) +
          (size_t)(kListCap + kWarps * kStack + 2 * kFront) * sizeof(int);
@@ -611,7 +693,7 @@ Status smooth_particles_device(const glb_particle_rec *d_p, size_t n, int nsmoot
   int P = 1;
   while (P < nb) P <<= 1;
   const int mmax = (int)((n + nb - 1) / nb);
-  int cap = std::max(512, std::max(mmax + 64, 2 * K + 64));
+  int cap = std::max(mmax + 64, 2 * K + 64);
   cap = (cap + 31) / 32 * 32;
   const size_t smem = smoothing_smem_bytes(n, nsmooth);
   if (smem > 200 * 1024) return Status::err(-6, "Nsmooth too large for the shared-memory search");
@@ -627,7 +709,8 @@ Status smooth_particles_device(const glb_particle_rec *d_p, size_t n, int nsmoot
     int P = 0;
     DBuf<unsigned long long> key, key2;
     DBuf<unsigned> idx, sidx, mm;
-    DBuf<float4> pos, blo, bhi;
+    size_t nch = 0;
+    DBuf<float4> pos, blo, bhi, clo, chi;
     DBuf<int> flags;
     DBuf<unsigned char> tmp;
   };
@@ -643,6 +726,12 @@ Status smooth_particles_device(const glb_particle_rec *d_p, size_t n, int nsmoot
     CK(w.sidx.alloc(n));
     CK(w.pos.alloc(n));
     w.n = n;
+  }
+  const size_t nch = (n + 31) / 32;
+  if (w.nch < nch) {
+    CK(w.clo.alloc(nch));
+    CK(w.chi.alloc(nch));
+    w.nch = nch;
   }
   if (w.P < P) {
     CK(w.blo.alloc(2 * (size_t)P));
@@ -673,6 +762,7 @@ Status smooth_particles_device(const glb_particle_rec *d_p, size_t n, int nsmoot
   CK(cub::DeviceRadixSort::SortPairs(w.tmp.p, tb, w.key.p, w.key2.p, w.idx.p, w.sidx.p, (int)n, 0, 63, st));
   k_gather_pos<<<nblk(n, 256), 256, 0, st>>>(d_p, w.sidx.p, n, w.pos.p);
   k_bucket_box<<<nblk((size_t)P * 32, 256), 256, 0, st>>>(w.pos.p, n, nb, P, w.blo.p, w.bhi.p);
+  k_chunk_box<<<nblk(nch * 32, 256), 256, 0, st>>>(w.pos.p, n, w.clo.p, w.chi.p);
   for (int l = P / 2; l >= 1; l /= 2) k_box_up<<<nblk(l, 256), 256, 0, st>>>(l, w.blo.p, w.bhi.p);
   CK(cudaEventRecord(ev[1], st));
 
@@ -680,6 +770,8 @@ Status smooth_particles_device(const glb_particle_rec *d_p, size_t n, int nsmoot
   a.pos = w.pos.p;
   a.blo = w.blo.p;
   a.bhi = w.bhi.p;
+  a.clo = w.clo.p;
+  a.chi = w.chi.p;
   a.n = n;
   a.nb = nb;
   a.P = P;
