@@ -108,18 +108,28 @@ __device__ __forceinline__ unsigned long long warp_max64(unsigned long long v) {
 // patterns order like the values), by bitwise radix selection from the
 // highest bit in which the entries differ, first on the high 32-bit words and
 // then, among the entries sharing the selected high word, on the low words;
-// stops as soon as one entry is left.
+// stops as soon as one entry is left.  Exact zeros (a particle's distance to
+// itself or to a coincident one) are counted apart, so that the selection
+// starts from the highest bit in which the non-zero entries differ.
 __device__ __noinline__ double warp_select(const double *buf, int cnt, int k, int lane) {
   unsigned lo = kFull, hi = 0u;
+  int zeros = 0;
   for (int i = lane; i < cnt; i += 32) {
     const unsigned h = (unsigned)__double2hiint(buf[i]);
+    if (h == 0u && buf[i] == 0.0) {
+      ++zeros;
+      continue;
+    }
     lo = min(lo, h);
     hi = max(hi, h);
   }
+  zeros = (int)__reduce_add_sync(kFull, (unsigned)zeros);
+  if (k <= zeros) return 0.0;
+  k -= zeros;
   lo = __reduce_min_sync(kFull, lo);
   hi = __reduce_max_sync(kFull, hi);
   unsigned hword = lo;
-  int act = cnt;
+  int act = cnt - zeros;
   if (lo != hi) {
     const int top = 31 - __clz(lo ^ hi);
     unsigned above = top >= 31 ? 0u : ~((2u << top) - 1u);
@@ -128,8 +138,9 @@ __device__ __noinline__ double warp_select(const double *buf, int cnt, int k, in
       const unsigned bit = 1u << b;
       int c0 = 0;
       for (int i = lane; i < cnt; i += 32) {
-        const unsigned h = (unsigned)__double2hiint(buf[i]);
-        c0 += ((h & above) == prefix) && !(h & bit);
+        const double v = buf[i];
+        const unsigned h = (unsigned)__double2hiint(v);
+        c0 += ((h & above) == prefix) && !(h & bit) && v != 0.0;
       }
       c0 = (int)__reduce_add_sync(kFull, (unsigned)c0);
       if (k <= c0) {
@@ -144,7 +155,7 @@ __device__ __noinline__ double warp_select(const double *buf, int cnt, int k, in
         unsigned long long f = 0ull;
         for (int i = lane; i < cnt; i += 32) {
           const unsigned long long u = __double_as_longlong(buf[i]);
-          if (((unsigned)(u >> 32) & above) == prefix) f = u;
+          if (((unsigned)(u >> 32) & above) == prefix && u != 0ull) f = u;
         }
         return __longlong_as_double(warp_max64(f));
       }
@@ -413,6 +424,7 @@ __global__ void __launch_bounds__(kWarps * 32, GLB_KNN_MIN_BLOCKS) k_knn(KnnArgs
   int *list = reinterpret_cast<int *>(qbeta + mmax + (size_t)kWarps * a.cap);
   int *stack = list + kListCap + warp * kStack;
   int *front = list + kListCap + kWarps * kStack;
+  float *lkey = reinterpret_cast<float *>(front + 2 * kFront);  // gap bound of each sorted list entry
   __shared__ unsigned long long s_r2max;
   __shared__ int s_nlist, s_overflow, s_fn[2];
 
@@ -510,6 +522,7 @@ __global__ void __launch_bounds__(kWarps * 32, GLB_KNN_MIN_BLOCKS) k_knn(KnnArgs
         r += (gj < g) || (gj == g && (dj < d || (dj == d && j < i)));
       }
       ids[r] = list[i];
+      lkey[r] = g;
     }
     __syncthreads();
     for (int i = tid; i < nlist; i += blockDim.x) list[i] = ids[i];
@@ -539,11 +552,8 @@ __global__ void __launch_bounds__(kWarps * 32, GLB_KNN_MIN_BLOCKS) k_knn(KnnArgs
     if (!overflow) {
       // 32 listed boxes tested at once against the current bound
       for (int base = 0; base < nlist; base += 32) {
-        if (sorted) {
-          // every later entry is at least as far from this bucket's box
-          const int c0 = list[base];
-          if ((double)__double2float_rd(gap2_box(olo, ohi, a.blo[a.P + c0], a.bhi[a.P + c0])) >= beta) break;
-        }
+        // every later entry is at least as far from this bucket's box
+        if (sorted && (double)lkey[base] >= beta) break;
         const int li = base + lane;
         const int c = li < nlist ? list[li] : 0;
         const bool near = li < nlist && gap2_point(x.x, x.y, x.z, a.blo[a.P + c], a.bhi[a.P + c]) < beta;
@@ -678,7 +688,7 @@ size_t smoothing_smem_bytes(size_t n, int nsmooth) {
   int cap = std::max(mmax + 64, 2 * K + 64);
   cap = (cap + 31) / 32 * 32;
   return (size_t)mmax * (sizeof(float4) + sizeof(double)) + (size_t)kWarps * cap * sizeof(double) +
-         (size_t)(kListCap + kWarps * kStack + 2 * kFront) * sizeof(int);
+         (size_t)(2 * kListCap + kWarps * kStack + 2 * kFront) * sizeof(int);
 }
 
 Status smooth_particles_device(const glb_particle_rec *d_p, size_t n, int nsmooth, float *d_size,
