@@ -45,6 +45,9 @@
  *        SimFileFormat::csvFMT; writes FILE_S<NSMOOTH>.glmb beside it) -> OUT: the
  *        particle records; OUT.meta: {1, cm[3], bbox_ll[3], bbox_ur[3],
  *        z_original, nparticles[6]}, or {0} when the constructor throws.
+ *   particlefile FILE Z NSMOOTH MULTIMASS INV_AREA MINPSIZE MASSSCALING RECENTER TX TY XFILE N OUT
+ *        LensHaloParticles from an ascii position file (reads or writes
+ *        FILE.<NSMOOTH>sizes) -> force_halo at N physical positions.
  *   writesizes PFILE N NSMOOTH OUT     LensHaloParticles::writeSizes
  *   readsizes FILE N NSMOOTH MIN_SIZE OUT
  *        LensHaloParticles::readSizesFile -> OUT: {found, sizes[N]}, or {-1}
@@ -400,6 +403,26 @@ int main() {
         meta = {0.0};
       }
       write_arr(out + ".meta", meta);
+    } else if (cmd == "particlefile") {
+      /* LensHaloParticles(file, ascii, z, Nsmooth, cosmo, (tx, ty), recenter,
+       * multimass, inv_area, MinPSize, massscaling) -> force_halo at N
+       * physical positions (7 doubles each) */
+      std::string file, xf, out;
+      double z, inv_area, minp, mscale, tx, ty;
+      int nsmooth, multimass, recenter;
+      size_t n;
+      in >> file >> z >> nsmooth >> multimass >> inv_area >> minp >> mscale >> recenter >> tx >> ty >> xf >> n >> out;
+      Point_2d rot(tx, ty);
+      LensHaloParticles<PT> h(file, SimFileFormat::ascii, z, nsmooth, cosmo, rot, recenter != 0, multimass != 0,
+                              inv_area, minp, mscale, false);
+      std::vector<double> x = read_arr<double>(xf, 2 * n), o(7 * n);
+      for (size_t k = 0; k < n; ++k) {
+        double a[2] = {0, 0}, kk = 0, g[3] = {0, 0, 0}, ph = 0;
+        h.force_halo(a, &kk, g, &ph, &x[2 * k]);
+        double v[7] = {a[0], a[1], kk, g[0], g[1], g[2], ph};
+        std::copy(v, v + 7, &o[7 * k]);
+      }
+      write_arr(out, o);
     } else if (cmd == "writesizes") {
       std::string pf, out;
       size_t n;

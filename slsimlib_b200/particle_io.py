@@ -301,3 +301,51 @@ class MakeParticleLenses:
                 self.halos.append(LensHaloParticles(d[skip:skip + nk].copy(), redshift, inv_area=inv_area))
             skip += nk
         return self.halos
+
+
+# ------------------------------------------- LensHaloParticles from a file
+def lens_halo_particles_from_file(filename: str, redshift: float, Nsmooth: int, theta_rotate=(0.0, 0.0),
+                                  recenter: bool = False, multimass: bool = True, inv_area: float = 0.0,
+                                  MinPSize: float = 0.0, massscaling: float = 1.0):
+    """LensHaloParticles(simulation_filename, SimFileFormat::ascii, redshift,
+    Nsmooth, cosmo, theta_rotate, recenter, multimass, inv_area, MinPSize,
+    massscaling) (include/particle_halo.h:229-340): reads the ascii positions,
+    takes the sizes from <filename>.<Nsmooth>sizes or computes them (GPU) and
+    writes that file, then as the reference: sizes below MinPSize raised to it,
+    masses of all particles but the first multiplied by massscaling, positions
+    from comoving to physical (1/(1+z)), optional recentring on the centre of
+    mass, rotation, and a particle lens whose tree has no screening.  Returns
+    (slsimlib_b200.LensHaloParticles, the particle records used)."""
+    from . import LensHaloParticles, calculate_smoothing
+    pp, _ = read_positions_ascii(filename, multimass)
+    n = len(pp)
+    sizefile = f"{filename}.{int(Nsmooth)}sizes"
+    mn = float(MinPSize)
+    s = read_sizes_file(sizefile, n, Nsmooth, mn)
+    if s is None:
+        calculate_smoothing(Nsmooth, pp)
+        write_sizes(sizefile, Nsmooth, pp["Size"])
+        pp["Size"] = np.where(pp["Size"].astype(np.float64) < mn, np.float32(mn), pp["Size"])
+    else:
+        pp["Size"] = s
+    if n > 1:
+        pp["Mass"][1:] = (pp["Mass"][1:].astype(np.float64) * float(massscaling)).astype(np.float32)
+    sf = 1.0 / (1.0 + float(redshift))
+    pp["x"] = (pp["x"].astype(np.float64) * sf).astype(np.float32)
+    m = pp["Mass"] if multimass else np.full(n, pp["Mass"][0], dtype=np.float32)
+    mc = np.array([float(np.cumsum((pp["x"][:, k] * m).astype(np.float64))[-1]) for k in range(3)])
+    mass = float(np.cumsum(m.astype(np.float64))[-1])
+    mc = mc / mass
+    if recenter:
+        pp["x"] = (pp["x"].astype(np.float64) - mc).astype(np.float32)
+    tx, ty = float(theta_rotate[0]), float(theta_rotate[1])
+    if tx != 0.0 or ty != 0.0:
+        cx, sx, cy, sy = np.cos(tx), np.sin(tx), np.cos(ty), np.sin(ty)
+        coord = np.array([[cy, 0.0, -sy], [-sy * sx, cx, -cy * sx], [cx, sx, cy * cx]])
+        x = pp["x"].astype(np.float64)
+        t = np.zeros_like(x)
+        for r in range(3):
+            for j in range(3):
+                t[:, r] += coord[r, j] * x[:, j]
+        pp["x"] = t.astype(np.float32)
+    return LensHaloParticles(pp, redshift, inv_area=inv_area, max_range=0.0), pp

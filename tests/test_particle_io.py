@@ -199,3 +199,53 @@ def test_cpp_mirror_particle_files_match_reference(tmp_path, recenter):
     R = H.RefDriver()
     R.write_sizes(ref, 64, str(tmp_path / "ref.sizes"))
     assert open(tmp_path / "ref.sizes", "rb").read() == open(out + ".sizes", "rb").read()
+
+
+def write_ascii(path, p, multimass=True):
+    with open(path, "w") as f:
+        f.write(f"# nparticles {len(p)}\n")
+        if not multimass:
+            f.write("# mass 1e9\n")
+        for q in p:
+            v = [f"{float(c):.9g}" for c in q["x"]]
+            if multimass:
+                v.append(f"{float(q['Mass']):.9g}")
+            f.write(" ".join(v) + "\n")
+
+
+@needs_ref
+@pytest.mark.gpu
+@pytest.mark.parametrize("recenter,rot,mscale,minp", [(False, (0.0, 0.0), 1.0, 0.0), (True, (0.3, -0.2), 2.5, 2e-3)])
+def test_particle_lens_from_ascii_file_matches_reference(tmp_path, recenter, rot, mscale, minp):
+    """LensHaloParticles from an ascii position file: the sizes cache written
+    (smoothing on the GPU) and the lens's force against the reference's."""
+    from tests.test_gpu_parity import RTOL64, force_err, pack
+    r = np.random.default_rng(21)
+    p = synth.nfw_particles(r, 20000, 2e14, 5.0, 0.4, 0.0)
+    p["Mass"] = r.uniform(5e9, 2e10, len(p)).astype(np.float32)
+    for who in ("ref", "our"):
+        os.makedirs(tmp_path / who)
+        write_ascii(tmp_path / who / "sim.txt", p)
+    xx = r.uniform(-0.4, 0.4, (300, 2))
+    R = H.RefDriver()
+    xf = R._file(np.ascontiguousarray(xx))
+    of = R._file()
+    R.run([f"particlefile {tmp_path / 'ref' / 'sim.txt'} 0.4 32 1 0.0 {minp!r} {mscale!r} {int(recenter)} "
+           f"{rot[0]!r} {rot[1]!r} {xf} {len(xx)} {of}"])
+    ref = np.fromfile(of).reshape(-1, 7)
+    halo, _ = pio.lens_halo_particles_from_file(str(tmp_path / "our" / "sim.txt"), 0.4, 32, rot, recenter, True,
+                                                0.0, minp, mscale)
+    f = pack(*halo.force_halo(xx))
+    m, cols = force_err(f, ref)
+    assert m < RTOL64, cols
+    assert (open(tmp_path / "ref" / "sim.txt.32sizes", "rb").read()
+            == open(tmp_path / "our" / "sim.txt.32sizes", "rb").read())
+    # a second construction reads the sizes back from the cache (6 digits), on both sides
+    of2 = R._file()
+    R.run([f"particlefile {tmp_path / 'ref' / 'sim.txt'} 0.4 32 1 0.0 {minp!r} {mscale!r} {int(recenter)} "
+           f"{rot[0]!r} {rot[1]!r} {xf} {len(xx)} {of2}"])
+    ref2 = np.fromfile(of2).reshape(-1, 7)
+    halo2, _ = pio.lens_halo_particles_from_file(str(tmp_path / "our" / "sim.txt"), 0.4, 32, rot, recenter, True,
+                                                 0.0, minp, mscale)
+    m2, cols2 = force_err(pack(*halo2.force_halo(xx)), ref2)
+    assert m2 < RTOL64, cols2
