@@ -16,14 +16,17 @@
 //   1. particles are sorted along a 63-bit Morton curve of the bounding box
 //      and cut into buckets of S..2S-1 consecutive particles
 //      (S = 2*Nsmooth rounded up to 32);
-//   2. an implicit binary tree over the buckets carries float bounding boxes;
+//   2. an implicit binary tree over the buckets carries float bounding boxes,
+//      and every aligned 32-particle chunk of the sorted array has its box;
 //   3. one CTA per bucket: every query first takes the (Nsmooth+1)-th
 //      smallest squared distance within its own bucket as a bound; the CTA
 //      lists the buckets whose boxes lie within the largest bound of its
-//      queries; each warp then streams, per query, the listed buckets whose box
-//      lies within the query's current bound through a shared-memory buffer of
-//      squared distances below the bound, shrinking the buffer to exactly
-//      Nsmooth+1 entries (and the bound to their maximum) whenever it fills;
+//      queries, ordered by a lower bound of their gap to its own box; each
+//      warp then scans the list per query until that gap bound passes the
+//      query's current bound, and reads the chunks of the buckets within the
+//      bound into a shared-memory buffer of squared distances below it,
+//      cutting the buffer back to exactly Nsmooth+1 entries (and the bound to
+//      their maximum) after each bucket once it holds twice that;
 //   4. the (Nsmooth+1)-th smallest entry, selected exactly on its 64-bit
 //      pattern, is the answer.
 // Box tests use the same float subtraction as the distances, so a box is
