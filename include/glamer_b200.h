@@ -326,7 +326,7 @@ int glb_lens_last_timing(glb_lens *l, double *kernel_ms, double *total_ms);
  * N = 2*nsmooth+1 the reference's walk counts some particles twice for the
  * queries in its top node's first child; those values are reproduced too.
  * Errors: nsmooth < 1 or n <= nsmooth+1 (the reference exits) GLB_ERR_ARG;
- * nsmooth above about 430 GLB_ERR_UNSUPPORTED.  Synchronous; particles are
+ * nsmooth above about 800 GLB_ERR_UNSUPPORTED.  Synchronous; particles are
  * host records, only their Size is written. */
 int glb_particles_smoothing(glb_particle *particles, size_t n, int nsmooth);
 /* The same on device buffers: n records at particles_dev, n floats written to
