@@ -23,6 +23,7 @@
 #ifndef GLAMER_B200_HPP
 #define GLAMER_B200_HPP
 
+#include <algorithm>
 #include <array>
 #include <cmath>
 #include <cstddef>
@@ -381,6 +382,36 @@ class MakeParticleLenses {
     halos.clear();
   }
 
+  // particle_lens.cpp:447-478: drops the particles farther than radius from
+  // center (each swapped with the last kept one); re-sorted by type when more
+  // than one type remains (stable here)
+  void radialCut(std::array<double, 3> center, double radius) {
+    cut([&](const glb_particle &p) {
+      const double a = p.x[0] - center[0], b = p.x[1] - center[1], c = p.x[2] - center[2];
+      return a * a + b * b + c * c;
+    }, radius);
+  }
+  // particle_lens.cpp:497-520: the same with the distance in x, y
+  void cylindricalCut(std::array<double, 2> center, double radius) {
+    cut([&](const glb_particle &p) {
+      const double a = p.x[0] - center[0], b = p.x[1] - center[1];
+      return a * a + b * b;
+    }, radius);
+  }
+  // particle_lens.cpp:480-495: position of the largest Mass/Size^3 (float)
+  std::array<double, 3> densest_particle() const {
+    double dmax = -1;
+    std::array<double, 3> x{0, 0, 0};
+    for (const auto &p : data) {
+      const double d = p.Mass / p.Size / p.Size / p.Size;
+      if (d > dmax) {
+        dmax = d;
+        x = {p.x[0], p.x[1], p.x[2]};
+      }
+    }
+    return x;
+  }
+
   // particle_lens.cpp:153-209: records to comoving Mpc / Msun (divided by h),
   // one LensHaloParticles per particle type present
   void CreateHalos(const COSMOLOGY &cosmo, double redshift, double inv_area) {
@@ -480,6 +511,26 @@ class MakeParticleLenses {
       m += p.Mass;
     }
     for (int k = 0; k < 3; ++k) cm_[k] /= m;
+  }
+  template <class R2>
+  void cut(R2 r2of, double radius) {
+    const double radius2 = radius * radius;
+    size_t end = data.size(), i = 0;
+    while (i < end) {
+      if (r2of(data[i]) > radius2) {
+        --nparticles_[data[i].type];
+        --end;
+        std::swap(data[i], data[end]);
+      } else {
+        ++i;
+      }
+    }
+    data.resize(end);
+    int ntypes = 0;
+    for (size_t k : nparticles_) ntypes += k > 0;
+    if (ntypes > 1)
+      std::stable_sort(data.begin(), data.end(),
+                       [](const glb_particle &a, const glb_particle &b) { return a.type < b.type; });
   }
   void shift(std::array<double, 3> x) {
     for (auto &p : data)

@@ -40,11 +40,12 @@
  *        (a = Rsize, b = concentration), 1 = LensHaloRealNSIE (a = sigma,
  *        b = rcore, c = fratio, d = pa); each halo moved to Z with
  *        setZlensDist, as Lens::createFieldPlanes does.
- *   makeparticles FILE FMT NSMOOTH RECENTER OUT
+ *   makeparticles FILE FMT NSMOOTH RECENTER OUT [CUT CX CY CZ RADIUS]
  *        MakeParticleLenses from a glmb file (FMT 0) or a csv file (FMT 3-6,
- *        SimFileFormat::csvFMT; writes FILE_S<NSMOOTH>.glmb beside it) -> OUT: the
- *        particle records; OUT.meta: {1, cm[3], bbox_ll[3], bbox_ur[3],
- *        z_original, nparticles[6]}, or {0} when the constructor throws.
+ *        SimFileFormat::csvFMT; writes FILE_S<NSMOOTH>.glmb beside it), then
+ *        radialCut (CUT 1) or cylindricalCut (CUT 2) -> OUT: the particle
+ *        records; OUT.meta: {1, cm[3], bbox_ll[3], bbox_ur[3], z_original,
+ *        nparticles[6], densest_particle[3]}, or {0} when the constructor throws.
  *   particlefile FILE Z NSMOOTH MULTIMASS INV_AREA MINPSIZE MASSSCALING RECENTER TX TY XFILE N OUT
  *        LensHaloParticles from an ascii position file (reads or writes
  *        FILE.<NSMOOTH>sizes) -> force_halo at N physical positions.
@@ -382,8 +383,10 @@ int main() {
       write_time(tf, std::chrono::duration<double>(t1 - t0).count());
     } else if (cmd == "makeparticles") {
       std::string file, out;
-      int fmt, nsmooth, recenter;
+      int fmt, nsmooth, recenter, cut = 0;
+      double ccx = 0, ccy = 0, ccz = 0, crad = 0;
       in >> file >> fmt >> nsmooth >> recenter >> out;
+      in >> cut >> ccx >> ccy >> ccz >> crad;
       const SimFileFormat f = fmt == 0 ? SimFileFormat::glmb
                               : fmt == 3 ? SimFileFormat::csv3
                               : fmt == 4 ? SimFileFormat::csv4
@@ -392,6 +395,8 @@ int main() {
       try {
         std::unique_ptr<MakeParticleLenses> m(fmt == 0 ? new MakeParticleLenses(file, recenter != 0)
                                                        : new MakeParticleLenses(file, f, nsmooth, recenter != 0));
+        if (cut == 1) m->radialCut(Point_3d<>(ccx, ccy, ccz), crad);
+        if (cut == 2) m->cylindricalCut(Point_2d(ccx, ccy), crad);
         FILE *fp = fopen(out.c_str(), "wb");
         fwrite(m->data.data(), sizeof(PT), m->data.size(), fp);
         fclose(fp);
@@ -399,6 +404,10 @@ int main() {
         m->getBoundingBox(lo, hi);
         meta = {1.0, cm[0], cm[1], cm[2], lo[0], lo[1], lo[2], hi[0], hi[1], hi[2], m->getZoriginal()};
         for (size_t k : m->getnp()) meta.push_back((double)k);
+        Point_3d<> dp = m->densest_particle();
+        meta.push_back(dp[0]);
+        meta.push_back(dp[1]);
+        meta.push_back(dp[2]);
       } catch (const std::exception &e) {
         meta = {0.0};
       }

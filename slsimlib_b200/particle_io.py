@@ -271,6 +271,55 @@ class MakeParticleLenses:
         self.cm = self.cm - x
         self.halos = []
 
+    def _cut(self, r2: np.ndarray, radius: float) -> None:
+        # particle_lens.cpp:447-478 / 497-520: a particle beyond the radius is
+        # swapped with the last one still kept, and the scan goes on from the
+        # same place; the kept records are then sorted by type if more than one
+        # type has particles (stable here; the reference's std::sort leaves the
+        # order within a type unspecified)
+        d = self.data.copy()
+        out = r2 > float(radius) * float(radius)
+        i, end = 0, len(d)
+        while i < end:
+            if out[i]:
+                self.nparticles[int(d["type"][i])] -= 1
+                end -= 1
+                d[[i, end]] = d[[end, i]]
+                out[[i, end]] = out[[end, i]]
+            else:
+                i += 1
+        d = d[:end]
+        if sum(1 for k in self.nparticles if k > 0) > 1:
+            d = d[np.argsort(d["type"], kind="stable")]
+        self.data = d
+
+    def radialCut(self, center: Sequence[float], radius: float) -> None:
+        """Removes the particles farther than radius (Mpc/h) from center."""
+        c = np.asarray(center, dtype=np.float64)
+        x = self.data["x"].astype(np.float64)
+        a, b, e = x[:, 0] - c[0], x[:, 1] - c[1], x[:, 2] - c[2]
+        self._cut(a * a + b * b + e * e, radius)
+
+    def cylindricalCut(self, center: Sequence[float], radius: float) -> None:
+        """Removes the particles farther than radius (Mpc/h) from center in x, y."""
+        c = np.asarray(center, dtype=np.float64)
+        x = self.data["x"].astype(np.float64)
+        a, b = x[:, 0] - c[0], x[:, 1] - c[1]
+        self._cut(a * a + b * b, radius)
+
+    def densest_particle(self) -> np.ndarray:
+        """particle_lens.cpp:480-495: position of the largest Mass/Size^3
+        (float arithmetic, first maximum)."""
+        m, sz = self.data["Mass"], self.data["Size"]
+        with np.errstate(divide="ignore", invalid="ignore"):
+            d = ((m / sz) / sz) / sz
+        best, x = -1.0, np.zeros(3)
+        for i in range(len(d)):
+            if float(d[i]) > best:
+                best = float(d[i])
+                x = self.data["x"][i].astype(np.float64)
+        return x
+
     def getnp(self) -> List[int]:
         return list(self.nparticles)
 

@@ -315,12 +315,15 @@ class RefDriver:
         self.run([f"smooth {pf} {len(particles)} {int(nsmooth)} {of} {tf}"])
         return np.fromfile(of).astype(np.float32), float(np.fromfile(tf)[0])
 
-    def make_particles(self, filename, fmt, nsmooth, recenter=False):
-        """MakeParticleLenses in the reference -> (records, meta) or (None, None)
-        when it throws; meta = {cm[3], bbox_ll[3], bbox_ur[3], z_original,
-        nparticles[6]}."""
+    def make_particles(self, filename, fmt, nsmooth, recenter=False, cut=0, center=(0.0, 0.0, 0.0), radius=0.0):
+        """MakeParticleLenses in the reference (then radialCut for cut 1,
+        cylindricalCut for cut 2) -> (records, meta) or (None, None) when it
+        throws; meta = {cm[3], bbox_ll[3], bbox_ur[3], z_original, nparticles[6],
+        densest_particle[3]}."""
         of = self._file()
-        self.run([f"makeparticles {filename} {int(fmt)} {int(nsmooth)} {int(recenter)} {of}"])
+        c = " ".join(repr(float(v)) for v in center)
+        self.run([f"makeparticles {filename} {int(fmt)} {int(nsmooth)} {int(recenter)} {of} {int(cut)} {c} "
+                  f"{float(radius)!r}"])
         meta = np.fromfile(of + ".meta")
         if meta[0] == 0:
             return None, None

@@ -116,7 +116,8 @@ def test_csv5_and_glmb_match_reference(tmp_path, recenter):
     assert np.array_equal(m.data.view(np.uint8), ref.view(np.uint8))
     lo, hi = m.getBoundingBox()
     assert np.array_equal(np.concatenate([m.getCenterOfMass(), lo, hi]), meta[:9])
-    assert m.getZoriginal() == meta[9] and m.getnp() == [int(v) for v in meta[10:]]
+    assert m.getZoriginal() == meta[9] and m.getnp() == [int(v) for v in meta[10:16]]
+    assert np.array_equal(m.densest_particle(), meta[16:19])
     g_ref, g_our = tmp_path / "ref" / "sim.csv_S16.glmb", tmp_path / "our" / "sim.csv_S16.glmb"
     assert open(g_ref, "rb").read() == open(g_our, "rb").read()
     # the glmb constructor on the reference's file
@@ -199,6 +200,12 @@ def test_cpp_mirror_particle_files_match_reference(tmp_path, recenter):
     R = H.RefDriver()
     R.write_sizes(ref, 64, str(tmp_path / "ref.sizes"))
     assert open(tmp_path / "ref.sizes", "rb").read() == open(out + ".sizes", "rb").read()
+    if not recenter:
+        cx, cy, cz, rad = np.fromfile(out + ".cut.meta")
+        cut_ref, _ = R.make_particles(str(tmp_path / "ref" / "sim.csv"), 5, 16, False, 1, (cx, cy, cz), rad)
+        got_cut = np.fromfile(out + ".cut.bin", dtype=synth.PARTICLE_DTYPE)
+        assert 0 < len(got_cut) < len(p)
+        assert np.array_equal(got_cut.view(np.uint8), cut_ref.view(np.uint8))
 
 
 def write_ascii(path, p, multimass=True):
@@ -249,3 +256,21 @@ def test_particle_lens_from_ascii_file_matches_reference(tmp_path, recenter, rot
                                                  0.0, minp, mscale)
     m2, cols2 = force_err(pack(*halo2.force_halo(xx)), ref2)
     assert m2 < RTOL64, cols2
+
+
+@needs_ref
+@pytest.mark.parametrize("cut", [1, 2])
+def test_cuts_match_reference(tmp_path, cut):
+    """radialCut / cylindricalCut: the records kept, in the reference's order."""
+    p = particles(900, 10)
+    centre = (float(np.median(p["x"][:, 0])), float(np.median(p["x"][:, 1])), float(np.median(p["x"][:, 2])))
+    for who in ("ref", "our"):
+        os.makedirs(tmp_path / who)
+        write_csv(tmp_path / who / "sim.csv", p, 5)
+    ref, meta = H.RefDriver().make_particles(str(tmp_path / "ref" / "sim.csv"), 5, 16, False, cut, centre, 0.05)
+    m = pio.MakeParticleLenses(str(tmp_path / "our" / "sim.csv"), "csv5", 16, False)
+    (m.radialCut if cut == 1 else m.cylindricalCut)(centre if cut == 1 else centre[:2], 0.05)
+    assert 0 < len(m.data) < len(p)
+    assert np.array_equal(m.data.view(np.uint8), ref.view(np.uint8))
+    assert m.getnp() == [int(v) for v in meta[10:16]]
+    assert np.array_equal(m.densest_particle(), meta[16:19])
