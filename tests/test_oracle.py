@@ -204,7 +204,7 @@ def test_smoothing_oracle_errors():
 @pytest.mark.skipif(not H.ref_available(), reason="reference not compiled here")
 def test_smoothing_oracle_matches_reference_live():
     rng = np.random.default_rng(77)
-    for n, ns in ((6000, 32), (65, 32), (2500, 1)):
+    for n, ns in ((6000, 32), (65, 32), (2500, 1), (3, 1), (4, 1), (5, 2), (7, 3), (8, 3)):
         p = synth.nfw_particles(rng, n, 3e14, 4.0, 0.3, 0.0)
         ref, _ = H.RefDriver().smoothing(p, ns)
         assert np.array_equal(H.oracle_smoothing(p, ns), ref), (n, ns)
