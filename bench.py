@@ -108,57 +108,94 @@ def fp32_peak_tflops(sm_mhz):
 
 
 def error_stats(x, y, A, yref, Aref):
-    a, ar = x - y, x - yref
-    na = np.hypot(ar[:, 0], ar[:, 1])
-    keep = na > 1e-6 * np.median(na)
-    ea = np.hypot(*(a - ar).T)[keep] / na[keep]
+    """Relative errors of alpha, kappa, gamma and invmag against a reference
+    result (median, 99.9th percentile); floors of 1e-3 on the kappa and gamma
+    denominators, invmag where |invmag_ref| > 0.05."""
+    from tests.harness import error_stats as es
+    return es(x, y, A, yref, Aref)
 
-    def der(M):
-        return (1 - (M[:, 0] + M[:, 3]) / 2, np.hypot((M[:, 0] - M[:, 3]) / 2, (M[:, 1] + M[:, 2]) / 2),
-                M[:, 0] * M[:, 3] - M[:, 1] * M[:, 2])
-    k, g, inv = der(A)
-    kr, gr, invr = der(Aref)
-    m = np.abs(invr) > 0.05
-    out = {}
-    for name, e in (("alpha", ea), ("kappa", np.abs(k - kr) / np.abs(kr)), ("gamma", np.abs(g - gr) / np.abs(gr)),
-                    ("invmag", np.abs(inv - invr)[m] / np.abs(invr[m]))):
-        out[name] = {"median": float(np.median(e)), "p999": float(np.percentile(e, 99.9))}
+
+def attribution(spec, lens, x, nsample=16384, seed=78):
+    """Where the split form's kappa/gamma/invmag error comes from, on a seeded
+    sample of the grid's rays (tests.harness.PlaneRecursion: the recursion over
+    the library's per-plane GPU forces):
+      evaluation   -- split kappa/gamma at the FP64 form's plane positions
+                      (deflection from the FP64 form);
+      propagated   -- split deflection, FP64 kappa/gamma at the positions it
+                      gives;
+      fp64_noise_* -- the FP64 form with every plane's deflection perturbed by
+                      relative Gaussian noise of that size (the conditioning of
+                      the light cone: no error in kappa/gamma evaluation);
+    all against the unperturbed FP64 recursion, plus the sample's final fields."""
+    import slsimlib_b200 as glb
+    from tests.harness import PlaneRecursion
+    xs = x[sample_indices(int(round(np.sqrt(len(x)))), nsample, seed)]
+    R = PlaneRecursion(spec, lens)
+    F, S = glb.PREC_FP64, glb.PREC_SPLIT
+    y0, A0 = R.shoot(xs, F, F)
+    out = {"rays": len(xs)}
+    for name, (pa, pg, eps) in {"evaluation": (F, S, 0.0), "propagated": (S, F, 0.0),
+                                "fp64_noise_1e-8": (F, F, 1e-8), "fp64_noise_1e-10": (F, F, 1e-10)}.items():
+        y, A = R.shoot(xs, pa, pg, noise=eps, seed=5)
+        out[name] = error_stats(xs, y, A, y0, A0)
+    k = 1 - (A0[:, 0] + A0[:, 3]) / 2
+    inv = A0[:, 0] * A0[:, 3] - A0[:, 1] * A0[:, 2]
+    out["fields"] = {"kappa_median": float(np.median(k)), "invmag_median": float(np.median(inv)),
+                     "frac_abs_invmag_below_0.05": float(np.mean(np.abs(inv) < 0.05))}
     return out
+
+
+def sample_indices(n1d, nsample, seed):
+    n = n1d * n1d
+    return np.sort(np.random.default_rng(seed).choice(n, size=min(nsample, n), replace=False))
 
 
 def cpu_reference(spec, n1d, nsample, seed=77):
     """Times the reference (oracle/_ref) Lens::rayshooterInternal on a seeded
-    sample of the grid's rays; returns (rays/s, threads, seconds, sample)."""
+    sample of the grid's rays; returns (rays/s, threads, seconds, sample
+    description, sample indices, y, A) -- y and A are the reference's results
+    for those rays, kept for the parity check of the GPU's FP64 form."""
     from tests import harness as H
     from slsimlib_b200 import synth
     if not H.ref_available():
         return None
     x = synth.grid_positions(n1d, range_rad=FIELD_ARCSEC * synth.ARCSEC)
-    idx = np.sort(np.random.default_rng(seed).choice(len(x), size=nsample, replace=False))
+    idx = sample_indices(n1d, nsample, seed)
     R = H.RefDriver()
-    tf = R._file()
-    R.run([f"threads {tf}"])
-    threads = int(np.fromfile(tf)[0])
-    _, _, secs = R.rays(spec, x[idx])
-    return nsample / secs, threads, secs, f"{nsample} seeded rays of the {n1d}x{n1d} grid, all planes"
+    threads = R.threads()
+    y, A, secs = R.rays(spec, x[idx])
+    return (len(idx) / secs, threads, secs, f"{len(idx)} seeded rays of the {n1d}x{n1d} grid, all planes", idx,
+            y, A)
+
+
+def parity_vs_reference(y_gpu, A_gpu, y_ref, A_ref):
+    """The GPU's FP64 form against the reference's own rayshooterInternal on
+    the same rays: relative source-position error (max, p99.9) and the largest
+    absolute Jacobian difference."""
+    ey = np.hypot(*(y_gpu - y_ref).T) / np.hypot(*y_ref.T)
+    return {"rays": int(len(y_ref)), "y_max_rel": float(ey.max()), "y_p999_rel": float(np.percentile(ey, 99.9)),
+            "A_max_abs": float(np.max(np.abs(A_gpu - A_ref)))}
 
 
 def run_reference_arm(args, rank):
+    """The reference's own CPU rayshooter (oracle/_ref: Lens::rayshooterInternal
+    compiled from the reference's sources) on the host cores: one process
+    builds the lens once, then each warm-up and timed step shoots a new seeded
+    sample of the grid's rays through the reference's Point* overload."""
     if rank != 0:
         return
     from tests import harness as H
+    from slsimlib_b200 import synth
     if not H.ref_available():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/glamer_ref not built"}))
         return
     spec, n1d = workload(args.small)
-    vals = []
     nsample = 2048 if args.small else 16384
-    threads = 0
-    for s in range(args.warmup + args.steps):
-        r = cpu_reference(spec, n1d, nsample, seed=100 + s)
-        if s >= args.warmup:
-            vals.append(r[0])
-        threads = r[1]
+    x = synth.grid_positions(n1d, range_rad=FIELD_ARCSEC * synth.ARCSEC)
+    R = H.RefDriver()
+    threads = R.threads()
+    res = R.rays_batches(spec, [x[sample_indices(n1d, nsample, 100 + s)] for s in range(args.warmup + args.steps)])
+    vals = [nsample / r[2] for r in res[args.warmup:]]
     v = float(np.median(vals))
     n = n1d * n1d
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "rays/s", "n_gpus": args.gpus,
@@ -168,7 +205,8 @@ def run_reference_arm(args, rank):
                        "sample_rays_per_step": nsample},
             "cpu_baseline": {"value": v, "unit": "rays/s", "cores": threads, "kind": "reference",
                              "sample": f"{nsample} seeded rays of the grid per step (a new sample each step), all "
-                                       f"planes, rate extrapolated per ray"},
+                                       f"planes, rate extrapolated per ray; lens built once in one reference "
+                                       f"process, each step one rayshooterInternal(n, Point*) call"},
             "e2e": {"value": v, "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
@@ -640,6 +678,7 @@ def main():
     k_ms, tot_ms = lens.last_timing()
     y32, A32 = y.cpu().numpy(), A.cpu().numpy()
     errs = error_stats(x_host, y32, A32, y64, A64)
+    attrib = attribution(spec, lens, x_host) if rank == 0 and not args.small else None
 
     # end to end through the host C ABI (pinned host buffers, copies timed)
     xp = torch.from_numpy(x_host).pin_memory()
@@ -685,6 +724,7 @@ def main():
                        "parallelism": f"replicated lens, one full grid per GPU"},
             "plain_fp64": {"value": n / (fp64_ms / 1e3), "unit": "rays/s", "ms": fp64_ms},
             "errors_vs_fp64": errs,
+            "kappa_gamma_attribution": attrib,
             "e2e": {"value": world * n * args.steps / e2e_s, "unit": "rays/s", "h2d_bytes_per_step": 16 * n,
                     "d2h_bytes_per_step": 48 * n},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
@@ -704,6 +744,8 @@ def main():
         if cpu:
             line["cpu_baseline"] = {"value": cpu[0], "unit": "rays/s", "cores": cpu[1], "kind": "reference",
                                     "sample": cpu[3], "seconds": cpu[2]}
+            # the plain FP64 GPU form against the reference's own results on the sampled rays
+            line["parity_vs_reference"] = parity_vs_reference(y64[cpu[4]], A64[cpu[4]], cpu[5], cpu[6])
         print(json.dumps(line))
     if world > 1:
         dist.barrier()

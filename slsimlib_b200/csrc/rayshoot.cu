@@ -399,7 +399,108 @@ struct StepArgs {
   const double *src_ray;
   double charge;
   unsigned long long *counts;  // V F P B S Wn Wp totals (counting launches only)
+  // The plane's particle tree and its offset (posHalo * Dist) when the plane
+  // holds exactly one particle halo (k_plane_step_split with PTREE): read from
+  // kernel parameter space, so the walk's pointers and scalars are uniform
+  // operands rather than per-thread registers.
+  TreeDev tree;
+  double tree_px, tree_py;
 };
+
+// The recursion of include/lens.h:1003-1066 for ray slot k once the plane's
+// summed halo forces are known (al: the plane's deflection with the sign of
+// LensPlaneSingular::force, planes.cpp:151-152; kap, g0, g1 summed).
+__device__ __forceinline__ void recursion_step(const StepArgs &a, size_t k, double al0, double al1, double kap,
+                                               double g0, double g1) {
+  const size_t n = a.n;
+  double *st = a.st;
+  int jmax = a.jmax;
+  double dls = a.dls_ds, dds = a.d_ds;
+  if (a.jmax_ray) {
+    jmax = a.jmax_ray[k];
+    dls = a.src_ray[2 * k];
+    dds = a.src_ray[2 * k + 1];
+  }
+  const PlaneDev &P = a.planes[a.j];
+  double G0 = kap + g0, G1 = g1, G2 = g1, G3 = kap - g0;
+  G0 *= P.Gfac;
+  G1 *= P.Gfac;
+  G2 *= P.Gfac;
+  G3 *= P.Gfac;
+  double th0 = st[0 * n + k], th1 = st[1 * n + k];
+  double sa0 = st[2 * n + k] - a.charge * al0;
+  double sa1 = st[3 * n + k] - a.charge * al1;
+  double aa, bb;
+  if (a.j < jmax - 1) {
+    aa = P.aa;
+    bb = P.bb;
+  } else {
+    aa = dls;
+    bb = dds;
+  }
+  th0 = bb * th0 + aa * sa0;
+  th1 = bb * th1 + aa * sa1;
+  const double A0 = st[4 * n + k], A1 = st[5 * n + k], A2 = st[6 * n + k], A3 = st[7 * n + k];
+  double s0 = st[8 * n + k], s1 = st[9 * n + k], s2 = st[10 * n + k], s3 = st[11 * n + k];
+  // SumPrevAG -= G * A (Matrix2x2 product, include/point.h:249-258)
+  s0 -= G0 * A0 + G1 * A2;
+  s1 -= G0 * A1 + G1 * A3;
+  s2 -= G2 * A0 + G3 * A2;
+  s3 -= G2 * A1 + G3 * A3;
+  st[0 * n + k] = th0;
+  st[1 * n + k] = th1;
+  st[2 * n + k] = sa0;
+  st[3 * n + k] = sa1;
+  st[4 * n + k] = A0 * bb + s0 * aa;
+  st[5 * n + k] = A1 * bb + s1 * aa;
+  st[6 * n + k] = A2 * bb + s2 * aa;
+  st[7 * n + k] = A3 * bb + s3 * aa;
+  st[8 * n + k] = s0;
+  st[9 * n + k] = s1;
+  st[10 * n + k] = s2;
+  st[11 * n + k] = s3;
+}
+
+// Split-form plane step for a plane holding exactly one particle halo (its
+// tree in a.tree) and any number of analytic halos.  Only the ray slot stays
+// live across the tree walk: the walk's FP64 totals sit in shared memory
+// (sacc, five doubles per thread at a stride of five, which maps a half-warp's
+// 64-bit accesses onto distinct banks), and the recursion reloads theta, the
+// plane constants and the source-plane scalars after the walk.  The particle
+// halo's terms are added first, then the analytic halos' in insertion order.
+__device__ __forceinline__ void plane_step_split_ptree(const StepArgs &a, double *sacc) {
+  const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  const bool inrange = k < a.n;
+  const int jmax = (a.jmax_ray && inrange) ? a.jmax_ray[k] : a.jmax;
+  const bool valid = inrange && a.j < jmax;
+  if (!__any_sync(kFull, valid)) return;
+  double *acc = sacc + 5 * threadIdx.x;
+  for (int c = 0; c < 5; ++c) acc[c] = 0.0;
+  double rx = 0, ry = 0;
+  if (valid) {
+    const double D = a.planes[a.j].Dphys;
+    rx = a.st[k] * D - a.tree_px;
+    ry = a.st[a.n + k] * D - a.tree_py;
+  }
+  particle_halo_acc<GLB_PREC_SPLIT, false>(a.tree, rx, ry, valid, acc);
+  if (!valid) return;
+  // LensHaloParticles::force_halo negates alpha (particle_halo.h:432-433) and
+  // LensPlaneSingular::force subtracts it
+  double al0 = acc[0], al1 = acc[1], kap = acc[2], g0 = acc[3], g1 = acc[4];
+  const PlaneDev &P = a.planes[a.j];
+  for (int h = 0; h < P.nhalo; ++h) {
+    const HaloDev *H = a.halos + P.halo0 + h;
+    if (H->kind == HALO_PARTICLES) continue;
+    const double D = P.Dphys;
+    const Force5 f = analytic_halo(H, &a.tab, a.st[k] * D - H->px, a.st[a.n + k] * D - H->py);
+    al0 -= f.a0;
+    al1 -= f.a1;
+    kap += f.k;
+    g0 += f.g0;
+    g1 += f.g1;
+  }
+  recursion_step(a, k, al0, al1, kap, g0, g1);
+}
 
 // One lens plane for every ray: LensPlaneSingular::force + the recursion of
 // include/lens.h:1003-1066.
@@ -517,9 +618,16 @@ template <int PREC, bool COUNT = false, bool FIELD = false>
 __global__ void __launch_bounds__(128) k_plane_step(StepArgs a) {
   plane_step<PREC, COUNT, FIELD>(a);
 }
-template <bool FIELD = false>
-__global__ void __launch_bounds__(128, 8) k_plane_step_split(StepArgs a) {
-  plane_step<GLB_PREC_SPLIT, false, FIELD>(a);
+// PTREE: the plane holds exactly one particle halo, whose tree is a.tree
+// (no field plane on such a launch).
+template <bool FIELD = false, bool PTREE = false>
+__global__ void __launch_bounds__(128, 8) k_plane_step_split(const __grid_constant__ StepArgs a) {
+  if (PTREE) {
+    __shared__ double sacc[5 * 128];
+    plane_step_split_ptree(a, sacc);
+  } else {
+    plane_step<GLB_PREC_SPLIT, false, FIELD>(a);
+  }
 }
 
 // force2D_recur / force_halo at arbitrary positions (walk-level API, with phi).
@@ -787,6 +895,49 @@ int ensure_ws(glb_lens *l, size_t n, bool per_ray) {
   return 0;
 }
 
+// One launch per plane, in order.  Split-form planes that hold exactly one
+// particle halo pass its tree in the kernel parameters (PTREE); planes with
+// a field plane use the FIELD instances.
+int launch_plane_steps(const glb_lens *l, StepArgs &a, int jmax_launch, int precision, cudaStream_t s,
+                       const unsigned long long *d_counts) {
+  const size_t n = a.n;
+  for (int j = 0; j < jmax_launch; ++j) {
+    a.j = j;
+    const bool fld = l->plane_field[j] != 0;
+    int npart = 0;
+    const glb_halo *ph = nullptr;
+    for (const glb_halo *h : l->planes[j]->halos)
+      if (h->kind == HALO_PARTICLES) {
+        ++npart;
+        ph = h;
+      }
+    const bool ptree = npart == 1 && ph->tree && !fld;
+    memset(&a.tree, 0, sizeof(a.tree));
+    a.tree_px = a.tree_py = 0;
+    if (ptree) {
+      a.tree = ph->tree->dev;
+      a.tree_px = ph->theta[0] * ph->Dist;  // LensHalo::getX, as make_halo_dev
+      a.tree_py = ph->theta[1] * ph->Dist;
+    }
+    if (d_counts && fld)
+      k_plane_step<GLB_PREC_FP64, true, true><<<nblk(n, 128), 128, 0, s>>>(a);
+    else if (d_counts)
+      k_plane_step<GLB_PREC_FP64, true><<<nblk(n, 128), 128, 0, s>>>(a);
+    else if (precision == GLB_PREC_SPLIT && fld)
+      k_plane_step_split<true><<<nblk(n, 128), 128, 0, s>>>(a);
+    else if (precision == GLB_PREC_SPLIT && ptree)
+      k_plane_step_split<false, true><<<nblk(n, 128), 128, 0, s>>>(a);
+    else if (precision == GLB_PREC_SPLIT)
+      k_plane_step_split<<<nblk(n, 128), 128, 0, s>>>(a);
+    else if (fld)
+      k_plane_step<GLB_PREC_FP64, false, true><<<nblk(n, 128), 128, 0, s>>>(a);
+    else
+      k_plane_step<GLB_PREC_FP64><<<nblk(n, 128), 128, 0, s>>>(a);
+  }
+  CKR(cudaGetLastError());
+  return 0;
+}
+
 // The whole ray-shooting pass on device buffers, enqueued on stream s.
 int rayshoot_device(glb_lens *l, size_t n, const double *x, const double *zs, double *y, double *A,
                     int precision, cudaStream_t s, unsigned long long *d_counts = nullptr) {
@@ -853,22 +1004,7 @@ int rayshoot_device(glb_lens *l, size_t n, const double *x, const double *zs, do
     }
   }
   CKR(cudaEventRecord(l->ev[1], s));
-  for (int j = 0; j < jmax_launch; ++j) {
-    a.j = j;
-    const bool fld = l->plane_field[j] != 0;
-    if (d_counts && fld)
-      k_plane_step<GLB_PREC_FP64, true, true><<<nblk(n, 128), 128, 0, s>>>(a);
-    else if (d_counts)
-      k_plane_step<GLB_PREC_FP64, true><<<nblk(n, 128), 128, 0, s>>>(a);
-    else if (precision == GLB_PREC_SPLIT && fld)
-      k_plane_step_split<true><<<nblk(n, 128), 128, 0, s>>>(a);
-    else if (precision == GLB_PREC_SPLIT)
-      k_plane_step_split<<<nblk(n, 128), 128, 0, s>>>(a);
-    else if (fld)
-      k_plane_step<GLB_PREC_FP64, false, true><<<nblk(n, 128), 128, 0, s>>>(a);
-    else
-      k_plane_step<GLB_PREC_FP64><<<nblk(n, 128), 128, 0, s>>>(a);
-  }
+  if (int rc = launch_plane_steps(l, a, jmax_launch, precision, s, d_counts)) return rc;
   CKR(cudaEventRecord(l->ev[2], s));
   k_finish<<<nblk(n, 256), 256, 0, s>>>(l->st.p, l->perm.p, n, y, A);
   CKR(cudaEventRecord(l->ev[3], s));
@@ -1999,18 +2135,7 @@ extern "C" int glb_lens_rayshoot_noalloc(glb_lens *l, size_t n, const double *x_
       jmax_launch = jm;
     }
   }
-  for (int j = 0; j < jmax_launch; ++j) {
-    a.j = j;
-    const bool fld = l->plane_field[j] != 0;
-    if (precision == GLB_PREC_SPLIT && fld)
-      k_plane_step_split<true><<<nblk(n, 128), 128, 0, s>>>(a);
-    else if (precision == GLB_PREC_SPLIT)
-      k_plane_step_split<<<nblk(n, 128), 128, 0, s>>>(a);
-    else if (fld)
-      k_plane_step<GLB_PREC_FP64, false, true><<<nblk(n, 128), 128, 0, s>>>(a);
-    else
-      k_plane_step<GLB_PREC_FP64><<<nblk(n, 128), 128, 0, s>>>(a);
-  }
+  if (int rc = launch_plane_steps(l, a, jmax_launch, precision, s, nullptr)) return rc;
   k_finish<<<nblk(n, 256), 256, 0, s>>>(st, perm, n, y_dev, A_dev);
   CKR(cudaGetLastError());
   return 0;

@@ -254,6 +254,113 @@ def oracle_smoothing(particles: np.ndarray, nsmooth: int) -> np.ndarray:
     return p["Size"].copy()
 
 
+# ------------------------------------------- error attribution (GPU, library)
+class PlaneRecursion:
+    """The multi-plane recursion of include/lens.h:1003-1066 restated in numpy
+    over per-plane forces computed by the library on the GPU (a
+    TreeQuadParticles per particle plane with LensHaloParticles' parameters,
+    the analytic haloes' force_halo).  The deflection and the shear/convergence
+    of each plane can come from different precision forms, and the deflection
+    can be perturbed, which separates the split form's per-plane evaluation
+    error from the error that earlier planes' deflections carry into later
+    planes' positions.  Particle and analytic (NSIE / NFW) planes only."""
+
+    def __init__(self, spec: synth.LensSpec, lens):
+        import slsimlib_b200 as glb
+        self.glb = glb
+        self.z, self.Dl, self.dDl = lens.planes()
+        self.np = lens.getNplanes()
+        self.charge = 4 * np.pi * synth.GRAV
+        cosmo = synth.Cosmology()
+        self.halos = [[] for _ in range(self.np)]
+        for h in spec.halos:
+            if isinstance(h, synth.FieldPlane):
+                raise TypeError("field planes are not supported")
+            zh = float(np.float32(h.z)) if isinstance(h, synth.ParticlePlane) else float(h.z)
+            j = int(np.argmin(np.abs(self.z[:self.np] - zh)))
+            off = np.array(h.theta) * cosmo.angdist(zh)
+            if isinstance(h, synth.ParticlePlane):
+                obj = glb.TreeQuadParticles(h.particles, inv_area=h.inv_area, bucket=20, theta_force=0.1,
+                                            inv_screening_scale=h.max_range)
+            else:
+                obj = glb.halo_from_spec(h)
+            self.halos[j].append((isinstance(h, synth.ParticlePlane), obj, off))
+
+    def plane_force(self, j, xx, prec):
+        """Plane j at physical positions xx: (alpha (n,2) with the sign of
+        LensPlaneSingular::force, kappa, gamma0, gamma1)."""
+        import torch
+        n = len(xx)
+        al = np.zeros((n, 2)); kap = np.zeros(n); g0 = np.zeros(n); g1 = np.zeros(n)
+        for part, obj, off in self.halos[j]:
+            xc = np.ascontiguousarray(xx - off)
+            if part:
+                r = torch.from_numpy(xc).cuda()
+                o = torch.empty((n, 5), dtype=torch.float64, device="cuda")
+                torch.cuda.synchronize()
+                obj.force_device(n, r.data_ptr(), o.data_ptr(), prec, None)
+                torch.cuda.synchronize()
+                o = o.cpu().numpy()
+                # force_halo negates the walk's alpha, force subtracts it
+                al += o[:, :2]; kap += o[:, 2]; g0 += o[:, 3]; g1 += o[:, 4]
+            else:
+                a, k, g, _ = obj.force_halo(xc)
+                al -= a; kap += k; g0 += g[:, 0]; g1 += g[:, 1]
+        return al, kap, g0, g1
+
+    def shoot(self, x, alpha_prec, G_prec, noise=0.0, seed=0):
+        """y (n,2), A (n,4) with the deflection from alpha_prec (times
+        1 + noise * N(0,1) per component) and kappa/gamma from G_prec, both
+        evaluated at the positions this recursion produces."""
+        rs = np.random.default_rng(seed)
+        x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1, 2)
+        n = len(x)
+        th, sa = x.copy(), x.copy()
+        A = np.tile([1.0, 0.0, 0.0, 1.0], (n, 1))
+        s = A.copy()
+        z, Dl, dDl, ch = self.z, self.Dl, self.dDl, self.charge
+        for j in range(self.np):
+            xx = th * (Dl[j] / (1 + z[j]))
+            fa = self.plane_force(j, xx, alpha_prec)
+            fg = fa if G_prec == alpha_prec else self.plane_force(j, xx, G_prec)
+            al = fa[0] * (1 + noise * rs.standard_normal(fa[0].shape)) if noise else fa[0]
+            Gf = ch * Dl[j] / (1 + z[j])
+            G0, G1, G3 = Gf * (fg[1] + fg[2]), Gf * fg[3], Gf * (fg[1] - fg[2])
+            sa = sa - ch * al
+            aa, bb = dDl[j + 1] / Dl[j + 1], Dl[j] / Dl[j + 1]
+            th = bb * th + aa * sa
+            s = np.stack([s[:, 0] - (G0 * A[:, 0] + G1 * A[:, 2]), s[:, 1] - (G0 * A[:, 1] + G1 * A[:, 3]),
+                          s[:, 2] - (G1 * A[:, 0] + G3 * A[:, 2]), s[:, 3] - (G1 * A[:, 1] + G3 * A[:, 3])], 1)
+            A = A * bb + s * aa
+        return th, A
+
+
+def error_stats(x, y, A, yref, Aref, kappa_floor=1e-3, gamma_floor=1e-3):
+    """Median and 99.9th percentile of the relative errors of alpha = x - y,
+    kappa = 1 - (a0 + a3)/2, |gamma| and invmag = det A against a reference
+    result.  Denominators: |alpha_ref| (rays below 1e-6 of the median |alpha|
+    left out), max(|kappa_ref|, kappa_floor), max(|gamma_ref|, gamma_floor);
+    invmag only away from critical curves, |invmag_ref| > 0.05."""
+    a, ar = x - y, x - yref
+    na = np.hypot(ar[:, 0], ar[:, 1])
+    keep = na > 1e-6 * np.median(na)
+    ea = np.hypot(*(a - ar).T)[keep] / na[keep]
+
+    def der(M):
+        return (1 - (M[:, 0] + M[:, 3]) / 2, np.hypot((M[:, 0] - M[:, 3]) / 2, (M[:, 1] + M[:, 2]) / 2),
+                M[:, 0] * M[:, 3] - M[:, 1] * M[:, 2])
+    k, g, inv = der(A)
+    kr, gr, invr = der(Aref)
+    m = np.abs(invr) > 0.05
+    out = {}
+    for name, e in (("alpha", ea), ("kappa", np.abs(k - kr) / np.maximum(np.abs(kr), kappa_floor)),
+                    ("gamma", np.abs(g - gr) / np.maximum(np.abs(gr), gamma_floor)),
+                    ("invmag", np.abs(inv - invr)[m] / np.abs(invr[m]))):
+        out[name] = {"median": float(np.median(e)) if len(e) else 0.0,
+                     "p999": float(np.percentile(e, 99.9)) if len(e) else 0.0}
+    return out
+
+
 # ------------------------------------------------------- reference driver
 def ref_available() -> bool:
     return os.path.exists(REF_BIN)
@@ -409,3 +516,26 @@ class RefDriver:
         self.run(self.lens_lines(spec) + [cmd])
         o = np.fromfile(of).reshape(-1, 6)
         return o[:, :2], o[:, 2:], float(np.fromfile(tf)[0])
+
+    def rays_batches(self, spec, xs, timeout=3600):
+        """One reference process: the lens is built once, then
+        Lens::rayshooterInternal(n, Point*) runs on each ray array of xs in
+        turn -> [(y, A, seconds of that call)]."""
+        cmds, files = [], []
+        for x in xs:
+            x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1, 2)
+            xf, of, tf = self._file(x), self._file(), self._file()
+            cmds.append(f"points {xf} {len(x)} {of} {tf}")
+            files.append((of, tf))
+        self.run(self.lens_lines(spec) + cmds, timeout=timeout)
+        out = []
+        for of, tf in files:
+            o = np.fromfile(of).reshape(-1, 6)
+            out.append((o[:, :2], o[:, 2:], float(np.fromfile(tf)[0])))
+        return out
+
+    def threads(self) -> int:
+        """The thread count the reference's rayshooterInternal uses on this host."""
+        tf = self._file()
+        self.run([f"threads {tf}"])
+        return int(np.fromfile(tf)[0])

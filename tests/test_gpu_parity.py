@@ -190,6 +190,27 @@ def test_light_cone_matches_oracle_and_reset_source():
     assert np.max(np.abs(A - Ao)) < 1e-9
 
 
+def test_single_plane_full_grid_matches_reference():
+    """The single-plane workload at full size -- 2^18 NFW particles (1e14 Msun,
+    c = 5, z = 0.3, 1 kpc softening), a 512^2 GridMap over 30 arcsec, z_s = 2 --
+    in the FP64 form: against the reference's own GridMap (oracle/_ref) on
+    every ray when it is built here, else against the oracle on 4096 seeded
+    rays of the grid."""
+    spec = synth.single_plane_nfw(seed=1)
+    L = make_lens(spec)
+    rng_rad = 30 * synth.ARCSEC
+    gm = glb.GridMap(L, 512, (0.0, 0.0), rng_rad)
+    if H.ref_available():
+        yr, Ar, _ = H.RefDriver().grid(spec, 512, range_rad=rng_rad)
+        y, A = gm.y, gm.A
+    else:
+        idx = np.sort(np.random.default_rng(8).choice(512 * 512, size=4096, replace=False))
+        yr, Ar = H.OracleLens(spec).rayshoot(synth.grid_positions(512, range_rad=rng_rad)[idx])
+        y, A = gm.y[idx], gm.A[idx]
+    assert np.max(rel_err(y, yr)) < RTOL64
+    assert np.max(np.abs(A - Ar)) < 1e-9
+
+
 def test_lens_edge_cases():
     # no lens plane: identity (internal_rayshooter_multi.cpp:62-76)
     L = glb.Lens(2.0)
@@ -214,47 +235,48 @@ def test_lens_edge_cases():
 
 
 # ------------------------------------------------------- split precision
-def error_percentiles(y, A, yref, Aref, x):
-    """median and 99.9th percentile of |d alpha|/|alpha| and of the kappa,
-    gamma and invmag errors (invmag away from critical curves, |invmag|>0.05)."""
-    a, ar = x - y, x - yref
-    na = np.hypot(ar[:, 0], ar[:, 1])
-    keep = na > 1e-6 * np.median(na)
-    ea = np.hypot(*(a - ar).T)[keep] / na[keep]
-
-    def derived(M):
-        k = 1 - (M[:, 0] + M[:, 3]) / 2
-        g1 = (M[:, 0] - M[:, 3]) / 2
-        g2 = (M[:, 1] + M[:, 2]) / 2
-        inv = M[:, 0] * M[:, 3] - M[:, 1] * M[:, 2]
-        return k, np.hypot(g1, g2), inv
-    k, g, inv = derived(A)
-    kr, gr, invr = derived(Aref)
-    ek = np.abs(k - kr) / np.abs(kr)
-    eg = np.abs(g - gr) / np.abs(gr)
-    m = np.abs(invr) > 0.05
-    ei = np.abs(inv - invr)[m] / np.abs(invr[m])
-    return {n: (float(np.median(e)), float(np.percentile(e, 99.9))) for n, e in
-            (("alpha", ea), ("kappa", ek), ("gamma", eg), ("invmag", ei))}
+def within(st, name, med=1e-6, p999=1e-5):
+    return st[name]["median"] <= med and st[name]["p999"] <= p999
 
 
-@pytest.mark.parametrize("n_total,n_planes", [(200000, 1), (200000, 4)])
-def test_split_precision_deflection_tolerance(n_total, n_planes):
-    """The split form's deflection against the plain FP64 form: median
-    |d alpha|/|alpha| <= 1e-6 and 99.9th percentile <= 1e-5."""
+@pytest.mark.parametrize("n_total,n_planes", [(200000, 1), (200000, 4), (400000, 10)])
+def test_split_precision_tolerance(n_total, n_planes):
+    """The split form against the plain FP64 form (median <= 1e-6, 99.9th
+    percentile <= 1e-5; kappa and gamma relative to max(|ref|, 1e-3), invmag
+    where |invmag_ref| > 0.05).
+
+    The deflection is within the bounds end to end.  Kappa, gamma and invmag
+    are checked where the split form computes them: at the plane positions of
+    the FP64 form (tests.harness.PlaneRecursion, split kappa/gamma with the
+    FP64 deflection) -- on one plane that is the end-to-end result.  Through
+    several planes of particle lenses whose particles have Einstein radii of
+    about their softening length, a deflection difference of FP32 size at one
+    plane moves the ray by enough to change the shear at later planes by more
+    than the bound; the test shows that this is propagation of the deflection
+    difference (split deflection with FP64 kappa/gamma gives the same error)
+    and not an error of the kappa/gamma evaluation."""
     spec = synth.light_cone(seed=41, n_total=n_total, n_planes=n_planes, halos_per_plane=8)
     L = make_lens(spec)
     x = synth.grid_positions(96, range_rad=60 * synth.ARCSEC)
     y64, A64 = L.rayshooterInternal(x, precision=glb.PREC_FP64)
     y32, A32 = L.rayshooterInternal(x, precision=glb.PREC_SPLIT)
-    st = error_percentiles(y32, A32, y64, A64, x)
-    med, p999 = st["alpha"]
-    assert med <= 1e-6 and p999 <= 1e-5, st
+    st = H.error_stats(x, y32, A32, y64, A64)
+    assert within(st, "alpha"), st
     if n_planes == 1:
-        # one plane: kappa, gamma and invmag carry no upstream deflection error
         for name in ("kappa", "gamma", "invmag"):
-            med, p999 = st[name]
-            assert med <= 1e-6 and p999 <= 1e-5, (name, st)
+            assert within(st, name), (name, st)
+        return
+    R = H.PlaneRecursion(spec, L)
+    F, S = glb.PREC_FP64, glb.PREC_SPLIT
+    y0, A0 = R.shoot(x, F, F)
+    assert np.max(rel_err(y0, y64)) < 1e-10 and np.max(np.abs(A0 - A64)) < 1e-7  # the recursion is the library's
+    ev = H.error_stats(x, *R.shoot(x, F, S), y0, A0)
+    for name in ("kappa", "gamma", "invmag"):
+        assert within(ev, name), ("evaluation", name, ev)
+    pr = H.error_stats(x, *R.shoot(x, S, F), y0, A0)
+    for name in ("kappa", "gamma", "invmag"):
+        # the end-to-end error is the propagated one
+        assert 0.5 * st[name]["median"] <= pr[name]["median"] <= 2 * st[name]["median"] + 1e-12, (name, st, pr)
 
 
 # --------------------------------------------- tree-force forms, direct sum
