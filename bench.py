@@ -126,6 +126,8 @@ def attribution(spec, lens, x, nsample=16384, seed=78):
       fp64_noise_* -- the FP64 form with every plane's deflection perturbed by
                       relative Gaussian noise of that size (the conditioning of
                       the light cone: no error in kappa/gamma evaluation);
+      fp64_G_noise_6e-8 -- the FP64 form with every plane's kappa/gamma
+                      perturbed by FP32 unit roundoff;
     all against the unperturbed FP64 recursion, plus the sample's final fields."""
     import slsimlib_b200 as glb
     from tests.harness import PlaneRecursion
@@ -134,9 +136,10 @@ def attribution(spec, lens, x, nsample=16384, seed=78):
     F, S = glb.PREC_FP64, glb.PREC_SPLIT
     y0, A0 = R.shoot(xs, F, F)
     out = {"rays": len(xs)}
-    for name, (pa, pg, eps) in {"evaluation": (F, S, 0.0), "propagated": (S, F, 0.0),
-                                "fp64_noise_1e-8": (F, F, 1e-8), "fp64_noise_1e-10": (F, F, 1e-10)}.items():
-        y, A = R.shoot(xs, pa, pg, noise=eps, seed=5)
+    for name, (pa, pg, eps, geps) in {"evaluation": (F, S, 0.0, 0.0), "propagated": (S, F, 0.0, 0.0),
+                                      "fp64_noise_1e-8": (F, F, 1e-8, 0.0), "fp64_noise_1e-10": (F, F, 1e-10, 0.0),
+                                      "fp64_G_noise_6e-8": (F, F, 0.0, 6e-8)}.items():
+        y, A = R.shoot(xs, pa, pg, noise=eps, seed=5, g_noise=geps)
         out[name] = error_stats(xs, y, A, y0, A0)
     k = 1 - (A0[:, 0] + A0[:, 3]) / 2
     inv = A0[:, 0] * A0[:, 3] - A0[:, 1] * A0[:, 2]
@@ -518,20 +521,18 @@ def _c5_model(seed):
     return synth.light_cone(seed=seed)
 
 
-def run_served(args):
-    """32 resident light-cone models; Poisson request stream at swept rates;
-    request sizes log-uniform in 1e3-5e5 rays in 1-8 Gaussian blobs
-    (sigma 0.05-1 arcsec); z_s uniform in 1-3; split precision."""
-    import multiprocessing as mp
-    import threading
+def served_sweep(models, rates, nreq, seed=5, nslots=3):
+    """Poisson request streams at the given rates against resident light-cone
+    models: request sizes log-uniform in 1e3-5e5 rays in 1-8 Gaussian blobs
+    (sigma 0.05-1 arcsec), z_s uniform in 1-3, split precision.  Returns the
+    per-rate rays/s and p50/p99 request latency (submit to results), the
+    server's statistics and the deflection error of a few served requests
+    against the plain FP64 form."""
     import slsimlib_b200 as glb
     from slsimlib_b200 import synth
-    nm = 32 if not args.small else 4
-    with mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
-        specs = pool.map(_c5_model, [5000 + i for i in range(nm)])
-    models = [make_lens(s) for s in specs]
-    srv = glb.Server(models, max_rays_per_batch=2_000_000, precision=glb.PREC_SPLIT, nslots=3)
-    r = np.random.default_rng(5)
+    nm = len(models)
+    srv = glb.Server(models, max_rays_per_batch=2_000_000, precision=glb.PREC_SPLIT, nslots=nslots)
+    r = np.random.default_rng(seed)
     half = 30 * synth.ARCSEC
 
     def request():
@@ -544,8 +545,7 @@ def run_served(args):
         return int(r.integers(0, nm)), x, float(r.uniform(1, 3))
 
     sweep = []
-    nreq = 120 if not args.small else 30
-    for lam in (5.0, 20.0, 60.0):
+    for lam in rates:
         reqs = [request() for _ in range(nreq)]
         gaps = r.exponential(1 / lam, size=nreq)
         tickets = []
@@ -558,30 +558,39 @@ def run_served(args):
                 time.sleep(d)
             tickets.append(srv.submit(m, x, zs))
         lat, rays = [], 0
-        tdone = 0
         for (m, x, zs), t in zip(reqs, tickets):
             y, A, tm = srv.wait(t, timeout=600)
             lat.append((tm[2] - tm[0]) * 1e3)
             rays += len(x)
-            tdone = max(tdone, tm[2])
         wall = time.perf_counter() - t0
         sweep.append({"rate_req_per_s": lam, "requests": nreq, "rays": rays, "rays_per_s": rays / wall,
                       "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99))})
     st = srv.stats()
-    # error of served (split) results against the plain FP64 path on a few requests
     errs = []
-    for _ in range(4):
+    for _ in range(3):
         m, x, zs = request()
         y, A, _ = srv.wait(srv.submit(m, x, zs), timeout=600)
         y64, A64 = models[m].rayshooterInternal(x, np.full(len(x), zs), precision=glb.PREC_FP64)
         errs.append(error_stats(x, y, A, y64, A64)["alpha"])
     srv.close()
+    return sweep, st, {"median": float(np.median([e["median"] for e in errs])),
+                       "max_p999": float(max(e["p999"] for e in errs))}
+
+
+def run_served(args):
+    """32 resident light-cone models; Poisson request stream at swept rates;
+    request sizes log-uniform in 1e3-5e5 rays in 1-8 Gaussian blobs
+    (sigma 0.05-1 arcsec); z_s uniform in 1-3; split precision."""
+    import multiprocessing as mp
+    nm = 32 if not args.small else 4
+    with mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
+        specs = pool.map(_c5_model, [5000 + i for i in range(nm)])
+    models = [make_lens(s) for s in specs]
+    sweep, st, err = served_sweep(models, (5.0, 20.0, 60.0), 120 if not args.small else 30)
     top = max(sweep, key=lambda s: s["rays_per_s"])
     line = _base_line(args, "rays/s/GPU served; p50/p99 request ms", "rays/s", top["rays_per_s"],
                       None, "f32+f64", f"{nm} resident light-cone models, Poisson request stream",
-                      sweep=sweep, server=st,
-                      errors_vs_fp64_alpha={"median": float(np.median([e["median"] for e in errs])),
-                                            "max_p999": float(max(e["p999"] for e in errs))})
+                      sweep=sweep, server=st, errors_vs_fp64_alpha=err)
     print(json.dumps(line))
 
 
@@ -593,6 +602,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--small", action="store_true", help="a reduced workload for quick checks")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-served", action="store_true", help="skip the served-stream leg of the default line")
     ap.add_argument("--n1d", type=int, default=0,
                     help="rays per side of the light-cone grid (default 2048; a profiling size, not a bench line)")
     ap.add_argument("--workload", default="lightcone",
@@ -679,6 +689,19 @@ def main():
     y32, A32 = y.cpu().numpy(), A.cpu().numpy()
     errs = error_stats(x_host, y32, A32, y64, A64)
     attrib = attribution(spec, lens, x_host) if rank == 0 and not args.small else None
+    served = None
+    if rank == 0 and not args.no_served:
+        # the served form on a few resident models: this light cone and three
+        # more of the same kind (seeds 5000-5002), two Poisson rates
+        import multiprocessing as mp
+        with mp.get_context("spawn").Pool(3) as pool:
+            extra = pool.map(_c5_model, [5000, 5001, 5002] if not args.small else [5000])
+        models = [lens] + [make_lens(sp) for sp in extra]
+        sw, sst, serr = served_sweep(models, (20.0, 60.0), 60 if not args.small else 20)
+        served = {"models": len(models), "sweep": sw, "server": sst, "errors_vs_fp64_alpha": serr,
+                  "request_rays": "log-uniform 1e3-5e5 in 1-8 Gaussian blobs (0.05-1 arcsec), z_s uniform 1-3",
+                  "latency": "submit to results on the host (ms)"}
+        del models, extra
 
     # end to end through the host C ABI (pinned host buffers, copies timed)
     xp = torch.from_numpy(x_host).pin_memory()
@@ -725,6 +748,7 @@ def main():
             "plain_fp64": {"value": n / (fp64_ms / 1e3), "unit": "rays/s", "ms": fp64_ms},
             "errors_vs_fp64": errs,
             "kappa_gamma_attribution": attrib,
+            "served": served,
             "e2e": {"value": world * n * args.steps / e2e_s, "unit": "rays/s", "h2d_bytes_per_step": 16 * n,
                     "d2h_bytes_per_step": 48 * n},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",

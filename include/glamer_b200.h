@@ -45,6 +45,15 @@ enum {
   GLB_ERR_TIMEOUT = -8       /* glb_server_wait ran out of time */
 };
 
+/* Per-ray status of glb_lens_rayshoot_status / glb_lens_rayshoot_device_status. */
+enum {
+  GLB_RAY_OK = 0,        /* y and A written, all finite */
+  GLB_RAY_SKIPPED = 1,   /* skip flag set (the reference's in_image == MAYBE points,
+                            include/lens.h:959): y and A left as they were */
+  GLB_RAY_NONFINITE = 2  /* y or A written but not finite (the reference asserts,
+                            include/lens.h:1012-1037) */
+};
+
 /* Precision of the tree walk. */
 enum {
   GLB_PREC_FP64 = 0,  /* plain FP64 walk, the reference's arithmetic */
@@ -175,9 +184,31 @@ int glb_lens_reset_source(glb_lens *l, double z, int nearest, int *plane_index);
 int glb_lens_rayshoot(glb_lens *l, size_t n, const double *x, const double *zs, double *y,
                       double *A, int precision);
 /* The same on device buffers, enqueued on `stream` (a cudaStream_t, NULL for
- * the lens's own stream); returns once enqueued. */
+ * the calling thread's stream on this lens); returns once enqueued.
+ * Threads: any number of host threads may shoot rays through one lens at the
+ * same time (the reference reads the lens read-only during
+ * rayshooterInternal); each calling thread gets its own stream and work
+ * buffers on the lens, created on its first call and freed with the lens.
+ * Successive device-buffer calls of one thread are ordered on the GPU even
+ * when they name different streams (they share that thread's buffers).
+ * Adding halos or resetting the source plane while another thread shoots rays
+ * through the same lens is not supported (as in the reference). */
 int glb_lens_rayshoot_device(glb_lens *l, size_t n, const double *x_dev, const double *zs_dev,
                              double *y_dev, double *A_dev, int precision, void *stream);
+/* glb_lens_rayshoot with per-ray flags (Lens::rayshooterInternal(Npoints,
+ * Point*), FullRange/internal_rayshooter_multi.cpp:53-118, whose points with
+ * in_image == MAYBE are skipped, include/lens.h:959): skip (n bytes, NULL for
+ * none) != 0 leaves that ray's y and A untouched; status (n bytes, out) gets
+ * GLB_RAY_OK / GLB_RAY_SKIPPED / GLB_RAY_NONFINITE per ray.  The tree walk is
+ * stackless (preorder node array with skip links), so there is no stack
+ * overflow state. */
+int glb_lens_rayshoot_status(glb_lens *l, size_t n, const double *x, const double *zs,
+                             const unsigned char *skip, double *y, double *A, unsigned char *status,
+                             int precision);
+/* The same on device buffers (skip_dev may be NULL), enqueued on `stream`. */
+int glb_lens_rayshoot_device_status(glb_lens *l, size_t n, const double *x_dev, const double *zs_dev,
+                                    const unsigned char *skip_dev, double *y_dev, double *A_dev,
+                                    unsigned char *status_dev, int precision, void *stream);
 
 /* GridMap(LensHndl, N1d, center, range) (TreeCode_link/gridmap.cpp:93-120):
  * the N1d x N1d grid (x fastest, spacing range/(N1d-1)) is generated on the
@@ -242,10 +273,14 @@ int glb_gridmap_adaptive_surface_brightness(glb_lens *l, size_t n1d, const doubl
  * per call, at most 64 lens planes and 256 halos (larger calls return
  * GLB_ERR_ARG).  The first call on a device does a one-time set-up (looks up
  * the array's device address and copies the NFW tables) and should come
- * before any stream capture.  All calls share the one array, so calls that
- * overlap on the GPU (different streams or threads) race; serialise them.
+ * before any stream capture.  All calls share the one array, which keeps the
+ * last call's contents; so that no two calls use it at once, every call on a
+ * device waits on the GPU for the previous call on that device (one event per
+ * device, recorded after each call's last launch; the enqueue is serialised on
+ * the host), whatever stream or lens it names.  Calls on one device therefore
+ * run one after another on the GPU in the order the host made them.
  * Buffers are device pointers; the call returns once the work is enqueued on
- * `stream` (NULL: the lens's own stream). */
+ * `stream` (NULL: the lens's own stream, one per lens). */
 int glb_lens_rayshoot_noalloc(glb_lens *l, size_t n, const double *x_dev, const double *zs_dev,
                               double *y_dev, double *A_dev, int precision, void *stream);
 
@@ -289,10 +324,16 @@ int glb_batch_destroy(glb_batch *b);
  * time under a global mutex).  A resident request loop over `nmodels` lenses
  * kept on the device: requests (model, rays, source redshift) are queued by
  * glb_server_submit and admitted in arrival order into batches of at most
- * max_rays_per_batch rays (bounded by free device memory); a batch launches
- * as soon as one of `nslots` slots is free, so requests that arrive while
- * others run are batched and overlap on the GPU.  A request's results do not
- * depend on what it is batched with.  The lenses must outlive the server. */
+ * max_rays_per_batch rays; a batch launches as soon as one of `nslots` slots
+ * is free, so requests that arrive while others run are batched and overlap
+ * on the GPU.  Admission is by device memory: at every dispatch the server
+ * reads the HBM free at that moment (plus memory its stream-ordered pool
+ * holds unused), keeps 5 % of the device free, and admits the requests whose
+ * batch memory (about 170 bytes per ray) fits; a batch takes its memory when
+ * it launches and gives it back when its results are copied out, so a request
+ * that does not fit waits until batches in flight finish (GLB_ERR_OOM from
+ * glb_server_wait if none is in flight).  A request's results do not depend
+ * on what it is batched with.  The lenses must outlive the server. */
 typedef struct glb_server glb_server;
 int glb_server_create(glb_lens *const *models, int nmodels, size_t max_rays_per_batch, int precision, int nslots,
                       glb_server **out);
@@ -308,6 +349,9 @@ int glb_server_poll(glb_server *s, long long ticket, int *done);
 /* stats[0..5]: rays done, requests done, batches, busy seconds (first launch
  * to last completion), rays per batch budget, requests pending. */
 int glb_server_stats(glb_server *s, double *stats);
+/* Admission record: dispatches that waited for batches in flight to give
+ * device memory back, and the least admissible HBM (GB) seen at a dispatch. */
+int glb_server_admission(glb_server *s, double *memory_waits, double *min_free_gb);
 /* Stops the loop; batches already on the GPU finish, queued requests are
  * dropped. */
 int glb_server_destroy(glb_server *s);

@@ -39,6 +39,11 @@ PREC_FP64 = 0
 PREC_SPLIT = 1
 PREC_FP32 = 2
 
+# per-ray status bytes of Lens.rayshooterInternal_status
+RAY_OK = 0
+RAY_SKIPPED = 1
+RAY_NONFINITE = 2
+
 GLB_ERR_ARG = -1
 GLB_ERR_CUDA = -2
 GLB_ERR_OOM = -3
@@ -57,13 +62,14 @@ EXPORTED = [
     "glb_halo_params", "glb_halo_destroy", "glb_halo_field_plane",
     "glb_lens_create", "glb_lens_destroy", "glb_lens_insert_halo", "glb_lens_insert_field_plane",
     "glb_lens_nplanes", "glb_lens_planes",
-    "glb_lens_reset_source", "glb_lens_rayshoot", "glb_lens_rayshoot_device", "glb_gridmap", "glb_gridmap_pixelmap",
+    "glb_lens_reset_source", "glb_lens_rayshoot", "glb_lens_rayshoot_device", "glb_lens_rayshoot_status",
+    "glb_lens_rayshoot_device_status", "glb_gridmap", "glb_gridmap_pixelmap",
     "glb_gridmap_surface_brightness", "glb_gridmap_adaptive_surface_brightness",
     "glb_lens_last_timing", "glb_lens_count_interactions", "glb_lens_rayshoot_noalloc",
     "glb_batch_create_grids", "glb_batch_run", "glb_batch_autotune", "glb_batch_set_block", "glb_batch_info",
     "glb_batch_result", "glb_batch_destroy",
     "glb_server_create", "glb_server_submit", "glb_server_wait", "glb_server_poll", "glb_server_stats",
-    "glb_server_destroy",
+    "glb_server_destroy", "glb_server_admission",
     "glb_particles_smoothing", "glb_particles_smoothing_device",
 ]
 
@@ -116,6 +122,8 @@ def load_library():
     L.glb_lens_reset_source.argtypes = [_vp, C.c_double, C.c_int, C.POINTER(C.c_int)]
     L.glb_lens_rayshoot.argtypes = [_vp, C.c_size_t, _vp, _vp, _vp, _vp, C.c_int]
     L.glb_lens_rayshoot_device.argtypes = [_vp, C.c_size_t, _vp, _vp, _vp, _vp, C.c_int, _vp]
+    L.glb_lens_rayshoot_status.argtypes = [_vp, C.c_size_t, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int]
+    L.glb_lens_rayshoot_device_status.argtypes = [_vp, C.c_size_t, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int, _vp]
     L.glb_gridmap.argtypes = [_vp, C.c_size_t, _vp, C.c_double, _vp, _vp, C.c_int]
     L.glb_gridmap_pixelmap.argtypes = [_vp, C.c_size_t, _vp, C.c_double, C.c_int, _vp, C.c_int]
     L.glb_gridmap_surface_brightness.argtypes = [_vp, C.c_size_t, _vp, C.c_double, C.c_int, _vp, _vp,
@@ -138,6 +146,7 @@ def load_library():
     L.glb_server_wait.argtypes = [_vp, C.c_longlong, C.c_double, _vp]
     L.glb_server_poll.argtypes = [_vp, C.c_longlong, C.POINTER(C.c_int)]
     L.glb_server_stats.argtypes = [_vp, _vp]
+    L.glb_server_admission.argtypes = [_vp, _vp, _vp]
     L.glb_server_destroy.argtypes = [_vp]
     L.glb_particles_smoothing.argtypes = [_vp, C.c_size_t, C.c_int]
     L.glb_particles_smoothing_device.argtypes = [_vp, C.c_size_t, C.c_int, _vp, _vp, _vp]
@@ -417,6 +426,24 @@ class Lens:
         _check(load_library().glb_lens_rayshoot(self._h, n, _p(x), _p(zs), _p(y), _p(A), precision))
         return y, A
 
+    def rayshooterInternal_status(self, x, source_zs=None, skip=None, y=None, A=None, precision=PREC_FP64):
+        """rayshooterInternal with per-ray flags: skip (n,) bool -- those rays'
+        y and A keep the values passed in (the reference's in_image == MAYBE
+        points); returns y, A and a status byte per ray (RAY_OK, RAY_SKIPPED,
+        RAY_NONFINITE)."""
+        x = _f64(x, (-1, 2))
+        n = len(x)
+        zs = None if source_zs is None else _f64(source_zs)
+        if zs is not None and len(zs) != n:
+            raise ValueError("missing redshifts")
+        sk = None if skip is None else np.ascontiguousarray(skip, dtype=np.uint8)
+        y = np.zeros((n, 2)) if y is None else np.array(y, dtype=np.float64, copy=True).reshape(n, 2)
+        A = np.zeros((n, 4)) if A is None else np.array(A, dtype=np.float64, copy=True).reshape(n, 4)
+        st = np.zeros(n, dtype=np.uint8)
+        _check(load_library().glb_lens_rayshoot_status(self._h, n, _p(x), _p(zs), _p(sk), _p(y), _p(A), _p(st),
+                                                       precision))
+        return y, A, st
+
     def rayshoot_device(self, n, x_ptr, zs_ptr, y_ptr, A_ptr, precision=PREC_FP64, stream=None):
         """Device-buffer form (raw CUDA pointers)."""
         _check(load_library().glb_lens_rayshoot_device(self._h, n, x_ptr, zs_ptr, y_ptr, A_ptr, precision,
@@ -625,7 +652,10 @@ class Server:
     def stats(self):
         s = np.zeros(6)
         _check(load_library().glb_server_stats(self._h, _p(s)))
-        return dict(rays=s[0], requests=s[1], batches=s[2], busy_s=s[3], ray_budget=s[4], pending=s[5])
+        w, f = C.c_double(0), C.c_double(0)
+        _check(load_library().glb_server_admission(self._h, C.byref(w), C.byref(f)))
+        return dict(rays=s[0], requests=s[1], batches=s[2], busy_s=s[3], ray_budget=s[4], pending=s[5],
+                    memory_waits=w.value, min_free_gb=f.value)
 
     def close(self):
         if getattr(self, "_h", None) and _lib is not None:

@@ -469,17 +469,24 @@ double now_s() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
+// Device memory of one batch, in bytes per ray: x, sorted x, y, A (10
+// doubles), two 64-bit sort keys, three 32-bit index arrays, the radix sort's
+// temporary storage (bounded by kSortBytesPerRay per ray plus a constant) and
+// the 32-ray chunks.
+constexpr size_t kSortBytesPerRay = 32;
+constexpr size_t kBatchBytesPerRay = 10 * 8 + 2 * 8 + 3 * 4 + kSortBytesPerRay + 8;
+constexpr size_t kBatchBytesFixed = (size_t)4 << 20;
+
 struct Slot {
   cudaStream_t s = nullptr;
   cudaEvent_t ev = nullptr;
-  double *hx = nullptr, *hy = nullptr, *hA = nullptr;  // pinned staging
+  double *hx = nullptr, *hy = nullptr, *hA = nullptr;  // pinned staging (max_rays_per_batch)
   unsigned *hreq = nullptr;
-  DBuf<double> x, xs, y, A, bbox;
-  DBuf<unsigned long long> keys, keys2;
-  DBuf<unsigned> idx, perm, req_of;
-  DBuf<Chunk> chunks;
-  DBuf<char> tmp;
-  DBuf<int> counter;
+  // device memory of the batch in flight: taken from the device's stream-
+  // ordered pool on the slot's stream when the batch launches and given back
+  // on the same stream after its results are copied out
+  char *dmem = nullptr;
+  size_t dbytes = 0;
   std::vector<std::shared_ptr<Req>> reqs;
   std::vector<size_t> offs;
   size_t n = 0;
@@ -490,7 +497,10 @@ struct Slot {
 struct glb_server {
   int device = 0;
   int precision = GLB_PREC_FP64;
-  size_t cap = 0;  // rays per batch (the admission budget of one slot)
+  size_t cap = 0;  // rays per batch at most (max_rays_per_batch; the pinned staging of a slot)
+  size_t reserve = 0;  // device bytes admission leaves free for everything else
+  size_t total_bytes = 0;
+  cudaMemPool_t pool = nullptr;  // the device's default stream-ordered pool
   std::vector<glb_lens *> models;
   DBuf<LensDev> d_lenses;
   NFWTables tab{};
@@ -509,10 +519,28 @@ struct glb_server {
   std::thread dispatcher, completer;
   // statistics
   unsigned long long batches = 0, rays_done = 0, reqs_done = 0;
+  unsigned long long memory_waits = 0;  // dispatches held back until batches in flight gave memory back
   double busy_t0 = 0, busy_t1 = 0;
+  double min_free_gb = -1;  // least free HBM seen at admission
 };
 
 namespace {
+
+size_t batch_bytes(size_t n) { return kBatchBytesFixed + n * kBatchBytesPerRay; }
+
+// Device memory available to a new batch now: free HBM plus memory the
+// stream-ordered pool holds but no allocation uses, less the reserve.
+size_t admissible_bytes(glb_server *S) {
+  size_t freeb = 0, totb = 0;
+  if (cudaMemGetInfo(&freeb, &totb) != cudaSuccess) return 0;
+  size_t reserved = 0, used = 0;
+  cudaMemPoolGetAttribute(S->pool, cudaMemPoolAttrReservedMemCurrent, &reserved);
+  cudaMemPoolGetAttribute(S->pool, cudaMemPoolAttrUsedMemCurrent, &used);
+  const size_t avail = freeb + (reserved > used ? reserved - used : 0);
+  const double gb = avail / 1e9;
+  if (S->min_free_gb < 0 || gb < S->min_free_gb) S->min_free_gb = gb;
+  return avail > S->reserve ? avail - S->reserve : 0;
+}
 
 int launch_slot(glb_server *S, Slot &sl) {
   cudaStream_t s = sl.s;
@@ -528,16 +556,7 @@ int launch_slot(glb_server *S, Slot &sl) {
     n += q.n;
   }
   sl.n = n;
-  CKR(cudaMemcpyAsync(sl.x.p, sl.hx, 2 * n * sizeof(double), cudaMemcpyHostToDevice, s));
-  CKR(cudaMemcpyAsync(sl.req_of.p, sl.hreq, n * sizeof(unsigned), cudaMemcpyHostToDevice, s));
-  CKR(cudaMemcpyAsync(sl.bbox.p, bb.data(), bb.size() * sizeof(double), cudaMemcpyHostToDevice, s));
-  k_req_keys<<<nblk(n, 256), 256, 0, s>>>(sl.x.p, n, sl.req_of.p, sl.bbox.p, sl.keys.p, sl.idx.p);
-  int bits = 32;
-  while ((1ull << (bits - 32)) < nr + 1 && bits < 64) ++bits;
-  size_t tb = sl.tmp.n;
-  CKR(cub::DeviceRadixSort::SortPairs(sl.tmp.p, tb, sl.keys.p, sl.keys2.p, sl.idx.p, sl.perm.p, (int)n, 0, bits, s));
-  k_gather_sorted<<<nblk(n, 256), 256, 0, s>>>(sl.x.p, sl.perm.p, n, sl.xs.p);
-  // chunks: requests stay contiguous in sorted order; 32 rays per chunk
+  // the batch's device memory, carved from one stream-ordered allocation
   std::vector<Chunk> C;
   for (size_t r = 0; r < nr; ++r) {
     Req &q = *sl.reqs[r];
@@ -552,17 +571,44 @@ int launch_slot(glb_server *S, Slot &sl) {
       C.push_back(k);
     }
   }
-  CKR(cudaMemcpyAsync(sl.chunks.p, C.data(), C.size() * sizeof(Chunk), cudaMemcpyHostToDevice, s));
-  CKR(cudaMemsetAsync(sl.counter.p, 0, sizeof(int), s));
+  int bits = 32;
+  while ((1ull << (bits - 32)) < nr + 1 && bits < 64) ++bits;
+  size_t tb = 0;
+  CKR(cub::DeviceRadixSort::SortPairs(nullptr, tb, (unsigned long long *)nullptr, (unsigned long long *)nullptr,
+                                      (unsigned *)nullptr, (unsigned *)nullptr, (int)n, 0, bits, s));
+  auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+  const size_t o_x = 0, o_xs = o_x + al(16 * n), o_y = o_xs + al(16 * n), o_A = o_y + al(16 * n);
+  const size_t o_bb = o_A + al(32 * n), o_k = o_bb + al(32 * nr), o_k2 = o_k + al(8 * n);
+  const size_t o_idx = o_k2 + al(8 * n), o_perm = o_idx + al(4 * n), o_req = o_perm + al(4 * n);
+  const size_t o_ch = o_req + al(4 * n), o_cnt = o_ch + al(C.size() * sizeof(Chunk)), o_tmp = o_cnt + 256;
+  sl.dbytes = o_tmp + al(tb);
+  CKR(cudaMallocFromPoolAsync((void **)&sl.dmem, sl.dbytes, S->pool, s));
+  char *m = sl.dmem;
+  double *dx = (double *)(m + o_x), *dxs = (double *)(m + o_xs), *dy = (double *)(m + o_y), *dA = (double *)(m + o_A);
+  double *dbb = (double *)(m + o_bb);
+  unsigned long long *keys = (unsigned long long *)(m + o_k), *keys2 = (unsigned long long *)(m + o_k2);
+  unsigned *idx = (unsigned *)(m + o_idx), *perm = (unsigned *)(m + o_perm), *req_of = (unsigned *)(m + o_req);
+  Chunk *dch = (Chunk *)(m + o_ch);
+  int *counter = (int *)(m + o_cnt);
+  CKR(cudaMemcpyAsync(dx, sl.hx, 2 * n * sizeof(double), cudaMemcpyHostToDevice, s));
+  CKR(cudaMemcpyAsync(req_of, sl.hreq, n * sizeof(unsigned), cudaMemcpyHostToDevice, s));
+  CKR(cudaMemcpyAsync(dbb, bb.data(), bb.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+  k_req_keys<<<nblk(n, 256), 256, 0, s>>>(dx, n, req_of, dbb, keys, idx);
+  CKR(cub::DeviceRadixSort::SortPairs(m + o_tmp, tb, keys, keys2, idx, perm, (int)n, 0, bits, s));
+  k_gather_sorted<<<nblk(n, 256), 256, 0, s>>>(dx, perm, n, dxs);
+  // chunks: requests stay contiguous in sorted order; 32 rays per chunk
+  CKR(cudaMemcpyAsync(dch, C.data(), C.size() * sizeof(Chunk), cudaMemcpyHostToDevice, s));
+  CKR(cudaMemsetAsync(counter, 0, sizeof(int), s));
   if (S->precision == GLB_PREC_SPLIT)
-    k_batch<GLB_PREC_SPLIT><<<S->grid, 128, 0, s>>>(sl.chunks.p, (int)C.size(), S->d_lenses.p, S->tab, sl.xs.p,
-                                                    sl.perm.p, sl.y.p, sl.A.p, sl.counter.p);
+    k_batch<GLB_PREC_SPLIT><<<S->grid, 128, 0, s>>>(dch, (int)C.size(), S->d_lenses.p, S->tab, dxs, perm, dy, dA,
+                                                    counter);
   else
-    k_batch<GLB_PREC_FP64><<<S->grid, 128, 0, s>>>(sl.chunks.p, (int)C.size(), S->d_lenses.p, S->tab, sl.xs.p,
-                                                   sl.perm.p, sl.y.p, sl.A.p, sl.counter.p);
+    k_batch<GLB_PREC_FP64><<<S->grid, 128, 0, s>>>(dch, (int)C.size(), S->d_lenses.p, S->tab, dxs, perm, dy, dA,
+                                                   counter);
   CKR(cudaGetLastError());
-  CKR(cudaMemcpyAsync(sl.hy, sl.y.p, 2 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
-  CKR(cudaMemcpyAsync(sl.hA, sl.A.p, 4 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CKR(cudaMemcpyAsync(sl.hy, dy, 2 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CKR(cudaMemcpyAsync(sl.hA, dA, 4 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CKR(cudaFreeAsync(sl.dmem, s));
   CKR(cudaEventRecord(sl.ev, s));
   return 0;
 }
@@ -577,16 +623,40 @@ void dispatcher_main(glb_server *S) {
     std::vector<std::shared_ptr<Req>> take;
     {
       std::unique_lock<std::mutex> lk(S->mu);
-      S->cv_submit.wait(lk, [&] { return S->stop || (!S->pending.empty() && !S->free_slots.empty()); });
-      if (S->stop) return;
+      for (;;) {
+        S->cv_submit.wait(lk, [&] { return S->stop || (!S->pending.empty() && !S->free_slots.empty()); });
+        if (S->stop) return;
+        // admission by the device memory free now (re-read at every dispatch)
+        const size_t avail = admissible_bytes(S);
+        size_t budget = avail > kBatchBytesFixed ? (avail - kBatchBytesFixed) / kBatchBytesPerRay : 0;
+        budget = std::min(budget, S->cap);
+        if (S->pending.front()->n <= budget) {
+          size_t used = 0;
+          while (!S->pending.empty() && used + S->pending.front()->n <= budget &&
+                 (int)take.size() < kMaxReqPerBatch) {
+            used += S->pending.front()->n;
+            take.push_back(S->pending.front());
+            S->pending.pop_front();
+          }
+          break;
+        }
+        if (S->inflight.empty()) {
+          // nothing will give memory back: the request cannot run now
+          auto q = S->pending.front();
+          S->pending.pop_front();
+          q->status = GLB_ERR_OOM;
+          q->t_start = q->t_done = now_s();
+          q->done.store(1);
+          S->cv_done.notify_all();
+          continue;
+        }
+        // wait for a batch in flight to finish and give its memory back
+        ++S->memory_waits;
+        const unsigned long long b0 = S->batches;
+        S->cv_submit.wait(lk, [&] { return S->stop || S->batches != b0; });
+      }
       si = S->free_slots.front();
       S->free_slots.pop_front();
-      size_t budget = S->cap, used = 0;
-      while (!S->pending.empty() && used + S->pending.front()->n <= budget && (int)take.size() < kMaxReqPerBatch) {
-        used += S->pending.front()->n;
-        take.push_back(S->pending.front());
-        S->pending.pop_front();
-      }
     }
     Slot &sl = *S->slots[si];
     sl.reqs = take;
@@ -664,14 +734,14 @@ int glb_server_create(glb_lens *const *models, int nmodels, size_t max_rays_per_
   auto S = std::make_unique<glb_server>();
   CKR(cudaGetDevice(&S->device));
   S->precision = precision;
-  // admission budget: the requested rays per batch, bounded by free HBM
-  // (about 200 bytes of device memory per ray and slot)
+  // rays per batch at most (the pinned host staging of each slot); the device
+  // memory of a batch is taken when it launches, against the HBM free then
+  S->cap = std::min<size_t>(max_rays_per_batch ? max_rays_per_batch : (size_t)4 << 20, (size_t)1 << 30);
   size_t freeb = 0, totb = 0;
   CKR(cudaMemGetInfo(&freeb, &totb));
-  size_t by_mem = freeb / 2 / (size_t)nslots / 200;
-  S->cap = std::min<size_t>(max_rays_per_batch ? max_rays_per_batch : (size_t)4 << 20, by_mem);
-  S->cap = std::min<size_t>(S->cap, (size_t)1 << 30);
-  if (S->cap < 32) return fail(GLB_ERR_OOM, "not enough free device memory for the server");
+  S->reserve = totb / 20;  // 5 % of HBM stays free for other work
+  S->total_bytes = totb;
+  CKR(cudaDeviceGetDefaultMemPool(&S->pool, S->device));
   std::vector<LensDev> L(nmodels);
   for (int i = 0; i < nmodels; ++i) {
     if (!models[i] || models[i]->device != S->device) return fail(GLB_ERR_ARG, "models must be lenses on one device");
@@ -682,7 +752,7 @@ int glb_server_create(glb_lens *const *models, int nmodels, size_t max_rays_per_
   CKR(cudaMemcpy(S->d_lenses.p, L.data(), nmodels * sizeof(LensDev), cudaMemcpyHostToDevice));
   if (int rc = device_nfw_tables(S->tab)) return rc;
   if (int rc = persistent_grid(128, precision, &S->grid)) return rc;
-  size_t cap = S->cap, maxchunks = cap / 32 + kMaxReqPerBatch + 1;
+  size_t cap = S->cap;
   for (int i = 0; i < nslots; ++i) {
     auto sl = std::make_unique<Slot>();
     CKR(cudaStreamCreateWithFlags(&sl->s, cudaStreamNonBlocking));
@@ -691,22 +761,6 @@ int glb_server_create(glb_lens *const *models, int nmodels, size_t max_rays_per_
     CKR(cudaMallocHost((void **)&sl->hy, 2 * cap * sizeof(double)));
     CKR(cudaMallocHost((void **)&sl->hA, 4 * cap * sizeof(double)));
     CKR(cudaMallocHost((void **)&sl->hreq, cap * sizeof(unsigned)));
-    CKR(sl->x.alloc(2 * cap));
-    CKR(sl->xs.alloc(2 * cap));
-    CKR(sl->y.alloc(2 * cap));
-    CKR(sl->A.alloc(4 * cap));
-    CKR(sl->bbox.alloc(4 * (size_t)kMaxReqPerBatch));
-    CKR(sl->keys.alloc(cap));
-    CKR(sl->keys2.alloc(cap));
-    CKR(sl->idx.alloc(cap));
-    CKR(sl->perm.alloc(cap));
-    CKR(sl->req_of.alloc(cap));
-    CKR(sl->chunks.alloc(maxchunks));
-    CKR(sl->counter.alloc(1));
-    size_t tb = 0;
-    CKR(cub::DeviceRadixSort::SortPairs(nullptr, tb, sl->keys.p, sl->keys2.p, sl->idx.p, sl->perm.p, (int)cap, 0, 64,
-                                        sl->s));
-    CKR(sl->tmp.alloc(tb));
     S->slots.push_back(std::move(sl));
     S->free_slots.push_back(i);
   }
@@ -722,6 +776,8 @@ int glb_server_submit(glb_server *S, int model, size_t n, const double *x, doubl
   if (!S || !ticket || (n > 0 && (!x || !y || !A))) return fail(GLB_ERR_ARG, "null argument");
   if (model < 0 || model >= (int)S->models.size()) return fail(GLB_ERR_ARG, "unknown model");
   if (n > S->cap) return fail(GLB_ERR_ARG, "request larger than the server's ray budget per batch");
+  if (n > 0 && batch_bytes(n) + S->reserve > S->total_bytes)
+    return fail(GLB_ERR_OOM, "request larger than the device memory could ever hold");
   auto q = std::make_shared<Req>();
   q->model = model;
   q->n = n;
@@ -797,6 +853,14 @@ int glb_server_stats(glb_server *S, double *stats) {
   stats[3] = S->busy_t1 - S->busy_t0;
   stats[4] = (double)S->cap;
   stats[5] = (double)S->pending.size();
+  return 0;
+}
+
+int glb_server_admission(glb_server *S, double *memory_waits, double *min_free_gb) {
+  if (!S) return fail(GLB_ERR_ARG, "null server");
+  std::lock_guard<std::mutex> lk(S->mu);
+  if (memory_waits) *memory_waits = (double)S->memory_waits;
+  if (min_free_gb) *min_free_gb = S->min_free_gb;
   return 0;
 }
 

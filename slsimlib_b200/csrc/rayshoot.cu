@@ -14,7 +14,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -159,6 +161,36 @@ struct PlaneHost {
   std::vector<glb_halo *> halos;
 };
 
+// The per-call workspace of one calling thread on one lens: its stream,
+// timing events and device buffers.  Threads that shoot rays through the same
+// lens each get their own, so their calls run concurrently on the GPU while
+// the lens's device descriptors (planes, halos, trees) are only read.
+struct LensWS {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t done = nullptr;  // end of this workspace's last pass (orders reuse across streams)
+  DBuf<double> st;          // 12 n recursion state
+  DBuf<double> io;          // host-call staging: x 2n, zs n, y 2n, A 4n
+  DBuf<int> jmax_ray;
+  DBuf<double> src_ray;     // Dls/Ds, D/Ds per ray
+  DBuf<unsigned> keys, keys2, perm0, perm;
+  DBuf<char> sort_tmp;
+  DBuf<unsigned long long> bbox;
+  DBuf<unsigned char> status;  // per-ray status staging
+  size_t ws_n = 0;
+  float last_kernel_ms = 0, last_total_ms = 0;
+  bool timed = false;
+  ~LensWS() {
+    cudaSetDevice(device);
+    if (stream) cudaStreamSynchronize(stream);
+    for (cudaEvent_t e : ev)
+      if (e) cudaEventDestroy(e);
+    if (done) cudaEventDestroy(done);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
 struct glb_lens {
   Cosmo cosmo{0.3, 0.7, 0.7};
   double zsource = 0;
@@ -172,23 +204,16 @@ struct glb_lens {
   bool toggle_source_plane = false;
   double zs_implant = 0;
   int device = 0;
-  cudaStream_t stream = nullptr;
-  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-  // device copies of the plane / halo descriptors
+  cudaStream_t stream = nullptr;  // uploads of the descriptors
+  // device copies of the plane / halo descriptors (uploaded once under mu,
+  // then only read)
   bool dirty = true;
   DBuf<PlaneDev> d_planes;
   DBuf<HaloDev> d_halos;
   DBuf<double> d_planez, d_Dl;
-  // rayshoot workspace
-  DBuf<double> st;          // 12 n recursion state
-  DBuf<double> io;          // host-call staging: x 2n, zs n, y 2n, A 4n
-  DBuf<int> jmax_ray;
-  DBuf<double> src_ray;     // Dls/Ds, D/Ds per ray
-  DBuf<unsigned> keys, keys2, perm0, perm;
-  DBuf<char> sort_tmp;
-  DBuf<unsigned long long> bbox;
-  size_t ws_n = 0;
-  float last_kernel_ms = 0, last_total_ms = 0;
+  // per-thread workspaces (created on a thread's first call, freed with the lens)
+  std::mutex mu;
+  std::map<std::thread::id, std::unique_ptr<LensWS>> ws;
 };
 
 // ================================================================== kernels
@@ -206,6 +231,9 @@ __device__ inline double ord2d(unsigned long long u) {
 __global__ void k_ray_bbox(const double *x, size_t n, unsigned long long *bb) {
   unsigned long long mnx = ~0ull, mny = ~0ull, mxx = 0, mxy = 0;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    // a non-finite ray would stretch the box over everything (its own key is
+    // clamped to the box in k_ray_morton)
+    if (!isfinite(x[2 * i]) || !isfinite(x[2 * i + 1])) continue;
     unsigned long long ux = d2ord(x[2 * i]), uy = d2ord(x[2 * i + 1]);
     mnx = min(mnx, ux);
     mny = min(mny, uy);
@@ -308,27 +336,52 @@ __global__ void k_init_state(const double *x, const double *zs, const unsigned *
   }
 }
 
-__global__ void k_finish(const double *st, const unsigned *perm, size_t n, double *y, double *A) {
+// Per-ray status (include/glamer_b200.h): a skipped ray (the caller's flag,
+// the reference's in_image == MAYBE points, lens.h:959) keeps its y and A
+// untouched; a ray whose y or A is not finite is flagged where the reference
+// asserts (lens.h:1012-1037).
+__device__ __forceinline__ unsigned char ray_status(const double *y, const double *A) {
+  bool f = isfinite(y[0]) && isfinite(y[1]);
+  for (int c = 0; c < 4; ++c) f = f && isfinite(A[c]);
+  return f ? GLB_RAY_OK : GLB_RAY_NONFINITE;
+}
+
+__global__ void k_finish(const double *st, const unsigned *perm, size_t n, double *y, double *A,
+                         unsigned char *status = nullptr, const unsigned char *skip = nullptr) {
   size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (k >= n) return;
   unsigned i = perm[k];
-  y[2 * i] = st[0 * n + k];
-  y[2 * i + 1] = st[1 * n + k];
-  A[4 * i] = st[4 * n + k];
-  A[4 * i + 1] = st[5 * n + k];
-  A[4 * i + 2] = st[6 * n + k];
-  A[4 * i + 3] = st[7 * n + k];
+  if (skip && skip[i]) {
+    if (status) status[i] = GLB_RAY_SKIPPED;
+    return;
+  }
+  const double yy[2] = {st[0 * n + k], st[1 * n + k]};
+  const double AA[4] = {st[4 * n + k], st[5 * n + k], st[6 * n + k], st[7 * n + k]};
+  y[2 * i] = yy[0];
+  y[2 * i + 1] = yy[1];
+  A[4 * i] = AA[0];
+  A[4 * i + 1] = AA[1];
+  A[4 * i + 2] = AA[2];
+  A[4 * i + 3] = AA[3];
+  if (status) status[i] = ray_status(yy, AA);
 }
 
-__global__ void k_identity_rays(const double *x, size_t n, double *y, double *A) {
+__global__ void k_identity_rays(const double *x, size_t n, double *y, double *A, unsigned char *status = nullptr,
+                                const unsigned char *skip = nullptr) {
   size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
+  if (skip && skip[i]) {
+    if (status) status[i] = GLB_RAY_SKIPPED;
+    return;
+  }
   y[2 * i] = x[2 * i];
   y[2 * i + 1] = x[2 * i + 1];
   A[4 * i] = 1;
   A[4 * i + 1] = 0;
   A[4 * i + 2] = 0;
   A[4 * i + 3] = 1;
+  const double AA[4] = {1, 0, 0, 1};
+  if (status) status[i] = ray_status(x + 2 * i, AA);
 }
 
 // xygridpoints + PositionFromIndex (TreeCode_link/gridmap.cpp:293-321,
@@ -845,6 +898,7 @@ void combine_planes(glb_lens *l) {
 }
 
 int upload_lens(glb_lens *l) {
+  std::lock_guard<std::mutex> lk(l->mu);
   if (!l->dirty) return 0;
   size_t np = l->planes.size();
   std::vector<PlaneDev> P(np);
@@ -874,23 +928,39 @@ int upload_lens(glb_lens *l) {
   return 0;
 }
 
-int ensure_ws(glb_lens *l, size_t n, bool per_ray) {
+// The calling thread's workspace on lens l (created on its first call).
+int thread_ws(glb_lens *l, LensWS **out) {
+  std::lock_guard<std::mutex> lk(l->mu);
+  std::unique_ptr<LensWS> &w = l->ws[std::this_thread::get_id()];
+  if (!w) {
+    auto n = std::make_unique<LensWS>();
+    n->device = l->device;
+    CKR(cudaStreamCreateWithFlags(&n->stream, cudaStreamNonBlocking));
+    for (int i = 0; i < 4; ++i) CKR(cudaEventCreate(&n->ev[i]));
+    CKR(cudaEventCreateWithFlags(&n->done, cudaEventDisableTiming));
+    w = std::move(n);
+  }
+  *out = w.get();
+  return 0;
+}
+
+int ensure_ws(LensWS *w, size_t n, bool per_ray) {
   if (n > 0xffffffffull) return fail(GLB_ERR_ARG, "too many rays in one call (max 2^32-1)");
-  if (l->ws_n < n || (per_ray && l->jmax_ray.n < n)) {
-    size_t m = std::max(n, l->ws_n);
-    CKR(l->st.alloc(12 * m));
-    CKR(l->keys.alloc(m));
-    CKR(l->keys2.alloc(m));
-    CKR(l->perm0.alloc(m));
-    CKR(l->perm.alloc(m));
-    CKR(l->jmax_ray.alloc(m));
-    CKR(l->src_ray.alloc(2 * m));
+  if (w->ws_n < n || (per_ray && w->jmax_ray.n < n)) {
+    size_t m = std::max(n, w->ws_n);
+    CKR(w->st.alloc(12 * m));
+    CKR(w->keys.alloc(m));
+    CKR(w->keys2.alloc(m));
+    CKR(w->perm0.alloc(m));
+    CKR(w->perm.alloc(m));
+    CKR(w->jmax_ray.alloc(m));
+    CKR(w->src_ray.alloc(2 * m));
     size_t tb = 0;
-    CKR(cub::DeviceRadixSort::SortPairs(nullptr, tb, l->keys.p, l->keys2.p, l->perm0.p, l->perm.p, (int)m, 0, 32,
-                                        l->stream));
-    CKR(l->sort_tmp.alloc(tb));
-    CKR(l->bbox.alloc(4));
-    l->ws_n = m;
+    CKR(cub::DeviceRadixSort::SortPairs(nullptr, tb, w->keys.p, w->keys2.p, w->perm0.p, w->perm.p, (int)m, 0, 32,
+                                        w->stream));
+    CKR(w->sort_tmp.alloc(tb));
+    CKR(w->bbox.alloc(4));
+    w->ws_n = m;
   }
   return 0;
 }
@@ -939,43 +1009,48 @@ int launch_plane_steps(const glb_lens *l, StepArgs &a, int jmax_launch, int prec
 }
 
 // The whole ray-shooting pass on device buffers, enqueued on stream s.
-int rayshoot_device(glb_lens *l, size_t n, const double *x, const double *zs, double *y, double *A,
-                    int precision, cudaStream_t s, unsigned long long *d_counts = nullptr) {
+// The workspace w is the calling thread's; a pass first waits for the end of
+// its previous pass (which may have run on another stream), since both use
+// w's buffers.
+int rayshoot_device(glb_lens *l, LensWS *w, size_t n, const double *x, const double *zs, double *y, double *A,
+                    int precision, cudaStream_t s, unsigned long long *d_counts = nullptr,
+                    unsigned char *status = nullptr, const unsigned char *skip = nullptr) {
   if (n == 0) return 0;
   size_t np = l->planes.size();
   if (np == 0) {  // no lens plane (internal_rayshooter_multi.cpp:62-76)
-    k_identity_rays<<<nblk(n, 256), 256, 0, s>>>(x, n, y, A);
+    k_identity_rays<<<nblk(n, 256), 256, 0, s>>>(x, n, y, A, status, skip);
     CKR(cudaGetLastError());
     return 0;
   }
   if (int rc = upload_lens(l)) return rc;
-  if (int rc = ensure_ws(l, n, zs != nullptr)) return rc;
-  CKR(cudaEventRecord(l->ev[0], s));
+  if (int rc = ensure_ws(w, n, zs != nullptr)) return rc;
+  CKR(cudaStreamWaitEvent(s, w->done, 0));
+  CKR(cudaEventRecord(w->ev[0], s));
   // spatial ordering of the rays along a Morton curve
   if (n >= 64) {
     unsigned long long init[4] = {~0ull, ~0ull, 0ull, 0ull};
-    CKR(cudaMemcpyAsync(l->bbox.p, init, sizeof(init), cudaMemcpyHostToDevice, s));
-    k_ray_bbox<<<std::min(nblk(n, 256), 1184), 256, 0, s>>>(x, n, l->bbox.p);
-    k_ray_morton<<<nblk(n, 256), 256, 0, s>>>(x, n, l->bbox.p, l->keys.p, l->perm0.p);
-    size_t tb = l->sort_tmp.n;
-    CKR(cub::DeviceRadixSort::SortPairs(l->sort_tmp.p, tb, l->keys.p, l->keys2.p, l->perm0.p, l->perm.p, (int)n, 0,
+    CKR(cudaMemcpyAsync(w->bbox.p, init, sizeof(init), cudaMemcpyHostToDevice, s));
+    k_ray_bbox<<<std::min(nblk(n, 256), 1184), 256, 0, s>>>(x, n, w->bbox.p);
+    k_ray_morton<<<nblk(n, 256), 256, 0, s>>>(x, n, w->bbox.p, w->keys.p, w->perm0.p);
+    size_t tb = w->sort_tmp.n;
+    CKR(cub::DeviceRadixSort::SortPairs(w->sort_tmp.p, tb, w->keys.p, w->keys2.p, w->perm0.p, w->perm.p, (int)n, 0,
                                         32, s));
   } else {
-    k_identity<<<nblk(n, 256), 256, 0, s>>>(l->perm.p, n);
+    k_identity<<<nblk(n, 256), 256, 0, s>>>(w->perm.p, n);
   }
   SrcArgs sa{l->cosmo, l->d_planez.p, l->d_Dl.p, (int)np};
-  k_init_state<<<nblk(n, 256), 256, 0, s>>>(x, zs, l->perm.p, n, l->st.p, l->jmax_ray.p, l->src_ray.p, sa);
+  k_init_state<<<nblk(n, 256), 256, 0, s>>>(x, zs, w->perm.p, n, w->st.p, w->jmax_ray.p, w->src_ray.p, sa);
 
   StepArgs a;
   a.planes = l->d_planes.p;
   a.halos = l->d_halos.p;
   if (int rc = device_nfw_tables(a.tab)) return rc;
-  a.st = l->st.p;
+  a.st = w->st.p;
   a.n = n;
   a.charge = l->charge;
   a.counts = d_counts;
-  a.jmax_ray = zs ? l->jmax_ray.p : nullptr;
-  a.src_ray = zs ? l->src_ray.p : nullptr;
+  a.jmax_ray = zs ? w->jmax_ray.p : nullptr;
+  a.src_ray = zs ? w->src_ray.p : nullptr;
   int jmax_launch = (int)np;
   a.jmax = (int)np;
   a.dls_ds = 0;
@@ -1003,11 +1078,13 @@ int rayshoot_device(glb_lens *l, size_t n, const double *x, const double *zs, do
       jmax_launch = jm;
     }
   }
-  CKR(cudaEventRecord(l->ev[1], s));
+  CKR(cudaEventRecord(w->ev[1], s));
   if (int rc = launch_plane_steps(l, a, jmax_launch, precision, s, d_counts)) return rc;
-  CKR(cudaEventRecord(l->ev[2], s));
-  k_finish<<<nblk(n, 256), 256, 0, s>>>(l->st.p, l->perm.p, n, y, A);
-  CKR(cudaEventRecord(l->ev[3], s));
+  CKR(cudaEventRecord(w->ev[2], s));
+  k_finish<<<nblk(n, 256), 256, 0, s>>>(w->st.p, w->perm.p, n, y, A, status, skip);
+  CKR(cudaEventRecord(w->ev[3], s));
+  CKR(cudaEventRecord(w->done, s));
+  w->timed = true;
   CKR(cudaGetLastError());
   return 0;
 }
@@ -1392,7 +1469,6 @@ int glb_lens_create(double zsource, double omega_m, double omega_l, double hubbl
   l->charge = 4 * kPi * kGrav;  // lens.cpp:93
   CKR(cudaGetDevice(&l->device));
   CKR(cudaStreamCreateWithFlags(&l->stream, cudaStreamNonBlocking));
-  for (int i = 0; i < 4; ++i) CKR(cudaEventCreate(&l->ev[i]));
   combine_planes(l.get());
   *out = l.release();
   return 0;
@@ -1401,13 +1477,12 @@ int glb_lens_create(double zsource, double omega_m, double omega_l, double hubbl
 int glb_lens_destroy(glb_lens *l) {
   if (!l) return 0;
   cudaSetDevice(l->device);
+  l->ws.clear();  // each workspace synchronises its stream before it is freed
   if (l->stream) cudaStreamSynchronize(l->stream);
   for (auto &h : l->owned) {
     h->tree.reset();
     if (h->stream) cudaStreamDestroy(h->stream);
   }
-  for (int i = 0; i < 4; ++i)
-    if (l->ev[i]) cudaEventDestroy(l->ev[i]);
   cudaStream_t s = l->stream;
   delete l;
   if (s) cudaStreamDestroy(s);
@@ -1614,43 +1689,74 @@ int glb_lens_reset_source(glb_lens *l, double z, int nearest, int *plane_index) 
 
 int glb_lens_rayshoot_device(glb_lens *l, size_t n, const double *x_dev, const double *zs_dev, double *y_dev,
                              double *A_dev, int precision, void *stream) {
+  return glb_lens_rayshoot_device_status(l, n, x_dev, zs_dev, nullptr, y_dev, A_dev, nullptr, precision, stream);
+}
+
+int glb_lens_rayshoot_device_status(glb_lens *l, size_t n, const double *x_dev, const double *zs_dev,
+                                    const unsigned char *skip_dev, double *y_dev, double *A_dev,
+                                    unsigned char *status_dev, int precision, void *stream) {
   if (!l) return fail(GLB_ERR_ARG, "null lens");
   if (n > 0 && (!x_dev || !y_dev || !A_dev)) return fail(GLB_ERR_ARG, "null buffer");
   if (precision != GLB_PREC_FP64 && precision != GLB_PREC_SPLIT) return fail(GLB_ERR_ARG, "unknown precision");
   if (int rc = set_dev(l->device)) return rc;
-  cudaStream_t s = stream ? (cudaStream_t)stream : l->stream;
-  return rayshoot_device(l, n, x_dev, zs_dev, y_dev, A_dev, precision, s);
+  LensWS *w;
+  if (int rc = thread_ws(l, &w)) return rc;
+  cudaStream_t s = stream ? (cudaStream_t)stream : w->stream;
+  return rayshoot_device(l, w, n, x_dev, zs_dev, y_dev, A_dev, precision, s, nullptr, status_dev, skip_dev);
 }
 
-static int rayshoot_host(glb_lens *l, size_t n, const double *x, const double *zs, double *y, double *A,
-                         int precision, bool x_on_device) {
+// Host buffers in and out through the calling thread's staging buffer and
+// stream.  x_on_device: x is already a device array (GridMap positions).
+static int rayshoot_host(glb_lens *l, LensWS *w, size_t n, const double *x, const double *zs, double *y,
+                         double *A, int precision, bool x_on_device, const unsigned char *skip = nullptr,
+                         unsigned char *status = nullptr) {
   if (n == 0) return 0;
-  size_t need = (x_on_device ? 0 : 2 * n) + (zs ? n : 0) + 6 * n;
-  if (l->io.n < need) CKR(l->io.alloc(need));
-  double *dx = x_on_device ? const_cast<double *>(x) : l->io.p;
-  double *dzs = zs ? l->io.p + (x_on_device ? 0 : 2 * n) : nullptr;
-  double *dy = l->io.p + (x_on_device ? 0 : 2 * n) + (zs ? n : 0);
+  // staging (doubles): x 2n | zs n | y 2n | A 4n | skip + status (2n bytes, rounded up)
+  const size_t flag_words = (skip || status) ? (2 * n + 7) / 8 : 0;
+  size_t need = (x_on_device ? 0 : 2 * n) + (zs ? n : 0) + 6 * n + flag_words;
+  if (w->io.n < need) CKR(w->io.alloc(need));
+  cudaStream_t s = w->stream;
+  double *dx = x_on_device ? const_cast<double *>(x) : w->io.p;
+  double *dzs = zs ? w->io.p + (x_on_device ? 0 : 2 * n) : nullptr;
+  double *dy = w->io.p + (x_on_device ? 0 : 2 * n) + (zs ? n : 0);
   double *dA = dy + 2 * n;
-  if (!x_on_device) CKR(cudaMemcpyAsync(dx, x, 2 * n * sizeof(double), cudaMemcpyHostToDevice, l->stream));
-  if (zs) CKR(cudaMemcpyAsync(dzs, zs, n * sizeof(double), cudaMemcpyHostToDevice, l->stream));
-  if (int rc = rayshoot_device(l, n, dx, dzs, dy, dA, precision, l->stream)) return rc;
-  CKR(cudaMemcpyAsync(y, dy, 2 * n * sizeof(double), cudaMemcpyDeviceToHost, l->stream));
-  CKR(cudaMemcpyAsync(A, dA, 4 * n * sizeof(double), cudaMemcpyDeviceToHost, l->stream));
-  CKR(cudaStreamSynchronize(l->stream));
+  unsigned char *dflags = reinterpret_cast<unsigned char *>(dA + 4 * n);
+  unsigned char *dskip = skip ? dflags : nullptr;
+  unsigned char *dstatus = status ? dflags + n : nullptr;
+  if (!x_on_device) CKR(cudaMemcpyAsync(dx, x, 2 * n * sizeof(double), cudaMemcpyHostToDevice, s));
+  if (zs) CKR(cudaMemcpyAsync(dzs, zs, n * sizeof(double), cudaMemcpyHostToDevice, s));
+  if (skip) {
+    // skipped rays keep the caller's y and A: start from them
+    CKR(cudaMemcpyAsync(dskip, skip, n, cudaMemcpyHostToDevice, s));
+    CKR(cudaMemcpyAsync(dy, y, 2 * n * sizeof(double), cudaMemcpyHostToDevice, s));
+    CKR(cudaMemcpyAsync(dA, A, 4 * n * sizeof(double), cudaMemcpyHostToDevice, s));
+  }
+  if (int rc = rayshoot_device(l, w, n, dx, dzs, dy, dA, precision, s, nullptr, dstatus, dskip)) return rc;
+  CKR(cudaMemcpyAsync(y, dy, 2 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CKR(cudaMemcpyAsync(A, dA, 4 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  if (status) CKR(cudaMemcpyAsync(status, dstatus, n, cudaMemcpyDeviceToHost, s));
+  CKR(cudaStreamSynchronize(s));
   if (l->planes.size() > 0) {
-    cudaEventElapsedTime(&l->last_kernel_ms, l->ev[1], l->ev[2]);
-    cudaEventElapsedTime(&l->last_total_ms, l->ev[0], l->ev[3]);
+    cudaEventElapsedTime(&w->last_kernel_ms, w->ev[1], w->ev[2]);
+    cudaEventElapsedTime(&w->last_total_ms, w->ev[0], w->ev[3]);
   }
   return 0;
 }
 
 int glb_lens_rayshoot(glb_lens *l, size_t n, const double *x, const double *zs, double *y, double *A,
                       int precision) {
+  return glb_lens_rayshoot_status(l, n, x, zs, nullptr, y, A, nullptr, precision);
+}
+
+int glb_lens_rayshoot_status(glb_lens *l, size_t n, const double *x, const double *zs, const unsigned char *skip,
+                             double *y, double *A, unsigned char *status, int precision) {
   if (!l) return fail(GLB_ERR_ARG, "null lens");
   if (n > 0 && (!x || !y || !A)) return fail(GLB_ERR_ARG, "null buffer");
   if (precision != GLB_PREC_FP64 && precision != GLB_PREC_SPLIT) return fail(GLB_ERR_ARG, "unknown precision");
   if (int rc = set_dev(l->device)) return rc;
-  return rayshoot_host(l, n, x, zs, y, A, precision, false);
+  LensWS *w;
+  if (int rc = thread_ws(l, &w)) return rc;
+  return rayshoot_host(l, w, n, x, zs, y, A, precision, false, skip, status);
 }
 
 int glb_gridmap(glb_lens *l, size_t n1d, const double *center, double range, double *y, double *A, int precision) {
@@ -1659,13 +1765,15 @@ int glb_gridmap(glb_lens *l, size_t n1d, const double *center, double range, dou
   if (range <= 0) return fail(GLB_ERR_ARG, "GridMap range is <= 0!");
   if (precision != GLB_PREC_FP64 && precision != GLB_PREC_SPLIT) return fail(GLB_ERR_ARG, "unknown precision");
   if (int rc = set_dev(l->device)) return rc;
+  LensWS *w;
+  if (int rc = thread_ws(l, &w)) return rc;
   size_t n = n1d * n1d;
   DBuf<double> dx;
   CKR(dx.alloc(2 * n));
-  k_grid<<<nblk(n, 256), 256, 0, l->stream>>>(n1d, center[0], center[1], range, dx.p);
+  k_grid<<<nblk(n, 256), 256, 0, w->stream>>>(n1d, center[0], center[1], range, dx.p);
   CKR(cudaGetLastError());
-  int rc = rayshoot_host(l, n, dx.p, nullptr, y, A, precision, true);
-  CKR(cudaStreamSynchronize(l->stream));
+  int rc = rayshoot_host(l, w, n, dx.p, nullptr, y, A, precision, true);
+  CKR(cudaStreamSynchronize(w->stream));
   return rc;
 }
 
@@ -1679,19 +1787,21 @@ int glb_gridmap_pixelmap(glb_lens *l, size_t n1d, const double *center, double r
     return fail(GLB_ERR_UNSUPPORTED, "GridMap::writePixelMap() does not work for the input LensingVariable");
   if (lensvar < 0 || lensvar > 11) return fail(GLB_ERR_ARG, "unknown LensingVariable");
   if (int rc = set_dev(l->device)) return rc;
+  LensWS *w;
+  if (int rc = thread_ws(l, &w)) return rc;
   const size_t n = n1d * n1d;
   DBuf<double> dx, dy, dA, dm;
   CKR(dx.alloc(2 * n));
   CKR(dy.alloc(2 * n));
   CKR(dA.alloc(4 * n));
   CKR(dm.alloc(n));
-  k_grid<<<nblk(n, 256), 256, 0, l->stream>>>(n1d, center[0], center[1], range, dx.p);
+  k_grid<<<nblk(n, 256), 256, 0, w->stream>>>(n1d, center[0], center[1], range, dx.p);
   CKR(cudaGetLastError());
-  if (int rc = rayshoot_device(l, n, dx.p, nullptr, dy.p, dA.p, precision, l->stream)) return rc;
-  k_pixelmap<<<nblk(n, 256), 256, 0, l->stream>>>(dx.p, dy.p, dA.p, n, lensvar, dm.p);
+  if (int rc = rayshoot_device(l, w, n, dx.p, nullptr, dy.p, dA.p, precision, w->stream)) return rc;
+  k_pixelmap<<<nblk(n, 256), 256, 0, w->stream>>>(dx.p, dy.p, dA.p, n, lensvar, dm.p);
   CKR(cudaGetLastError());
-  CKR(cudaMemcpyAsync(map, dm.p, n * sizeof(double), cudaMemcpyDeviceToHost, l->stream));
-  CKR(cudaStreamSynchronize(l->stream));
+  CKR(cudaMemcpyAsync(map, dm.p, n * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
+  CKR(cudaStreamSynchronize(w->stream));
   return 0;
 }
 
@@ -1739,19 +1849,21 @@ int glb_gridmap_surface_brightness(glb_lens *l, size_t n1d, const double *center
   SourceDev S;
   if (int rc = make_source_dev(source_kind, source_params, S)) return rc;
   if (int rc = set_dev(l->device)) return rc;
+  LensWS *w;
+  if (int rc = thread_ws(l, &w)) return rc;
   const size_t n = n1d * n1d;
   DBuf<double> dx, dy, dA, dsb;
   CKR(dx.alloc(2 * n));
   CKR(dy.alloc(2 * n));
   CKR(dA.alloc(4 * n));
   CKR(dsb.alloc(n));
-  k_grid<<<nblk(n, 256), 256, 0, l->stream>>>(n1d, center[0], center[1], range, dx.p);
+  k_grid<<<nblk(n, 256), 256, 0, w->stream>>>(n1d, center[0], center[1], range, dx.p);
   CKR(cudaGetLastError());
-  if (int rc = rayshoot_device(l, n, dx.p, nullptr, dy.p, dA.p, precision, l->stream)) return rc;
-  k_surface_brightness<<<nblk(n, 256), 256, 0, l->stream>>>(dy.p, n, S, dsb.p);
+  if (int rc = rayshoot_device(l, w, n, dx.p, nullptr, dy.p, dA.p, precision, w->stream)) return rc;
+  k_surface_brightness<<<nblk(n, 256), 256, 0, w->stream>>>(dy.p, n, S, dsb.p);
   CKR(cudaGetLastError());
-  CKR(cudaMemcpyAsync(sb, dsb.p, n * sizeof(double), cudaMemcpyDeviceToHost, l->stream));
-  CKR(cudaStreamSynchronize(l->stream));
+  CKR(cudaMemcpyAsync(sb, dsb.p, n * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
+  CKR(cudaStreamSynchronize(w->stream));
   if (total) {  // GridMap::RefreshSurfaceBrightnesses: sum in point order times resolution^2
     const double res = range / (double)(n1d - 1), res2 = pow(res, 2);
     double t = 0;
@@ -1782,7 +1894,7 @@ constexpr size_t kRefineChunk = 4u << 20;     // sub-rays per launch
 // source position, as the reference does) in one batched call; the sub-rays'
 // surface brightness is summed per pixel on the host in the reference's (u, v)
 // order.  out[k] = refined flux of pixel P[k].
-static int refine_pixels(glb_lens *l, const std::vector<size_t> &P, const std::vector<double> &ysrc,
+static int refine_pixels(glb_lens *l, LensWS *w, const std::vector<size_t> &P, const std::vector<double> &ysrc,
                          const std::vector<double> &sb0, double resolution, const SourceDev &S, int precision,
                          std::vector<double> &out) {
   const size_t np = P.size();
@@ -1817,12 +1929,12 @@ static int refine_pixels(glb_lens *l, const std::vector<size_t> &P, const std::v
             x[2 * ((size_t)u * n + v) + 1] = ll1 + (0.5 + v) * res;
           }
       }
-      CKR(cudaMemcpyAsync(dx.p, hx.data(), 2 * cnt * sizeof(double), cudaMemcpyHostToDevice, l->stream));
-      if (int rc = rayshoot_device(l, cnt, dx.p, nullptr, dy.p, dA.p, precision, l->stream)) return rc;
-      k_surface_brightness<<<nblk(cnt, 256), 256, 0, l->stream>>>(dy.p, cnt, S, dsb.p);
+      CKR(cudaMemcpyAsync(dx.p, hx.data(), 2 * cnt * sizeof(double), cudaMemcpyHostToDevice, w->stream));
+      if (int rc = rayshoot_device(l, w, cnt, dx.p, nullptr, dy.p, dA.p, precision, w->stream)) return rc;
+      k_surface_brightness<<<nblk(cnt, 256), 256, 0, w->stream>>>(dy.p, cnt, S, dsb.p);
       CKR(cudaGetLastError());
-      CKR(cudaMemcpyAsync(hsb.data(), dsb.p, cnt * sizeof(double), cudaMemcpyDeviceToHost, l->stream));
-      CKR(cudaStreamSynchronize(l->stream));
+      CKR(cudaMemcpyAsync(hsb.data(), dsb.p, cnt * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
+      CKR(cudaStreamSynchronize(w->stream));
       for (size_t a = a0; a < a1; ++a) {
         const size_t k = act[a];
         of[k] = nf[k];
@@ -1852,6 +1964,8 @@ int glb_gridmap_adaptive_surface_brightness(glb_lens *l, size_t n1d, const doubl
   if (int rc = glb_gridmap(l, n1d, center, range, ysrc.data(), A.data(), precision)) return rc;
   SourceDev S;
   if (int rc = make_source_dev(source_kind, source_params, S)) return rc;
+  LensWS *w;
+  if (int rc = thread_ws(l, &w)) return rc;
   const double resolution = range / (double)(n1d - 1);
   double total_flux = total0 / resolution / resolution;  // gridmap.cpp:195
   if (total_flux == 0) {
@@ -1867,7 +1981,7 @@ int glb_gridmap_adaptive_surface_brightness(glb_lens *l, size_t n1d, const doubl
     for (long i = 0; i < N; ++i)
       if (to_refine(sb, i, j, N, total_flux, f)) cand.push_back((size_t)(i + j * N));
   std::vector<double> refined;
-  if (int rc = refine_pixels(l, cand, ysrc, sb, resolution, S, precision, refined)) return rc;
+  if (int rc = refine_pixels(l, w, cand, ysrc, sb, resolution, S, precision, refined)) return rc;
   std::vector<double> cache(n, 0.0);
   std::vector<char> have(n, 0);
   for (size_t k = 0; k < cand.size(); ++k) {
@@ -1885,7 +1999,7 @@ int glb_gridmap_adaptive_surface_brightness(glb_lens *l, size_t n1d, const doubl
         nfl = cache[k];
       } else {
         std::vector<double> one;
-        if (int rc = refine_pixels(l, std::vector<size_t>{k}, ysrc, sb, resolution, S, precision, one)) return rc;
+        if (int rc = refine_pixels(l, w, std::vector<size_t>{k}, ysrc, sb, resolution, S, precision, one)) return rc;
         nfl = one[0];
       }
       total_flux -= sb[k];
@@ -1902,35 +2016,39 @@ int glb_lens_count_interactions(glb_lens *l, size_t n, const double *x, const do
                                 unsigned long long *counts) {
   if (!l || !counts || (n > 0 && !x)) return fail(GLB_ERR_ARG, "null argument");
   if (int rc = set_dev(l->device)) return rc;
+  LensWS *w;
+  if (int rc = thread_ws(l, &w)) return rc;
   DBuf<double> dx, dzs, dy, dA;
   DBuf<unsigned long long> dc;
   CKR(dx.alloc(2 * n));
   CKR(dy.alloc(2 * n));
   CKR(dA.alloc(4 * n));
   CKR(dc.alloc(7));
-  CKR(cudaMemsetAsync(dc.p, 0, 7 * sizeof(unsigned long long), l->stream));
-  CKR(cudaMemcpyAsync(dx.p, x, 2 * n * sizeof(double), cudaMemcpyHostToDevice, l->stream));
+  CKR(cudaMemsetAsync(dc.p, 0, 7 * sizeof(unsigned long long), w->stream));
+  CKR(cudaMemcpyAsync(dx.p, x, 2 * n * sizeof(double), cudaMemcpyHostToDevice, w->stream));
   if (zs) {
     CKR(dzs.alloc(n));
-    CKR(cudaMemcpyAsync(dzs.p, zs, n * sizeof(double), cudaMemcpyHostToDevice, l->stream));
+    CKR(cudaMemcpyAsync(dzs.p, zs, n * sizeof(double), cudaMemcpyHostToDevice, w->stream));
   }
-  if (int rc = rayshoot_device(l, n, dx.p, zs ? dzs.p : nullptr, dy.p, dA.p, GLB_PREC_FP64, l->stream, dc.p))
+  if (int rc = rayshoot_device(l, w, n, dx.p, zs ? dzs.p : nullptr, dy.p, dA.p, GLB_PREC_FP64, w->stream, dc.p))
     return rc;
-  CKR(cudaMemcpyAsync(counts, dc.p, 7 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, l->stream));
-  CKR(cudaStreamSynchronize(l->stream));
+  CKR(cudaMemcpyAsync(counts, dc.p, 7 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, w->stream));
+  CKR(cudaStreamSynchronize(w->stream));
   return 0;
 }
 
 int glb_lens_last_timing(glb_lens *l, double *kernel_ms, double *total_ms) {
   if (!l) return fail(GLB_ERR_ARG, "null lens");
   if (int rc = set_dev(l->device)) return rc;
-  if (l->planes.size() > 0 && cudaEventQuery(l->ev[0]) != cudaErrorNotReady) {
-    CKR(cudaEventSynchronize(l->ev[3]));
-    cudaEventElapsedTime(&l->last_kernel_ms, l->ev[1], l->ev[2]);
-    cudaEventElapsedTime(&l->last_total_ms, l->ev[0], l->ev[3]);
+  LensWS *w;
+  if (int rc = thread_ws(l, &w)) return rc;
+  if (l->planes.size() > 0 && w->timed && cudaEventQuery(w->ev[0]) != cudaErrorNotReady) {
+    CKR(cudaEventSynchronize(w->ev[3]));
+    cudaEventElapsedTime(&w->last_kernel_ms, w->ev[1], w->ev[2]);
+    cudaEventElapsedTime(&w->last_total_ms, w->ev[0], w->ev[3]);
   }
-  if (kernel_ms) *kernel_ms = l->last_kernel_ms;
-  if (total_ms) *total_ms = l->last_total_ms;
+  if (kernel_ms) *kernel_ms = w->last_kernel_ms;
+  if (total_ms) *total_ms = w->last_total_ms;
   return 0;
 }
 
@@ -1974,6 +2092,12 @@ __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
 std::mutex g_noalloc_mu;
 unsigned char *g_noalloc_ptr[64] = {};
+// Calls on one device are put in order on the GPU: each call's stream waits
+// for the previous call's last launch (an event, not an allocation), and the
+// enqueue itself is serialised on the host, so two calls never use the
+// shared scratch at the same time whatever streams or lenses they name.
+cudaEvent_t g_noalloc_ev[64] = {};
+std::mutex g_noalloc_call_mu;
 
 // Once per device, with that device current: the device address of the
 // scratch array (its host-side name is only a stand-in) and the NFW tables.
@@ -1993,6 +2117,7 @@ int noalloc_setup(int dev, unsigned char **out) {
     CKR(cub::DeviceRadixSort::SortPairs(nullptr, tb, (unsigned *)nullptr, (unsigned *)nullptr,
                                         (unsigned *)nullptr, (unsigned *)nullptr, (int)kNoAllocMaxRays, 0, 32));
     if (tb > kNoAllocSortBytes) return fail(GLB_ERR_ARG, "no-alloc scratch: radix-sort temporary storage too small");
+    CKR(cudaEventCreateWithFlags(&g_noalloc_ev[dev], cudaEventDisableTiming));
     g_noalloc_ptr[dev] = p;
   }
   *out = g_noalloc_ptr[dev];
@@ -2055,6 +2180,9 @@ extern "C" int glb_lens_rayshoot_noalloc(glb_lens *l, size_t n, const double *x_
     CKR(cudaGetLastError());
     return 0;
   }
+  // from here on the scratch is in use: after the previous call on this device
+  std::lock_guard<std::mutex> order(g_noalloc_call_mu);
+  CKR(cudaStreamWaitEvent(s, g_noalloc_ev[l->device], 0));
   // plane and halo descriptors of this lens (host stack arrays, no heap),
   // copied into the scratch; pageable copies are staged before they return
   PlaneDev P[kNoAllocMaxPlanes];
@@ -2138,6 +2266,7 @@ extern "C" int glb_lens_rayshoot_noalloc(glb_lens *l, size_t n, const double *x_
   if (int rc = launch_plane_steps(l, a, jmax_launch, precision, s, nullptr)) return rc;
   k_finish<<<nblk(n, 256), 256, 0, s>>>(st, perm, n, y_dev, A_dev);
   CKR(cudaGetLastError());
+  CKR(cudaEventRecord(g_noalloc_ev[l->device], s));
   return 0;
 }
 

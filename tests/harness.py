@@ -308,10 +308,11 @@ class PlaneRecursion:
                 al -= a; kap += k; g0 += g[:, 0]; g1 += g[:, 1]
         return al, kap, g0, g1
 
-    def shoot(self, x, alpha_prec, G_prec, noise=0.0, seed=0):
+    def shoot(self, x, alpha_prec, G_prec, noise=0.0, seed=0, g_noise=0.0):
         """y (n,2), A (n,4) with the deflection from alpha_prec (times
-        1 + noise * N(0,1) per component) and kappa/gamma from G_prec, both
-        evaluated at the positions this recursion produces."""
+        1 + noise * N(0,1) per component) and kappa/gamma from G_prec (times
+        1 + g_noise * N(0,1) per component), both evaluated at the positions
+        this recursion produces."""
         rs = np.random.default_rng(seed)
         x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1, 2)
         n = len(x)
@@ -325,7 +326,10 @@ class PlaneRecursion:
             fg = fa if G_prec == alpha_prec else self.plane_force(j, xx, G_prec)
             al = fa[0] * (1 + noise * rs.standard_normal(fa[0].shape)) if noise else fa[0]
             Gf = ch * Dl[j] / (1 + z[j])
-            G0, G1, G3 = Gf * (fg[1] + fg[2]), Gf * fg[3], Gf * (fg[1] - fg[2])
+            kap, g0, g1 = fg[1], fg[2], fg[3]
+            if g_noise:
+                kap, g0, g1 = (v * (1 + g_noise * rs.standard_normal(v.shape)) for v in (kap, g0, g1))
+            G0, G1, G3 = Gf * (kap + g0), Gf * g1, Gf * (kap - g0)
             sa = sa - ch * al
             aa, bb = dDl[j + 1] / Dl[j + 1], Dl[j] / Dl[j + 1]
             th = bb * th + aa * sa
