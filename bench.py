@@ -628,6 +628,7 @@ def main():
     import torch.distributed as dist
     import slsimlib_b200 as glb
     from slsimlib_b200 import synth
+    from slsimlib_b200.replicas import max_over_ranks
 
     torch.cuda.set_device(local)
     if world > 1:
@@ -676,11 +677,8 @@ def main():
             shoot(glb.PREC_SPLIT)
         t1.record(stream)
         torch.cuda.synchronize()
-    ms = t0.elapsed_time(t1)
+    ms = max_over_ranks(t0.elapsed_time(t1), device=dev)
     if world > 1:
-        tt = torch.tensor([ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
         dist.barrier()
     # per-launch plane-step time from the library's events (last step)
     shoot(glb.PREC_SPLIT)
@@ -718,11 +716,7 @@ def main():
     h0 = time.perf_counter()
     for _ in range(args.steps):
         shoot_host()
-    e2e_s = time.perf_counter() - h0
-    if world > 1:
-        tt = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = float(tt.item())
+    e2e_s = max_over_ranks(time.perf_counter() - h0, device=dev)
 
     if rank == 0:
         clocks = clk.summary()

@@ -127,6 +127,14 @@ int glb_halo_nfw(float mass, float Rsize, double z, float concentration, float f
  * float pa, cosmo) (MultiPlane/lens_halos.cpp:1043-1078). */
 int glb_halo_nsie(float mass, double z, float sigma, float rcore, float fratio, float pa,
                   glb_halo **out);
+/* An NSIE with the member values a constructed LensHaloRealNSIE holds
+ * (include/lens_halos.h:1023-1070; constructor MultiPlane/lens_halos.cpp:1043-1078):
+ * mass (after the cored halo's mass reset by integration, lens_halos.cpp:1073-1075),
+ * Rsize, Rmax, sigma, rcore, fratio and the stored angle pa_internal
+ * (= pi/2 - the constructor's pa, lens_halos.cpp:1058).  For mirroring an
+ * existing reference halo exactly (the link-level drop-in). */
+int glb_halo_nsie_state(float mass, float Rsize, float Rmax, double z, float sigma, float rcore, float fratio,
+                        float pa_internal, glb_halo **out);
 /* LensHalo::setTheta (include/lens_halos.h:105): angular position, radians. */
 int glb_halo_set_theta(glb_halo *h, double tx, double ty);
 /* LensHalo::force_halo (include/lens_halos.h:182-190) at n positions xcm

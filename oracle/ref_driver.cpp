@@ -25,6 +25,8 @@
  *                                                    TIMEFILE gets the ctor wall seconds
  *   rays XFILE N ZFILE OUT TIMEFILE                  rayshooterInternal(N, RAY*) with per-ray z
  *   points XFILE N OUT TIMEFILE                      rayshooterInternal(N, Point*)
+ *   lpoints XFILE N ZFILE OUT                        rayshooterInternal(N, LinkedPoint*, source_zs)
+ *   rayshooter XFILE N OUT                           rayshooter(RAY&) per ray
  *   sourcesb KIND A B C D E F G YFILE N OUT
  *        Source::SurfaceBrightness at N source-plane positions -> OUT: N values
  *        and the source's total flux.  KIND 0 SourceUniform(Point_2d(A,B), 1, C);
@@ -56,12 +58,32 @@
  *   smooth PFILE N NSMOOTH OUT TIMEFILE
  *        LensHaloParticles<ParticleType<float>>::calculate_smoothing -> OUT: the
  *        N particle sizes; TIMEFILE gets the wall seconds.
+ * Refinement clients of rayshooterInternal (the reference's own code, run
+ * through whichever rayshooter the binary was linked with):
+ *   findcritmap N CX CY RANGE OUT
+ *        GridMap ctor + ImageFinding::find_crit(lens, gridmap, curves)
+ *        (TreeCode_link/find_crit.cpp:1036-1090) -> OUT: curves (see dump_curves).
+ *   magcontour N CX CY RANGE INVMAG OUT
+ *        GridMap ctor + ImageFinding::find_magnification_contour -> OUT:
+ *        {ncontours, per contour: n, hits_boundary, per point x[2] y[2] A[4]}.
+ *   gridrefine N CX CY RANGE STRIDE OUT
+ *        Grid ctor, then Grid::RefineLeaves on every STRIDE-th image point
+ *        (TreeCode_link/grid_maintenance.cpp:543-600) -> OUT: {npoints, per
+ *        point (point-list order) x[2] image->x[2] A[4]}.
+ *   gridcrit N CX CY RANGE RES OUT
+ *        Grid ctor + ImageFinding::find_crit(lens, grid, curves, &n, RES)
+ *        (kist refinement rounds, TreeCode_link/find_crit.cpp:37-) -> OUT: curves.
+ *   dropin PREC   the GPU drop-in's precision (binaries linked with it only)
  */
 #include "slsimlib.h"
 #include "particle_halo.h"
 #include "sersic_source.h"
 #include "gridmap.h"
+#include "grid_maintenance.h"
 #include "oracle.h"
+#ifdef GLAMER_B200_DROPIN
+#include "glamer_b200_dropin.hpp"
+#endif
 
 #include <chrono>
 #include <cstdio>
@@ -128,6 +150,24 @@ static void fix_cored_nsie_mass(LensHaloRealNSIE &h, float nominal_mass) {
     h.setMass(nominal_mass);
     h.setMass(h.MassBy1DIntegation(h.getRsize()));
   }
+}
+
+/* {ncurves, per curve: type, touches_edge, npoints, critical_area,
+ * critical_center[2], caustic_area, caustic_center[2], then per point of
+ * critcurve x[2] y[2] A[4]} */
+static void dump_curves(const std::string &out, const std::vector<ImageFinding::CriticalCurve> &c) {
+  std::vector<double> o{(double)c.size()};
+  for (const auto &k : c) {
+    double h[9] = {(double)(int)k.type, (double)k.touches_edge, (double)k.critcurve.size(), k.critical_area,
+                   k.critical_center[0], k.critical_center[1], k.caustic_area, k.caustic_center[0],
+                   k.caustic_center[1]};
+    o.insert(o.end(), h, h + 9);
+    for (const RAY &r : k.critcurve) {
+      double v[8] = {r.x[0], r.x[1], r.y[0], r.y[1], r.A.a[0], r.A.a[1], r.A.a[2], r.A.a[3]};
+      o.insert(o.end(), v, v + 8);
+    }
+  }
+  write_arr(out, o);
 }
 
 int main() {
@@ -296,6 +336,33 @@ int main() {
       }
       write_arr(out, o);
       write_time(tf, secs);
+    } else if (cmd == "lpoints" || cmd == "rayshooter") {
+      std::string xf, zf, out;
+      size_t n;
+      in >> xf >> n;
+      if (cmd == "lpoints") in >> zf;
+      in >> out;
+      std::vector<double> x = read_arr<double>(xf, 2 * n), o(6 * n);
+      if (cmd == "lpoints") {
+        std::vector<double> z = read_arr<double>(zf, n);
+        std::vector<LinkedPoint> p(n);
+        for (size_t i = 0; i < n; ++i) { p[i].x[0] = x[2 * i]; p[i].x[1] = x[2 * i + 1]; }
+        lens->rayshooterInternal(n, p.data(), z);
+        for (size_t i = 0; i < n; ++i) {
+          double v[6] = {p[i].image->x[0], p[i].image->x[1], p[i].A.a[0], p[i].A.a[1], p[i].A.a[2], p[i].A.a[3]};
+          std::copy(v, v + 6, &o[6 * i]);
+        }
+      } else {
+        for (size_t i = 0; i < n; ++i) {
+          RAY r;
+          r.x[0] = x[2 * i];
+          r.x[1] = x[2 * i + 1];
+          lens->rayshooter(r);
+          double v[6] = {r.y[0], r.y[1], r.A.a[0], r.A.a[1], r.A.a[2], r.A.a[3]};
+          std::copy(v, v + 6, &o[6 * i]);
+        }
+      }
+      write_arr(out, o);
     } else if (cmd == "sourcesb") {
       int kind;
       double p[7];
@@ -368,6 +435,71 @@ int main() {
         std::copy(v, v + 7, &o[7 * k]);
       }
       write_arr(out, o);
+    } else if (cmd == "findcritmap" || cmd == "magcontour") {
+      size_t N;
+      double c[2], range, invmag = 0;
+      std::string out;
+      in >> N >> c[0] >> c[1] >> range;
+      if (cmd == "magcontour") in >> invmag;
+      in >> out;
+      GridMap gm(lens.get(), N, c, range);
+      if (cmd == "findcritmap") {
+        std::vector<ImageFinding::CriticalCurve> crits;
+        ImageFinding::find_crit(*lens, gm, crits);
+        dump_curves(out, crits);
+      } else {
+        std::vector<std::vector<RAY>> contour;
+        std::vector<bool> hits;
+        ImageFinding::find_magnification_contour(*lens, gm, invmag, contour, hits);
+        std::vector<double> o{(double)contour.size()};
+        for (size_t i = 0; i < contour.size(); ++i) {
+          o.push_back((double)contour[i].size());
+          o.push_back((double)hits[i]);
+          for (const RAY &r : contour[i]) {
+            double v[8] = {r.x[0], r.x[1], r.y[0], r.y[1], r.A.a[0], r.A.a[1], r.A.a[2], r.A.a[3]};
+            o.insert(o.end(), v, v + 8);
+          }
+        }
+        write_arr(out, o);
+      }
+    } else if (cmd == "gridrefine" || cmd == "gridcrit") {
+      size_t N;
+      double c[2], range, arg;
+      std::string out;
+      in >> N >> c[0] >> c[1] >> range >> arg >> out;
+      Grid grid(lens.get(), N, c, range);
+      if (cmd == "gridrefine") {
+        std::vector<Point *> pts;
+        PointList::iterator it;
+        it.current = grid.i_tree->pointlist.Top();
+        const size_t stride = (size_t)arg;
+        for (size_t i = 0; i < grid.i_tree->pointlist.size(); ++i, --it)
+          if (i % stride == 0) pts.push_back(*it);
+        grid.RefineLeaves(lens.get(), pts);
+        std::vector<double> o{(double)grid.i_tree->pointlist.size()};
+        it.current = grid.i_tree->pointlist.Top();
+        for (size_t i = 0; i < grid.i_tree->pointlist.size(); ++i, --it) {
+          const Point *p = *it;
+          double v[8] = {p->x[0], p->x[1], p->image->x[0], p->image->x[1], p->A.a[0], p->A.a[1], p->A.a[2],
+                         p->A.a[3]};
+          o.insert(o.end(), v, v + 8);
+        }
+        write_arr(out, o);
+      } else {
+        std::vector<ImageFinding::CriticalCurve> crits;
+        int ncrit = 0;
+        ImageFinding::find_crit(lens.get(), &grid, crits, &ncrit, arg, 0.0, false);
+        crits.resize(ncrit);
+        dump_curves(out, crits);
+      }
+    } else if (cmd == "dropin") {
+      int prec;
+      in >> prec;
+#ifdef GLAMER_B200_DROPIN
+      glamer_b200_dropin::set_precision(prec);
+#else
+      (void)prec;
+#endif
     } else if (cmd == "smooth") {
       std::string pf, out, tf;
       size_t n;

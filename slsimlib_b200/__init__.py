@@ -59,7 +59,7 @@ EXPORTED = [
     "glb_tree_create", "glb_tree_destroy", "glb_tree_force2D_recur", "glb_tree_force_device", "glb_tree_export",
     "glb_tree_build_ms", "glb_direct_sum_device",
     "glb_halo_particles", "glb_halo_nfw", "glb_halo_nsie", "glb_halo_set_theta", "glb_halo_force",
-    "glb_halo_params", "glb_halo_destroy", "glb_halo_field_plane",
+    "glb_halo_params", "glb_halo_destroy", "glb_halo_field_plane", "glb_halo_nsie_state",
     "glb_lens_create", "glb_lens_destroy", "glb_lens_insert_halo", "glb_lens_insert_field_plane",
     "glb_lens_nplanes", "glb_lens_planes",
     "glb_lens_reset_source", "glb_lens_rayshoot", "glb_lens_rayshoot_device", "glb_lens_rayshoot_status",

@@ -61,8 +61,22 @@ def build_library(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
+def reference_dir():
+    """The reference source tree the oracle binaries are compiled from (read
+    only): $GLAMER_REFERENCE, else the checkout this build was prepared beside;
+    None when neither exists (the GPU box: the binaries travel prebuilt)."""
+    for d in (os.environ.get("GLAMER_REFERENCE"), "/root/reference"):
+        if d and os.path.exists(os.path.join(d, "include", "quadTree.h")):
+            return d
+    return None
+
+
 def build_oracle() -> None:
-    subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
+    cmd = ["make", "-s", "-C", os.path.join(ROOT, "oracle")]
+    ref = reference_dir()
+    if ref:
+        cmd.append(f"REF={ref}")
+    subprocess.check_call(cmd)
 
 
 if __name__ == "__main__":

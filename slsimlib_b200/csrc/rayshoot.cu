@@ -106,8 +106,9 @@ int device_nfw_tables(NFWTables &out) {
   std::call_once(g_nfw_host_once, make_host_tables);
   int dev = 0;
   CKR(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(GLB_ERR_ARG, "device index beyond the 64 devices the library supports");
   std::lock_guard<std::mutex> lk(g_dev_nfw_mu);
-  DevNFWTables &D = g_dev_nfw[dev & 63];
+  DevNFWTables &D = g_dev_nfw[dev];
   if (!D.x) {
     double **dst[5] = {&D.x, &D.f, &D.g, &D.g2, &D.h};
     const std::vector<double> *src[5] = {&g_nfw_host.x, &g_nfw_host.f, &g_nfw_host.g, &g_nfw_host.g2,
@@ -1408,6 +1409,36 @@ int glb_halo_nsie(float mass, double z, float sigma, float rcore, float fratio, 
     d.mass = (double)h->mass;
   }
   *out = h.release();
+  return 0;
+}
+
+int glb_halo_nsie_state(float mass, float Rsize, float Rmax, double z, float sigma, float rcore, float fratio,
+                        float pa_internal, glb_halo **out) {
+  if (!out) return fail(GLB_ERR_ARG, "null argument");
+  if (!(Rsize > 0) || !(Rmax >= Rsize)) return fail(GLB_ERR_ARG, "need 0 < Rsize <= Rmax");
+  // the constructor's arithmetic for everything but the size, the mass and the
+  // angle, which are then set to the values the mirrored halo holds
+  glb_halo *h = nullptr;
+  if (int rc = glb_halo_nsie(mass, z, sigma, 0.0f, fratio, 0.0f, &h)) return rc;
+  h->mass = mass;
+  h->Rsize = Rsize;
+  h->Rmax = Rmax;
+  NSIEDev &d = h->nsie;
+  d.bc = (double)rcore;
+  const double p = (double)pa_internal;
+  d.c1 = cos(p);
+  d.s1 = sin(p);
+  d.c2 = cos(-p);
+  d.s2 = sin(-p);
+  d.c3 = cos(-2 * p);
+  d.s3 = sin(-2 * p);
+  d.Rsize = (double)Rsize;
+  d.Rmax = (double)Rmax;
+  d.Rsize2 = (double)(Rsize * Rsize);
+  d.Rmax2 = (double)(Rmax * Rmax);
+  d.dRmaxRsize = (double)(Rmax - Rsize);
+  d.mass = (double)mass;
+  *out = h;
   return 0;
 }
 

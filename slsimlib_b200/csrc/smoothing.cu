@@ -727,10 +727,11 @@ Status smooth_particles_device(const glb_particle_rec *d_p, size_t n, int nsmoot
     DBuf<int> flags;
     DBuf<unsigned char> tmp;
   };
-  static Workspace *wss = new Workspace[16];
+  static Workspace *wss = new Workspace[64];
   int dev = 0;
   CK(cudaGetDevice(&dev));
-  Workspace &w = wss[dev & 15];
+  if (dev < 0 || dev >= 64) return Status::err(-1, "device index beyond the 64 devices the library supports");
+  Workspace &w = wss[dev];
   std::lock_guard<std::mutex> lock(w.mu);
   if (w.n < n) {
     CK(w.key.alloc(n));

@@ -277,18 +277,19 @@ class MakeParticleLenses:
         # same place; the kept records are then sorted by type if more than one
         # type has particles (stable here; the reference's std::sort leaves the
         # order within a type unspecified)
-        d = self.data.copy()
+        # The scan's result in closed form: with K records kept, a kept record
+        # at a position below K stays there, and the removed records' places
+        # below K, in ascending order, receive the kept records at K and above
+        # taken from the end backwards (each swap brings in the last record
+        # not yet scanned).
+        d = self.data
         out = r2 > float(radius) * float(radius)
-        i, end = 0, len(d)
-        while i < end:
-            if out[i]:
-                self.nparticles[int(d["type"][i])] -= 1
-                end -= 1
-                d[[i, end]] = d[[end, i]]
-                out[[i, end]] = out[[end, i]]
-            else:
-                i += 1
-        d = d[:end]
+        for t, c in zip(*np.unique(d["type"][out], return_counts=True)):
+            self.nparticles[int(t)] -= int(c)
+        K = int(np.count_nonzero(~out))
+        order = np.arange(K)
+        order[np.nonzero(out[:K])[0]] = (np.nonzero(~out[K:])[0] + K)[::-1]
+        d = d[order]
         if sum(1 for k in self.nparticles if k > 0) > 1:
             d = d[np.argsort(d["type"], kind="stable")]
         self.data = d

@@ -2,26 +2,12 @@
 
 Rays are independent and lenses are read-only, so the path needs no
 collective: every process (one per GPU) holds a replica of the lens and shoots
-its own rays.  Two layouts:
-
-* weak scaling (``bench.py``): every rank shoots a full grid;
-* strong scaling: one grid split into contiguous, Morton-ordered ray ranges,
-  ``shard(n, rank, world)``.
-
-The only communication is timing: ``max_over_ranks`` (the slowest rank sets
-the wall time) and barriers, over whatever torch.distributed backend the
-process group uses (NCCL on GPUs, gloo in the CPU tests).
+its own grid (weak scaling, ``bench.py --gpus N``).  The only communication is
+timing: ``max_over_ranks`` (the slowest rank sets the time) over whatever
+torch.distributed backend the process group uses (NCCL on GPUs, gloo in the
+CPU tests).
 """
 from __future__ import annotations
-
-
-def shard(n: int, rank: int, world: int) -> tuple[int, int]:
-    """Contiguous range [lo, hi) of n rays for `rank`; sizes differ by <= 1."""
-    if world <= 0 or not 0 <= rank < world:
-        raise ValueError("rank outside [0, world)")
-    q, r = divmod(n, world)
-    lo = rank * q + min(rank, r)
-    return lo, lo + q + (1 if rank < r else 0)
 
 
 def max_over_ranks(value: float, device=None) -> float:

@@ -17,6 +17,9 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_DIR = os.path.join(ROOT, "oracle")
 ORACLE_SO = os.path.join(ORACLE_DIR, "liboracle.so")
 REF_BIN = os.path.join(ORACLE_DIR, "_ref", "glamer_ref")
+# the reference's sources linked with the GPU drop-in (slsimlib_b200/dropin) in
+# place of FullRange/internal_rayshooter_multi.cpp
+DROPIN_BIN = os.path.join(ORACLE_DIR, "_ref", "glamer_gpu")
 
 _dp = C.POINTER(C.c_double)
 _vp = C.c_void_p
@@ -371,9 +374,12 @@ def ref_available() -> bool:
 
 
 class RefDriver:
-    """Runs commands against the reference compiled in place (oracle/_ref)."""
+    """Runs commands against the reference compiled in place (oracle/_ref);
+    binary=DROPIN_BIN runs the same reference code with the GPU drop-in as
+    its rayshooter."""
 
-    def __init__(self):
+    def __init__(self, binary: str = REF_BIN):
+        self.bin = binary
         self.tmp = tempfile.mkdtemp(prefix="glamer_ref_")
         self.lines = []
         self.k = 0
@@ -387,7 +393,7 @@ class RefDriver:
 
     def run(self, lines, timeout=3600):
         script = "\n".join(lines) + "\n"
-        r = subprocess.run([REF_BIN], input=script.encode(), stdout=subprocess.PIPE,
+        r = subprocess.run([self.bin], input=script.encode(), stdout=subprocess.PIPE,
                            stderr=subprocess.PIPE, timeout=timeout)
         if r.returncode != 0:
             raise RuntimeError(f"glamer_ref failed: {r.stderr.decode()[-2000:]}")
