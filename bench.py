@@ -509,7 +509,8 @@ def run_batched(args):
     m = float(np.median(ms))
     line = _base_line(args, "rays/s/GPU, batched uneven lenses in one persistent launch", "rays/s", total / (m / 1e3),
                       m, "f32+f64", f"{nl} lens realisations, {total} rays, {rp} ray-planes, CUDA graph",
-                      ray_planes_per_s=rp / (m / 1e3), autotune={"block": block, "ms": tune_ms},
+                      ray_planes_per_s=rp / (m / 1e3), autotune={"block": block, "tile": f"{b.tile()}x{32 // b.tile()}",
+                                                                  "ms": tune_ms},
                       plain_fp64={"value": total / (ms64 / 1e3), "unit": "rays/s"},
                       errors_vs_fp64_alpha={"median_of_medians": float(np.median([e["median"] for e in errs])),
                                             "max_p999": float(max(e["p999"] for e in errs))})

@@ -236,6 +236,20 @@ int glb_gridmap(glb_lens *l, size_t n1d, const double *center, double range, dou
 int glb_gridmap_pixelmap(glb_lens *l, size_t n1d, const double *center, double range, int lensvar, double *map,
                          int precision);
 
+/* GridMap(lens, N1d, center, range).writePixelMapUniform<double>(map_center,
+ * nx, ny, lensvar) (include/gridmap.h:98-102,506-690): a PixelMap of nx x ny
+ * pixels of side range / (nx - 1) centred on map_center (cleared to 0); each
+ * grid point writes its LensingVariable value into the pixel that
+ * PixelMap::find_index gives for its image position
+ * (ImageProcessing/pixelmap.cpp: ix = (long)((x - lower corner) / resolution),
+ * points outside dropped).  Where several grid points fall in one pixel the
+ * reference keeps the last written (from its threads' chunks; one thread: the
+ * largest grid index); here the largest grid index.  map: nx * ny doubles,
+ * index ix + nx * iy.  lensvar as glb_gridmap_pixelmap; nx >= 2. */
+int glb_gridmap_pixelmap_uniform(glb_lens *l, size_t n1d, const double *center, double range,
+                                 const double *map_center, size_t nx, size_t ny, int lensvar, double *map,
+                                 int precision);
+
 /* GridMap(lens, N1d, center, range).RefreshSurfaceBrightnesses(&source)
  * (TreeCode_link/gridmap.cpp:174-187): the grid shot on the GPU and the
  * source's surface brightness evaluated there at every ray's source-plane
@@ -307,19 +321,25 @@ int glb_lens_count_interactions(glb_lens *l, size_t n, const double *x, const do
 /* No counterpart in the reference (which shoots one GridMap at a time under a
  * global mutex, TreeCode_link/gridmap.cpp:15,116-119): the GridMaps of many
  * lenses (nlens lenses, grid sides n1d[i], centres centers[2i..2i+1], ranges
- * ranges[i]) shot by one persistent kernel launch.  Each warp takes 8 x 4-ray
- * grid tiles from a shared counter and carries them through all planes of
- * their lens.  The lenses stay owned by the caller and must outlive the batch. */
+ * ranges[i]) shot by one persistent kernel launch.  Each warp takes 32-ray
+ * grid tiles (8 x 4 by default) from a shared counter and carries them through
+ * all planes of their lens.  The lenses stay owned by the caller and must
+ * outlive the batch. */
 typedef struct glb_batch glb_batch;
 int glb_batch_create_grids(glb_lens *const *lenses, int nlens, const size_t *n1d, const double *centers,
                            const double *ranges, int precision, glb_batch **out);
 /* Runs the batch; use_graph != 0 records the launch into a CUDA graph on the
  * first call and replays it afterwards.  Returns when the results are ready. */
 int glb_batch_run(glb_batch *b, int use_graph);
-/* Times block sizes 64, 128 and 256 (persistent grid each) and keeps the
- * fastest. */
+/* Autotuner: times block sizes 64, 128 and 256 (persistent grid each) at the
+ * current tile, then warp tiles of 8 x 4, 16 x 2 and 32 x 1 rays at the best
+ * block size, and keeps the fastest pair (the walk is stackless: no stack
+ * depth to tune). */
 int glb_batch_autotune(glb_batch *b, int *best_block, double *best_ms);
 int glb_batch_set_block(glb_batch *b, int block);
+/* The warp tile's width in rays (8, 16 or 32; height 32 / width). */
+int glb_batch_tile(glb_batch *b, int *tile_width);
+int glb_batch_set_tile(glb_batch *b, int tile_width);
 int glb_batch_info(glb_batch *b, size_t *total_rays, double *last_ms, int *block);
 /* y (2 n1d^2) and A (4 n1d^2) of lens i, GridMap order, host memory. */
 int glb_batch_result(glb_batch *b, int i, double *y, double *A);

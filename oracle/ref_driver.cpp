@@ -74,6 +74,9 @@
  *        Grid ctor + ImageFinding::find_crit(lens, grid, curves, &n, RES)
  *        (kist refinement rounds, TreeCode_link/find_crit.cpp:37-) -> OUT: curves.
  *   dropin PREC   the GPU drop-in's precision (binaries linked with it only)
+ *   uniform N CX CY RANGE MCX MCY NX NY VAR OUT
+ *        GridMap ctor + writePixelMapUniform<double>({MCX, MCY}, NX, NY,
+ *        LensingVariable VAR) (include/gridmap.h:506-690) -> OUT: NX*NY values.
  */
 #include "slsimlib.h"
 #include "particle_halo.h"
@@ -492,6 +495,17 @@ int main() {
         crits.resize(ncrit);
         dump_curves(out, crits);
       }
+    } else if (cmd == "uniform") {
+      size_t N, nx, ny;
+      double c[2], mc[2], range;
+      int var;
+      std::string out;
+      in >> N >> c[0] >> c[1] >> range >> mc[0] >> mc[1] >> nx >> ny >> var >> out;
+      GridMap gm(lens.get(), N, c, range);
+      PixelMap<double> map = gm.writePixelMapUniform<double>(mc, nx, ny, (LensingVariable)var);
+      std::vector<double> o(nx * ny);
+      for (size_t i = 0; i < nx * ny; ++i) o[i] = map[i];
+      write_arr(out, o);
     } else if (cmd == "dropin") {
       int prec;
       in >> prec;

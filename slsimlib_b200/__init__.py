@@ -63,11 +63,11 @@ EXPORTED = [
     "glb_lens_create", "glb_lens_destroy", "glb_lens_insert_halo", "glb_lens_insert_field_plane",
     "glb_lens_nplanes", "glb_lens_planes",
     "glb_lens_reset_source", "glb_lens_rayshoot", "glb_lens_rayshoot_device", "glb_lens_rayshoot_status",
-    "glb_lens_rayshoot_device_status", "glb_gridmap", "glb_gridmap_pixelmap",
+    "glb_lens_rayshoot_device_status", "glb_gridmap", "glb_gridmap_pixelmap", "glb_gridmap_pixelmap_uniform",
     "glb_gridmap_surface_brightness", "glb_gridmap_adaptive_surface_brightness",
     "glb_lens_last_timing", "glb_lens_count_interactions", "glb_lens_rayshoot_noalloc",
     "glb_batch_create_grids", "glb_batch_run", "glb_batch_autotune", "glb_batch_set_block", "glb_batch_info",
-    "glb_batch_result", "glb_batch_destroy",
+    "glb_batch_result", "glb_batch_destroy", "glb_batch_tile", "glb_batch_set_tile",
     "glb_server_create", "glb_server_submit", "glb_server_wait", "glb_server_poll", "glb_server_stats",
     "glb_server_destroy", "glb_server_admission",
     "glb_particles_smoothing", "glb_particles_smoothing_device",
@@ -126,6 +126,8 @@ def load_library():
     L.glb_lens_rayshoot_device_status.argtypes = [_vp, C.c_size_t, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int, _vp]
     L.glb_gridmap.argtypes = [_vp, C.c_size_t, _vp, C.c_double, _vp, _vp, C.c_int]
     L.glb_gridmap_pixelmap.argtypes = [_vp, C.c_size_t, _vp, C.c_double, C.c_int, _vp, C.c_int]
+    L.glb_gridmap_pixelmap_uniform.argtypes = [_vp, C.c_size_t, _vp, C.c_double, _vp, C.c_size_t, C.c_size_t,
+                                               C.c_int, _vp, C.c_int]
     L.glb_gridmap_surface_brightness.argtypes = [_vp, C.c_size_t, _vp, C.c_double, C.c_int, _vp, _vp,
                                                  C.POINTER(C.c_double), C.c_int]
     L.glb_gridmap_adaptive_surface_brightness.argtypes = [_vp, C.c_size_t, _vp, C.c_double, C.c_int, _vp, _vp,
@@ -137,6 +139,8 @@ def load_library():
     L.glb_batch_run.argtypes = [_vp, C.c_int]
     L.glb_batch_autotune.argtypes = [_vp, C.POINTER(C.c_int), C.POINTER(C.c_double)]
     L.glb_batch_set_block.argtypes = [_vp, C.c_int]
+    L.glb_batch_tile.argtypes = [_vp, C.POINTER(C.c_int)]
+    L.glb_batch_set_tile.argtypes = [_vp, C.c_int]
     L.glb_batch_info.argtypes = [_vp, C.POINTER(C.c_size_t), C.POINTER(C.c_double), C.POINTER(C.c_int)]
     L.glb_batch_result.argtypes = [_vp, C.c_int, _vp, _vp]
     L.glb_batch_destroy.argtypes = [_vp]
@@ -524,6 +528,20 @@ def writePixelMap(lens: Lens, N1d: int, center: Sequence[float], range_: float, 
     return out.reshape(int(N1d), int(N1d))
 
 
+def writePixelMapUniform(lens: Lens, N1d: int, center: Sequence[float], range_: float, map_center: Sequence[float],
+                         Nx: int, Ny: int, lensvar: int, precision=PREC_FP64) -> np.ndarray:
+    """GridMap(lens, N1d, center, range).writePixelMapUniform(map_center, Nx, Ny,
+    lensvar) (include/gridmap.h:98-102,506-690) computed on the GPU: an
+    (Ny, Nx) map of pixel side range / (Nx - 1); grid points write their value
+    into the pixel containing them (the largest grid index where several do)."""
+    c = np.ascontiguousarray(center, dtype=np.float64)
+    mc = np.ascontiguousarray(map_center, dtype=np.float64)
+    out = np.zeros(int(Nx) * int(Ny))
+    _check(load_library().glb_gridmap_pixelmap_uniform(lens._h, int(N1d), _p(c), float(range_), _p(mc), int(Nx),
+                                                       int(Ny), int(lensvar), _p(out), precision))
+    return out.reshape(int(Ny), int(Nx))
+
+
 SOURCE_UNIFORM, SOURCE_GAUSSIAN, SOURCE_SERSIC = 0, 1, 2
 
 
@@ -593,6 +611,15 @@ class GridBatch:
 
     def set_block(self, block: int):
         _check(load_library().glb_batch_set_block(self._h, block))
+
+    def tile(self) -> int:
+        """Width in rays of the warp tile (8, 16, 32; height 32 / width)."""
+        w = C.c_int(0)
+        _check(load_library().glb_batch_tile(self._h, C.byref(w)))
+        return w.value
+
+    def set_tile(self, width: int):
+        _check(load_library().glb_batch_set_tile(self._h, width))
 
     def info(self):
         n, ms, b = C.c_size_t(0), C.c_double(0), C.c_int(0)

@@ -36,57 +36,81 @@ struct LensDev {
 
 struct Chunk {
   int lens;
-  int kind;   // 0: grid tile of 8 x 4 rays, 1: ray list
+  int kind;   // 0: grid tile of 32 rays (2^lanes wide), 1: ray list
   int n1d;    // grid side
-  int lanes;  // list: rays in this chunk (<= 32)
+  int lanes;  // list: rays in this chunk (<= 32); grid tile: log2 of its width (3, 4 or 5)
   int a, b;   // grid: tile origin (ix0, iy0); list: first sorted ray
   long long out;  // grid: output offset of the lens's grid
   double c0, c1, range;
   double zs;  // source redshift; < 0 for the lens's own source plane
 };
 
+// Shared memory of k_batch, per thread: the recursion state (theta,
+// SumPrevAlphas, A, SumPrevAG: 12 doubles) and the plane's summed forces (5)
+// at [c * blockDim + t], and one particle halo's walk totals (5 contiguous
+// doubles at 5 t, a stride that puts a half-warp's 64-bit accesses on
+// distinct banks).  Keeping them out of registers leaves the tree walk the
+// registers it needs.
+constexpr int kBatchSmemDoubles = 22;
+inline size_t batch_smem_bytes(int block) { return (size_t)kBatchSmemDoubles * block * sizeof(double); }
+
 // LensPlaneSingular::force for one plane (planes.cpp:114-161): the plane's
-// halos summed into out = {alpha0, alpha1, kappa, gamma0, gamma1}.
+// halos summed into f[c * stride] = {alpha0, alpha1, kappa, gamma0, gamma1};
+// h[0..4] receives one particle halo's walk totals.
 template <int PREC>
 __device__ __forceinline__ void plane_force(const PlaneDev &P, const HaloDev *halos, const NFWTables *tab,
-                                            double xx0, double xx1, bool valid, double *out) {
-  for (int h = 0; h < P.nhalo; ++h) {
-    const HaloDev *H = halos + P.halo0 + h;
+                                            double xx0, double xx1, bool valid, double *f, double *h,
+                                            int stride) {
+  for (int c = 0; c < 5; ++c) f[c * stride] = 0.0;
+  for (int k = 0; k < P.nhalo; ++k) {
+    const HaloDev *H = halos + P.halo0 + k;
     const double xc0 = xx0 - H->px, xc1 = xx1 - H->py;
-    double acc[6] = {0, 0, 0, 0, 0, 0};
+    double a[5];
     if (H->kind == HALO_PARTICLES) {
-      particle_halo_acc<PREC, false>(H->tree, xc0, xc1, valid, acc);
-      acc[0] = -acc[0];
-      acc[1] = -acc[1];
+      for (int c = 0; c < 5; ++c) h[c] = 0.0;
+      particle_halo_acc<PREC, false>(H->tree, xc0, xc1, valid, h);
+      // force_halo negates the walk's alpha (particle_halo.h:432-433)
+      a[0] = -h[0];
+      a[1] = -h[1];
+      a[2] = h[2];
+      a[3] = h[3];
+      a[4] = h[4];
     } else if (H->kind == HALO_FIELD) {
-      const Force6 f = field_plane_force<false>(&H->htree, tab, xc0, xc1, valid);
-      acc[0] = -f.a0;
-      acc[1] = -f.a1;
-      acc[2] = f.k;
-      acc[3] = f.g0;
-      acc[4] = f.g1;
+      const Force6 g = field_plane_force<false>(&H->htree, tab, xc0, xc1, valid);
+      a[0] = -g.a0;
+      a[1] = -g.a1;
+      a[2] = g.k;
+      a[3] = g.g0;
+      a[4] = g.g1;
     } else if (valid) {
-      const Force5 f = analytic_halo(H, tab, xc0, xc1);
-      acc[0] = f.a0;
-      acc[1] = f.a1;
-      acc[2] = f.k;
-      acc[3] = f.g0;
-      acc[4] = f.g1;
+      const Force5 g = analytic_halo(H, tab, xc0, xc1);
+      a[0] = g.a0;
+      a[1] = g.a1;
+      a[2] = g.k;
+      a[3] = g.g0;
+      a[4] = g.g1;
+    } else {
+      continue;
     }
-    out[0] -= acc[0];
-    out[1] -= acc[1];
-    out[2] += acc[2];
-    out[3] += acc[3];
-    out[4] += acc[4];
+    f[0] -= a[0];
+    f[stride] -= a[1];
+    f[2 * stride] += a[2];
+    f[3 * stride] += a[3];
+    f[4 * stride] += a[4];
   }
 }
-
 template <int PREC>
-// capped at 80 registers (3 blocks of 256 per SM) for occupancy (64 registers measured slower here)
+// capped at 80 registers (3 blocks of 256 per SM) for occupancy (64 registers measured slower here);
+// dynamic shared memory: batch_smem_bytes(blockDim.x)
 __global__ void __launch_bounds__(256, 3) k_batch(const Chunk *chunks, int nchunks, const LensDev *lenses,
                                                NFWTables tab, const double *xs, const unsigned *outidx,
                                                double *y, double *A, int *counter) {
+  extern __shared__ double bsm[];
   const int lane = threadIdx.x & 31;
+  const int B = blockDim.x;
+  double *st = bsm + threadIdx.x;          // st[c * B], c = 0..11
+  double *f = bsm + 12 * B + threadIdx.x;  // f[c * B], c = 0..4
+  double *h = bsm + 17 * B + 5 * threadIdx.x;  // h[0..4]
   for (;;) {
     int c = 0;
     if (lane == 0) c = atomicAdd(counter, 1);
@@ -98,7 +122,7 @@ __global__ void __launch_bounds__(256, 3) k_batch(const Chunk *chunks, int nchun
     double t0 = 0, t1 = 0;
     long long oi = 0;
     if (ch.kind == 0) {
-      const int ix = ch.a + (lane & 7), iy = ch.b + (lane >> 3);
+      const int ix = ch.a + (lane & ((1 << ch.lanes) - 1)), iy = ch.b + (lane >> ch.lanes);
       valid = ix < ch.n1d && iy < ch.n1d;
       if (valid) {
         const long long idx = (long long)ix + (long long)iy * ch.n1d;
@@ -128,42 +152,59 @@ __global__ void __launch_bounds__(256, 3) k_batch(const Chunk *chunks, int nchun
     }
     int jw = valid ? jmax : 0;
     for (int o = 16; o > 0; o >>= 1) jw = max(jw, __shfl_xor_sync(kFull, jw, o));
-    double sa0 = t0, sa1 = t1;
-    double A0 = 1, A1 = 0, A2 = 0, A3 = 1, s0 = 1, s1 = 0, s2 = 0, s3 = 1;
+    st[0] = t0;
+    st[B] = t1;
+    st[2 * B] = t0;
+    st[3 * B] = t1;
+    st[4 * B] = 1;
+    st[5 * B] = 0;
+    st[6 * B] = 0;
+    st[7 * B] = 1;
+    st[8 * B] = 1;
+    st[9 * B] = 0;
+    st[10 * B] = 0;
+    st[11 * B] = 1;
     for (int j = 0; j < jw; ++j) {
       const bool v = valid && j < jmax;
-      const PlaneDev P = L.planes[j];
-      double f[5] = {0, 0, 0, 0, 0};
-      plane_force<PREC>(P, L.halos, &tab, t0 * P.Dphys, t1 * P.Dphys, v, f);
+      {
+        const PlaneDev &P = L.planes[j];
+        plane_force<PREC>(P, L.halos, &tab, st[0] * P.Dphys, st[B] * P.Dphys, v, f, h, B);
+      }
       if (v) {
-        // include/lens.h:1027-1066
-        double G0 = (f[2] + f[3]) * P.Gfac, G1 = f[4] * P.Gfac, G2 = f[4] * P.Gfac, G3 = (f[2] - f[3]) * P.Gfac;
-        sa0 -= L.charge * f[0];
-        sa1 -= L.charge * f[1];
+        // include/lens.h:1027-1066, the state reloaded from shared memory
+        const PlaneDev &P = L.planes[j];
+        const double G0 = (f[2 * B] + f[3 * B]) * P.Gfac, G1 = f[4 * B] * P.Gfac, G2 = G1,
+                     G3 = (f[2 * B] - f[3 * B]) * P.Gfac;
+        const double sa0 = st[2 * B] - L.charge * f[0], sa1 = st[3 * B] - L.charge * f[B];
         double aa = P.aa, bb = P.bb;
         if (j >= jmax - 1) {
           aa = dls;
           bb = dds;
         }
-        t0 = bb * t0 + aa * sa0;
-        t1 = bb * t1 + aa * sa1;
-        s0 -= G0 * A0 + G1 * A2;
-        s1 -= G0 * A1 + G1 * A3;
-        s2 -= G2 * A0 + G3 * A2;
-        s3 -= G2 * A1 + G3 * A3;
-        A0 = A0 * bb + s0 * aa;
-        A1 = A1 * bb + s1 * aa;
-        A2 = A2 * bb + s2 * aa;
-        A3 = A3 * bb + s3 * aa;
+        st[0] = bb * st[0] + aa * sa0;
+        st[B] = bb * st[B] + aa * sa1;
+        st[2 * B] = sa0;
+        st[3 * B] = sa1;
+        const double A0 = st[4 * B], A1 = st[5 * B], A2 = st[6 * B], A3 = st[7 * B];
+        const double s0 = st[8 * B] - (G0 * A0 + G1 * A2), s1 = st[9 * B] - (G0 * A1 + G1 * A3);
+        const double s2 = st[10 * B] - (G2 * A0 + G3 * A2), s3 = st[11 * B] - (G2 * A1 + G3 * A3);
+        st[8 * B] = s0;
+        st[9 * B] = s1;
+        st[10 * B] = s2;
+        st[11 * B] = s3;
+        st[4 * B] = A0 * bb + s0 * aa;
+        st[5 * B] = A1 * bb + s1 * aa;
+        st[6 * B] = A2 * bb + s2 * aa;
+        st[7 * B] = A3 * bb + s3 * aa;
       }
     }
     if (valid) {
-      y[2 * oi] = t0;
-      y[2 * oi + 1] = t1;
-      A[4 * oi] = A0;
-      A[4 * oi + 1] = A1;
-      A[4 * oi + 2] = A2;
-      A[4 * oi + 3] = A3;
+      y[2 * oi] = st[0];
+      y[2 * oi + 1] = st[B];
+      A[4 * oi] = st[4 * B];
+      A[4 * oi + 1] = st[5 * B];
+      A[4 * oi + 2] = st[6 * B];
+      A[4 * oi + 3] = st[7 * B];
     }
   }
 }
@@ -211,9 +252,11 @@ int persistent_grid(int block, int precision, int *grid) {
   CKR(cudaGetDevice(&dev));
   CKR(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   if (precision == GLB_PREC_SPLIT)
-    CKR(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<GLB_PREC_SPLIT>, block, 0));
+    CKR(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<GLB_PREC_SPLIT>, block,
+                                                      batch_smem_bytes(block)));
   else
-    CKR(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<GLB_PREC_FP64>, block, 0));
+    CKR(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<GLB_PREC_FP64>, block,
+                                                      batch_smem_bytes(block)));
   *grid = sms * std::max(per_sm, 1);
   return 0;
 }
@@ -228,6 +271,8 @@ struct glb_batch {
   int block = 128, grid = 0;
   std::vector<glb_lens *> lenses;
   std::vector<size_t> n1d, offset;
+  std::vector<double> centers, ranges;
+  int tile_log2w = 3;  // grid tiles of 8 x 4 rays (autotuned: 8 x 4, 16 x 2, 32 x 1)
   size_t total = 0;
   DBuf<LensDev> d_lenses;
   DBuf<Chunk> d_chunks;
@@ -242,14 +287,57 @@ struct glb_batch {
 };
 
 namespace {
+// The chunk list of the batch's grids: tiles of 2^log2w x 32 / 2^log2w rays,
+// the largest grids first (uneven lenses finish together).
+int batch_chunks(glb_batch *b, int log2w) {
+  std::vector<Chunk> C;
+  const int tw = 1 << log2w, th = 32 / tw;
+  for (size_t i = 0; i < b->lenses.size(); ++i) {
+    const int N = (int)b->n1d[i];
+    for (int iy = 0; iy < N; iy += th)
+      for (int ix = 0; ix < N; ix += tw) {
+        Chunk c;
+        memset(&c, 0, sizeof(c));
+        c.lens = (int)i;
+        c.kind = 0;
+        c.n1d = N;
+        c.lanes = log2w;
+        c.a = ix;
+        c.b = iy;
+        c.out = (long long)b->offset[i];
+        c.c0 = b->centers[2 * i];
+        c.c1 = b->centers[2 * i + 1];
+        c.range = b->ranges[i];
+        c.zs = -1;
+        C.push_back(c);
+      }
+  }
+  if (C.size() > 0x7fffffffull) return fail(GLB_ERR_ARG, "too many chunks");
+  std::stable_sort(C.begin(), C.end(), [&](const Chunk &x, const Chunk &y) { return x.n1d > y.n1d; });
+  if (b->d_chunks.n < C.size()) CKR(b->d_chunks.alloc(C.size()));
+  CKR(cudaMemcpy(b->d_chunks.p, C.data(), C.size() * sizeof(Chunk), cudaMemcpyHostToDevice));
+  b->nchunks = (int)C.size();
+  b->tile_log2w = log2w;
+  return 0;
+}
+
+void drop_graph(glb_batch *b) {
+  if (b->exec) {
+    cudaGraphExecDestroy(b->exec);
+    cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+  }
+}
+
 int batch_enqueue(glb_batch *b) {
   (void)cudaGetLastError();  // launch errors below are this launch's own
   CKR(cudaMemsetAsync(b->counter.p, 0, sizeof(int), b->stream));
   if (b->precision == GLB_PREC_SPLIT)
-    k_batch<GLB_PREC_SPLIT><<<b->grid, b->block, 0, b->stream>>>(b->d_chunks.p, b->nchunks, b->d_lenses.p, b->tab,
+    k_batch<GLB_PREC_SPLIT><<<b->grid, b->block, batch_smem_bytes(b->block), b->stream>>>(b->d_chunks.p, b->nchunks, b->d_lenses.p, b->tab,
                                                                  nullptr, nullptr, b->y.p, b->A.p, b->counter.p);
   else
-    k_batch<GLB_PREC_FP64><<<b->grid, b->block, 0, b->stream>>>(b->d_chunks.p, b->nchunks, b->d_lenses.p, b->tab,
+    k_batch<GLB_PREC_FP64><<<b->grid, b->block, batch_smem_bytes(b->block), b->stream>>>(b->d_chunks.p, b->nchunks, b->d_lenses.p, b->tab,
                                                                 nullptr, nullptr, b->y.p, b->A.p, b->counter.p);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess)
@@ -273,7 +361,6 @@ int glb_batch_create_grids(glb_lens *const *lenses, int nlens, const size_t *n1d
   CKR(cudaEventCreate(&b->e1));
   b->precision = precision;
   std::vector<LensDev> L(nlens);
-  std::vector<Chunk> C;
   for (int i = 0; i < nlens; ++i) {
     if (!lenses[i]) return fail(GLB_ERR_ARG, "null lens");
     if (lenses[i]->device != b->device) return fail(GLB_ERR_ARG, "all lenses of a batch must be on one device");
@@ -283,36 +370,17 @@ int glb_batch_create_grids(glb_lens *const *lenses, int nlens, const size_t *n1d
     b->lenses.push_back(lenses[i]);
     b->n1d.push_back(n1d[i]);
     b->offset.push_back(b->total);
-    int N = (int)n1d[i];
-    for (int iy = 0; iy < N; iy += 4)
-      for (int ix = 0; ix < N; ix += 8) {
-        Chunk c;
-        memset(&c, 0, sizeof(c));
-        c.lens = i;
-        c.kind = 0;
-        c.n1d = N;
-        c.a = ix;
-        c.b = iy;
-        c.out = (long long)b->total;
-        c.c0 = centers[2 * i];
-        c.c1 = centers[2 * i + 1];
-        c.range = ranges[i];
-        c.zs = -1;
-        C.push_back(c);
-      }
-    b->total += (size_t)N * N;
+    b->centers.push_back(centers[2 * i]);
+    b->centers.push_back(centers[2 * i + 1]);
+    b->ranges.push_back(ranges[i]);
+    b->total += n1d[i] * n1d[i];
   }
-  if (C.size() > 0x7fffffffull) return fail(GLB_ERR_ARG, "too many chunks");
-  // the largest lenses' chunks first: uneven lenses finish together
-  std::stable_sort(C.begin(), C.end(), [&](const Chunk &x, const Chunk &y) { return x.n1d > y.n1d; });
-  b->nchunks = (int)C.size();
   CKR(b->d_lenses.alloc(nlens));
-  CKR(b->d_chunks.alloc(C.size()));
   CKR(b->y.alloc(2 * b->total));
   CKR(b->A.alloc(4 * b->total));
   CKR(b->counter.alloc(1));
   CKR(cudaMemcpy(b->d_lenses.p, L.data(), nlens * sizeof(LensDev), cudaMemcpyHostToDevice));
-  CKR(cudaMemcpy(b->d_chunks.p, C.data(), C.size() * sizeof(Chunk), cudaMemcpyHostToDevice));
+  if (int rc = batch_chunks(b.get(), 3)) return rc;
   if (int rc = device_nfw_tables(b->tab)) return rc;
   if (int rc = persistent_grid(b->block, precision, &b->grid)) return rc;
   *out = b.release();
@@ -344,22 +412,32 @@ int glb_batch_run(glb_batch *b, int use_graph) {
   return 0;
 }
 
-// Project autotuner: times the candidate block sizes (each with its persistent
-// grid) and keeps the fastest.  The graph is rebuilt on the next graph run.
+// Project autotuner, one dimension at a time: the block size (64, 128, 256
+// threads, each with its persistent grid) at the current tile, then the warp
+// tile (8 x 4, 16 x 2, 32 x 1 rays: the shape of the 32 neighbouring rays a
+// warp walks together) at that block size; each candidate timed twice, the
+// fastest kept.  The walk keeps no node stack (preorder array with skip
+// links), so there is no stack depth to tune.  The graph is rebuilt on the
+// next graph run.
 int glb_batch_autotune(glb_batch *b, int *best_block, double *best_ms) {
   if (!b) return fail(GLB_ERR_ARG, "null batch");
   if (int rc = set_dev(b->device)) return rc;
-  const int cands[3] = {64, 128, 256};
-  double best = 1e300;
-  int bb = b->block, bg = b->grid;
-  for (int c : cands) {
-    b->block = c;
-    if (int rc = persistent_grid(c, b->precision, &b->grid)) return rc;
-    double t = 1e300;
+  drop_graph(b);
+  auto time_it = [&](double *t) -> int {
+    *t = 1e300;
     for (int rep = 0; rep < 2; ++rep) {
       if (int rc = glb_batch_run(b, 0)) return rc;
-      t = std::min(t, (double)b->last_ms);
+      *t = std::min(*t, (double)b->last_ms);
     }
+    return 0;
+  };
+  double best = 1e300;
+  int bb = b->block, bg = b->grid;
+  for (int c : {64, 128, 256}) {
+    b->block = c;
+    if (int rc = persistent_grid(c, b->precision, &b->grid)) return rc;
+    double t;
+    if (int rc = time_it(&t)) return rc;
     if (t < best) {
       best = t;
       bb = c;
@@ -368,15 +446,35 @@ int glb_batch_autotune(glb_batch *b, int *best_block, double *best_ms) {
   }
   b->block = bb;
   b->grid = bg;
-  if (b->exec) {
-    cudaGraphExecDestroy(b->exec);
-    cudaGraphDestroy(b->graph);
-    b->exec = nullptr;
-    b->graph = nullptr;
+  int bt = b->tile_log2w;
+  for (int w : {3, 4, 5}) {
+    if (w == bt) continue;
+    if (int rc = batch_chunks(b, w)) return rc;
+    double t;
+    if (int rc = time_it(&t)) return rc;
+    if (t < best) {
+      best = t;
+      bt = w;
+    }
   }
+  if (int rc = batch_chunks(b, bt)) return rc;
   if (best_block) *best_block = bb;
   if (best_ms) *best_ms = best;
   return 0;
+}
+
+int glb_batch_tile(glb_batch *b, int *tile_width) {
+  if (!b || !tile_width) return fail(GLB_ERR_ARG, "null argument");
+  *tile_width = 1 << b->tile_log2w;
+  return 0;
+}
+
+int glb_batch_set_tile(glb_batch *b, int tile_width) {
+  if (!b || (tile_width != 8 && tile_width != 16 && tile_width != 32))
+    return fail(GLB_ERR_ARG, "tile width must be 8, 16 or 32");
+  if (int rc = set_dev(b->device)) return rc;
+  drop_graph(b);
+  return batch_chunks(b, tile_width == 8 ? 3 : tile_width == 16 ? 4 : 5);
 }
 
 int glb_batch_set_block(glb_batch *b, int block) {
@@ -384,12 +482,7 @@ int glb_batch_set_block(glb_batch *b, int block) {
   if (int rc = set_dev(b->device)) return rc;
   b->block = block;
   if (int rc = persistent_grid(block, b->precision, &b->grid)) return rc;
-  if (b->exec) {
-    cudaGraphExecDestroy(b->exec);
-    cudaGraphDestroy(b->graph);
-    b->exec = nullptr;
-    b->graph = nullptr;
-  }
+  drop_graph(b);
   return 0;
 }
 
@@ -600,10 +693,10 @@ int launch_slot(glb_server *S, Slot &sl) {
   CKR(cudaMemcpyAsync(dch, C.data(), C.size() * sizeof(Chunk), cudaMemcpyHostToDevice, s));
   CKR(cudaMemsetAsync(counter, 0, sizeof(int), s));
   if (S->precision == GLB_PREC_SPLIT)
-    k_batch<GLB_PREC_SPLIT><<<S->grid, 128, 0, s>>>(dch, (int)C.size(), S->d_lenses.p, S->tab, dxs, perm, dy, dA,
+    k_batch<GLB_PREC_SPLIT><<<S->grid, 128, batch_smem_bytes(128), s>>>(dch, (int)C.size(), S->d_lenses.p, S->tab, dxs, perm, dy, dA,
                                                     counter);
   else
-    k_batch<GLB_PREC_FP64><<<S->grid, 128, 0, s>>>(dch, (int)C.size(), S->d_lenses.p, S->tab, dxs, perm, dy, dA,
+    k_batch<GLB_PREC_FP64><<<S->grid, 128, batch_smem_bytes(128), s>>>(dch, (int)C.size(), S->d_lenses.p, S->tab, dxs, perm, dy, dA,
                                                    counter);
   CKR(cudaGetLastError());
   CKR(cudaMemcpyAsync(sl.hy, dy, 2 * n * sizeof(double), cudaMemcpyDeviceToHost, s));

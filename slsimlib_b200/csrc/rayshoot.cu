@@ -785,9 +785,7 @@ __global__ void __launch_bounds__(256) k_direct_sum(const glb_particle_rec *p, s
 // 4 KAPPA = 1 - (a0 + a3)/2, 5 GAMMA = |(gamma1, gamma2)|, 6 GAMMA1 = (a0 - a3)/2,
 // 7 GAMMA2 = (a1 + a2)/2, 8 GAMMA3 = (a2 - a1)/2, 9 INVMAG = a0 a3 - a1 a2
 // (include/point.h:377-381, 446-448).
-__global__ void k_pixelmap(const double *x, const double *y, const double *A, size_t n, int var, double *map) {
-  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
+__device__ inline double lensing_value(const double *x, const double *y, const double *A, size_t i, int var) {
   const double a0 = A[4 * i], a1 = A[4 * i + 1], a2 = A[4 * i + 2], a3 = A[4 * i + 3];
   const double d0 = x[2 * i] - y[2 * i], d1 = x[2 * i + 1] - y[2 * i + 1];
   double v = 0;
@@ -807,7 +805,42 @@ __global__ void k_pixelmap(const double *x, const double *y, const double *A, si
     case 9: v = a0 * a3 - a1 * a2; break;
     default: v = 0; break;  // DELAYT: dt = 0
   }
-  map[i] = v;
+  return v;
+}
+
+__global__ void k_pixelmap(const double *x, const double *y, const double *A, size_t n, int var, double *map) {
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  map[i] = lensing_value(x, y, A, i, var);
+}
+
+// GridMap::writePixelMapUniform (include/gridmap.h:506-690): every grid point
+// writes its value into the pixel PixelMap::find_index gives for its image
+// position (ImageProcessing/pixelmap.cpp: the map's lower corner
+// p1 = center - N res / 2, ix = (long)((x - p1) / res), -1 outside).  Where
+// several grid points share a pixel the reference keeps the last one written;
+// here that is the largest grid index (the order of one thread).
+struct UniformMap {
+  double p10, p11, res;
+  long long nx, ny;
+};
+__device__ inline long long uniform_pixel(const UniformMap &M, double x0, double x1) {
+  const long long ix = (long long)((x0 - M.p10) / M.res), iy = (long long)((x1 - M.p11) / M.res);
+  if (ix < 0 || ix >= M.nx || iy < 0 || iy >= M.ny) return -1;
+  return ix + M.nx * iy;
+}
+__global__ void k_uniform_owner(const double *x, size_t n, UniformMap M, long long *owner) {
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const long long p = uniform_pixel(M, x[2 * i], x[2 * i + 1]);
+  if (p >= 0) atomicMax(owner + p, (long long)i);
+}
+__global__ void k_uniform_write(const double *x, const double *y, const double *A, size_t n, int var, UniformMap M,
+                                const long long *owner, double *map) {
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const long long p = uniform_pixel(M, x[2 * i], x[2 * i + 1]);
+  if (p >= 0 && owner[p] == (long long)i) map[p] = lensing_value(x, y, A, i, var);
 }
 
 // Source::SurfaceBrightness at the source-plane positions y:
@@ -1868,6 +1901,47 @@ static int make_source_dev(int source_kind, const double *source_params, SourceD
   } else {
     return fail(GLB_ERR_UNSUPPORTED, "source kind outside this library (0 uniform, 1 Gaussian, 2 Sersic)");
   }
+  return 0;
+}
+
+int glb_gridmap_pixelmap_uniform(glb_lens *l, size_t n1d, const double *center, double range,
+                                 const double *map_center, size_t nx, size_t ny, int lensvar, double *map,
+                                 int precision) {
+  if (!l || !center || !map_center || !map) return fail(GLB_ERR_ARG, "null argument");
+  if (n1d < 1) return fail(GLB_ERR_ARG, "GridMap size is < 1!");  // gridmap.cpp:102
+  if (range <= 0) return fail(GLB_ERR_ARG, "GridMap range is <= 0!");
+  if (nx < 2 || ny < 1) return fail(GLB_ERR_ARG, "the uniform map needs nx >= 2 (resolution range / (nx - 1)) and ny >= 1");
+  if (precision != GLB_PREC_FP64 && precision != GLB_PREC_SPLIT) return fail(GLB_ERR_ARG, "unknown precision");
+  if (lensvar == 10 || lensvar == 11)  // PHI throws (gridmap.h:640-690); a new grid has no surface brightness
+    return fail(GLB_ERR_UNSUPPORTED, "GridMap::writePixelMapUniform() does not work for the input LensingVariable");
+  if (lensvar < 0 || lensvar > 11) return fail(GLB_ERR_ARG, "unknown LensingVariable");
+  if (int rc = set_dev(l->device)) return rc;
+  LensWS *w;
+  if (int rc = thread_ws(l, &w)) return rc;
+  const size_t n = n1d * n1d, nm = nx * ny;
+  UniformMap M;
+  M.res = range / (double)(nx - 1);  // x_range / (Nx - 1), gridmap.h:514
+  M.p10 = map_center[0] - ((double)nx * M.res) / 2.;
+  M.p11 = map_center[1] - ((double)ny * M.res) / 2.;
+  M.nx = (long long)nx;
+  M.ny = (long long)ny;
+  DBuf<double> dx, dy, dA, dm;
+  DBuf<long long> own;
+  CKR(dx.alloc(2 * n));
+  CKR(dy.alloc(2 * n));
+  CKR(dA.alloc(4 * n));
+  CKR(dm.alloc(nm));
+  CKR(own.alloc(nm));
+  k_grid<<<nblk(n, 256), 256, 0, w->stream>>>(n1d, center[0], center[1], range, dx.p);
+  CKR(cudaGetLastError());
+  if (int rc = rayshoot_device(l, w, n, dx.p, nullptr, dy.p, dA.p, precision, w->stream)) return rc;
+  CKR(cudaMemsetAsync(dm.p, 0, nm * sizeof(double), w->stream));  // PixelMap::Clean
+  CKR(cudaMemsetAsync(own.p, 0xff, nm * sizeof(long long), w->stream));  // -1: no grid point
+  k_uniform_owner<<<nblk(n, 256), 256, 0, w->stream>>>(dx.p, n, M, own.p);
+  k_uniform_write<<<nblk(n, 256), 256, 0, w->stream>>>(dx.p, dy.p, dA.p, n, lensvar, M, own.p, dm.p);
+  CKR(cudaGetLastError());
+  CKR(cudaMemcpyAsync(map, dm.p, nm * sizeof(double), cudaMemcpyDeviceToHost, w->stream));
+  CKR(cudaStreamSynchronize(w->stream));
   return 0;
 }
 

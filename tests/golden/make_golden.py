@@ -6,7 +6,7 @@ oracle/Makefile from the SLsimLib tree).  Each fixture stores its inputs and
 the reference's outputs, so tests need neither the reference tree nor the
 generator at run time.
 
-    make -C oracle && python tests/golden/make_golden.py [tree halos lens field sources adaptive smoothing]
+    make -C oracle REF=<SLsimLib> && python tests/golden/make_golden.py [tree halos lens field sources adaptive smoothing uniform]
 """
 from __future__ import annotations
 
@@ -209,6 +209,32 @@ def smoothing_fixture():
     np.savez_compressed(os.path.join(OUT, "smoothing.npz"), **arrays)
 
 
+UNIFORM_MAPS = (  # (map centre in arcsec, Nx, Ny, LensingVariable) on a 24^2 GridMap over 20 arcsec
+    ((0.0, 0.0), 24, 24, 4),      # one pixel per grid point, KAPPA
+    ((1.0, -0.5), 37, 31, 9),     # finer, offset, rectangular: INVMAG
+    ((-2.0, 1.5), 41, 29, 2),     # ALPHA1
+    ((0.5, 0.5), 33, 33, 5),      # GAMMA
+)
+
+
+def uniform_fixture():
+    """GridMap::writePixelMapUniform (include/gridmap.h:506-690) on the lens of
+    lens_small.npz; maps with at least as many pixels per side as the grid, so
+    that no two grid points share a pixel (the reference's threads leave the
+    value of a shared pixel unspecified)."""
+    spec = lens_spec_from_fixture(np.load(os.path.join(OUT, "lens_small.npz")))
+    R = H.RefDriver()
+    rng_range = 20 * synth.ARCSEC
+    arrays = {"grid_n": 24, "grid_range": rng_range}
+    for k, ((cx, cy), nx, ny, var) in enumerate(UNIFORM_MAPS):
+        of = R._file()
+        R.run(R.lens_lines(spec) + [f"uniform 24 0 0 {rng_range!r} {cx * synth.ARCSEC!r} {cy * synth.ARCSEC!r} "
+                                    f"{nx} {ny} {var} {of}"])
+        arrays[f"map{k}"] = np.fromfile(of).reshape(ny, nx)
+        arrays[f"map{k}_args"] = np.array([cx * synth.ARCSEC, cy * synth.ARCSEC, nx, ny, var])
+    np.savez_compressed(os.path.join(OUT, "uniform_maps.npz"), **arrays)
+
+
 def lens_spec_from_fixture(d) -> synth.LensSpec:
     """Rebuilds the LensSpec of lens_small.npz (insertion order as generated)."""
     halos = []
@@ -227,7 +253,8 @@ if __name__ == "__main__":
     if not H.ref_available():
         sys.exit("oracle/_ref/glamer_ref missing: run `make -C oracle` where the reference tree exists")
     fixtures = {"tree": tree_fixture, "halos": halo_fixture, "lens": lens_fixture, "field": field_fixture,
-                "sources": source_fixture, "adaptive": adaptive_fixture, "smoothing": smoothing_fixture}
+                "sources": source_fixture, "adaptive": adaptive_fixture, "smoothing": smoothing_fixture,
+                "uniform": uniform_fixture}
     for name in (sys.argv[1:] or fixtures):
         fixtures[name]()
     print("golden fixtures written to", OUT)

@@ -368,6 +368,21 @@ def error_stats(x, y, A, yref, Aref, kappa_floor=1e-3, gamma_floor=1e-3):
     return out
 
 
+def uniform_map_restated(x, values, map_center, nx, ny, rng):
+    """GridMap::writePixelMapUniform restated (include/gridmap.h:506-690;
+    PixelMap's lower corner and find_index, ImageProcessing/pixelmap.cpp): the
+    grid points in order, each writing its value into its pixel (truncation
+    toward zero), the last write kept."""
+    res = rng / (nx - 1)
+    p1 = np.array(map_center) - np.array([nx, ny]) * res / 2.0
+    out = np.zeros(nx * ny)
+    for i in range(len(x)):
+        ix, iy = int((x[i, 0] - p1[0]) / res), int((x[i, 1] - p1[1]) / res)
+        if 0 <= ix < nx and 0 <= iy < ny:
+            out[ix + nx * iy] = values[i]
+    return out.reshape(ny, nx)
+
+
 # ------------------------------------------------------- reference driver
 def ref_available() -> bool:
     return os.path.exists(REF_BIN)

