@@ -142,6 +142,15 @@ int glb_halo_set_theta(glb_halo *h, double tx, double ty);
  * glb_tree_force2D_recur; analytic halos start from zero. */
 int glb_halo_force(glb_halo *h, size_t n, const double *xcm, double *alpha, double *kappa,
                    double *gamma, double *phi);
+/* LensHalo::force_halo(alpha, kappa, gamma, phi, xcm, subtract_point, screening)
+ * (MultiPlane/lens_halos.cpp:1528-1640): with subtract_point != 0 an NFW or
+ * NSIE halo adds, inside Rmax, the point mass scaled by `screening`
+ * (force_point) -- and NFW's force_halo_sym adds the unscaled point mass once
+ * more (alpha_h + 1, gamma_h + 2, -log(r^2)/2 in phi), as the reference does
+ * -- and contributes nothing beyond Rmax.  Particle haloes and field planes
+ * take no such argument (LensHaloParticles::force_halo ignores it). */
+int glb_halo_force_ex(glb_halo *h, size_t n, const double *xcm, double *alpha, double *kappa, double *gamma,
+                      double *phi, int subtract_point, double screening);
 /* LensPlaneTree(z, halos, n, sigma_background, inv_screening_scale)
  * (MultiPlane/planes.cpp:13-18): a plane of field haloes whose force is
  * TreeQuadHalos::force2D (include/quadTreeHalos.h:556-815) -- every halo of a

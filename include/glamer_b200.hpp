@@ -146,15 +146,14 @@ class LensHalo {
 
   // LensHalo::force_halo (lens_halos.h:182-190).  Analytic haloes add to
   // alpha, kappa, gamma and phi; particle haloes overwrite them and return
-  // alpha pointing toward the mass (particle_halo.h:426-434).  The point-mass
-  // subtraction and its screening are outside this library.
+  // alpha pointing toward the mass (particle_halo.h:426-434).  subtract_point
+  // and screening as LensHalo::force_point / force_halo_sym
+  // (lens_halos.cpp:1528-1640; glb_halo_force_ex).
   virtual void force_halo(PosType *alpha, KappaType *kappa, KappaType *gamma, KappaType *phi, PosType const *xcm,
                           bool subtract_point = false, PosType screening = 1.0) {
-    if (subtract_point || screening != 1.0)
-      throw std::runtime_error("force_halo: subtract_point / screening are not supported by libglamer_b200");
     PosType a[2];
     KappaType k, g[3], p;
-    check(glb_halo_force(h_.get(), 1, xcm, a, &k, g, &p));
+    check(glb_halo_force_ex(h_.get(), 1, xcm, a, &k, g, &p, subtract_point ? 1 : 0, screening));
     if (overwrites()) {
       alpha[0] = a[0];
       alpha[1] = a[1];

@@ -12,8 +12,9 @@
  *   tree PFILE N BUCKET THETA INV_AREA MAX_RANGE PERIODIC INV_SCREEN RFILE NR OUT [EXPORT]
  *        TreeQuadParticles ctor + force2D_recur at NR rays -> OUT: per ray
  *        alpha[2] kappa gamma[3] phi.  EXPORT: 16 doubles per branch (preorder).
- *   nfw MASS RSIZE Z CONC FRATIO PA XFILE N OUT      LensHaloNFW::force_halo
- *   nsie MASS Z SIGMA RCORE FRATIO PA XFILE N OUT    LensHaloRealNSIE::force_halo
+ *   nfw MASS RSIZE Z CONC FRATIO PA XFILE N OUT [SCREEN]   LensHaloNFW::force_halo
+ *   nsie MASS Z SIGMA RCORE FRATIO PA XFILE N OUT [SCREEN] LensHaloRealNSIE::force_halo
+ *        (SCREEN given: force_halo(..., subtract_point = true, SCREEN))
  *   lens ZSOURCE                                     new Lens (replaces previous)
  *   particles PFILE N Z INV_AREA MAX_RANGE TX TY     moveinMainHalo(LensHaloParticles, true)
  *   addnfw MASS RSIZE Z CONC TX TY                   insertMainHalo(LensHaloNFW, true)
@@ -221,10 +222,13 @@ int main() {
         fix_cored_nsie_mass(*nh, mass);
         h.reset(nh);
       }
+      double screen = 1.0;
+      const bool sub = static_cast<bool>(in >> screen);
       std::vector<double> x = read_arr<double>(xf, 2 * n), o(7 * n + 3);
       for (size_t i = 0; i < n; ++i) {
         double a[2] = {0, 0}, k = 0, g[3] = {0, 0, 0}, ph = 0;
-        h->force_halo(a, &k, g, &ph, &x[2 * i]);
+        if (sub) h->force_halo(a, &k, g, &ph, &x[2 * i], true, screen);
+        else h->force_halo(a, &k, g, &ph, &x[2 * i]);
         double v[7] = {a[0], a[1], k, g[0], g[1], g[2], ph};
         std::copy(v, v + 7, &o[7 * i]);
       }

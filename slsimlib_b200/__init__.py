@@ -58,7 +58,7 @@ EXPORTED = [
     "glb_last_error", "glb_version", "glb_set_option",
     "glb_tree_create", "glb_tree_destroy", "glb_tree_force2D_recur", "glb_tree_force_device", "glb_tree_export",
     "glb_tree_build_ms", "glb_direct_sum_device",
-    "glb_halo_particles", "glb_halo_nfw", "glb_halo_nsie", "glb_halo_set_theta", "glb_halo_force",
+    "glb_halo_particles", "glb_halo_nfw", "glb_halo_nsie", "glb_halo_set_theta", "glb_halo_force", "glb_halo_force_ex",
     "glb_halo_params", "glb_halo_destroy", "glb_halo_field_plane", "glb_halo_nsie_state",
     "glb_lens_create", "glb_lens_destroy", "glb_lens_insert_halo", "glb_lens_insert_field_plane",
     "glb_lens_nplanes", "glb_lens_planes",
@@ -110,6 +110,7 @@ def load_library():
                                 C.POINTER(_vp)]
     L.glb_halo_set_theta.argtypes = [_vp, C.c_double, C.c_double]
     L.glb_halo_force.argtypes = [_vp, C.c_size_t, _vp, _vp, _vp, _vp, _vp]
+    L.glb_halo_force_ex.argtypes = [_vp, C.c_size_t, _vp, _vp, _vp, _vp, _vp, C.c_int, C.c_double]
     L.glb_halo_params.argtypes = [_vp, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)]
     L.glb_halo_destroy.argtypes = [_vp]
     L.glb_halo_field_plane.argtypes = [_vp, C.c_int, C.c_double, C.c_double, C.c_double, C.POINTER(_vp)]
@@ -252,7 +253,7 @@ class _Halo:
         _check(load_library().glb_halo_set_theta(h, self.theta[0], self.theta[1]))
         return h
 
-    def force_halo(self, xcm):
+    def force_halo(self, xcm, subtract_point=False, screening=1.0):
         """LensHalo::force_halo at positions xcm (n,2) relative to the halo
         centre, physical Mpc: alpha (n,2), kappa, gamma (n,3), phi."""
         L = load_library()
@@ -260,7 +261,8 @@ class _Halo:
         h = self._make()
         try:
             a, k, g, ph = _forces(len(x))
-            _check(L.glb_halo_force(h, len(x), _p(x), _p(a), _p(k), _p(g), _p(ph)))
+            _check(L.glb_halo_force_ex(h, len(x), _p(x), _p(a), _p(k), _p(g), _p(ph), int(bool(subtract_point)),
+                                       float(screening)))
             return a, k, g, ph
         finally:
             L.glb_halo_destroy(h)

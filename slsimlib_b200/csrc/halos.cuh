@@ -76,29 +76,53 @@ __host__ __device__ __forceinline__ void point_mass(double mass, double x0, doub
   if (PHI) out[5] += 0.5 * mass * log(rcm2) / kPi;
 }
 
-// LensHalo::force_halo -> force_point / force_halo_sym with LensHaloNFW's
-// alpha_h, kappa_h, gamma_h, phi_h (include/lens_halos.h:842-856).
+// LensHalo::force_point with subtract_point = true (lens_halos.cpp:1548-1562):
+// inside Rmax (rcm2 < Rmax^2 as floats) the point mass scaled by `screening`
+// is added (rcm2 == 0: nothing) and the halo's own terms follow; beyond Rmax
+// the halo contributes nothing.  Returns whether the own terms follow.
 template <bool PHI>
+__host__ __device__ __forceinline__ bool subtract_point_terms(double mass, double Rmax2, double x0, double x1,
+                                                              double screening, double *out) {
+  const double rcm2 = x0 * x0 + x1 * x1;
+  if (!(rcm2 < Rmax2)) return false;
+  if (rcm2 == 0) return true;
+  double fac = screening * mass / rcm2 / kPi;
+  out[0] += fac * x0;
+  out[1] += fac * x1;
+  fac = 2.0 * fac / rcm2;
+  out[3] += 0.5 * (x0 * x0 - x1 * x1) * fac;
+  out[4] += x0 * x1 * fac;
+  if (PHI) out[5] += -0.5 * mass * log(rcm2) / kPi;
+  return true;
+}
+
+// LensHalo::force_halo -> force_point / force_halo_sym with LensHaloNFW's
+// alpha_h, kappa_h, gamma_h, phi_h (include/lens_halos.h:842-856).  SUB: the
+// force_halo_sym terms of subtract_point = true (lens_halos.cpp:1620-1640:
+// alpha_h + 1, gamma_h + 2 and -log(rcm2)/2 in the potential, after
+// subtract_point_terms; nothing beyond Rmax).
+template <bool PHI, bool SUB = false>
 __device__ __forceinline__ void nfw_force(const NFWDev &d, const NFWTables &T, double x0, double x1,
                                  double *out) {
   double rcm2 = x0 * x0 + x1 * x1;
   if (!(rcm2 < d.Rmax2)) {
-    point_mass<PHI>(d.mass, x0, x1, rcm2, out);
+    if (!SUB) point_mass<PHI>(d.mass, x0, x1, rcm2, out);
     return;
   }
   if (rcm2 < 1e-20) rcm2 = 1e-20;
   double prefac = d.mass / rcm2 / kPi;
   double x = sqrt(rcm2) / d.rscale;
-  double tmp = (-1.0 * nfw_interp(T, 1, x) / d.gmax) * prefac;
+  double tmp = (-1.0 * nfw_interp(T, 1, x) / d.gmax + (SUB ? 1.0 : 0.0)) * prefac;
   out[0] += tmp * x0;
   out[1] += tmp * x1;
   out[2] += 0.5 * x * x * nfw_interp(T, 0, x) / d.gmax * prefac;
-  tmp = (-0.5 * x * x * nfw_interp(T, 2, x) / d.gmax) * prefac / rcm2;
+  tmp = (-0.5 * x * x * nfw_interp(T, 2, x) / d.gmax + (SUB ? 2.0 : 0.0)) * prefac / rcm2;
   out[3] += 0.5 * (x0 * x0 - x1 * x1) * tmp;
   out[4] += x0 * x1 * tmp;
   if (PHI) {
     double phih = 0.25 * (nfw_interp(T, 3, x) - d.h_xmax) / d.gmax + d.log_rsize;
     out[5] += phih * d.mass / kPi;
+    if (SUB) out[5] -= 0.5 * log(rcm2) * d.mass / kPi;
   }
 }
 

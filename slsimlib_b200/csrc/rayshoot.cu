@@ -685,8 +685,10 @@ __global__ void __launch_bounds__(128, 8) k_plane_step_split(const __grid_consta
 }
 
 // force2D_recur / force_halo at arbitrary positions (walk-level API, with phi).
+// subtract: LensHalo::force_halo's subtract_point = true with `screening`
+// (analytic haloes; particle trees and field planes take no such argument).
 __global__ void __launch_bounds__(128) k_halo_force(HaloDev H, NFWTables tab, size_t n, const double *x,
-                                                    double *out) {
+                                                    double *out, int subtract = 0, double screening = 1.0) {
   const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   const bool valid = k < n;
   if (!__any_sync(kFull, valid)) return;
@@ -700,6 +702,13 @@ __global__ void __launch_bounds__(128) k_halo_force(HaloDev H, NFWTables tab, si
     particle_halo_acc<GLB_PREC_FP64, true>(H.tree, x0, x1, valid, acc);
   } else if (H.kind == HALO_FIELD) {
     field_plane_acc<true>(H.htree, tab, x0, x1, valid, acc);
+  } else if (valid && subtract) {
+    if (H.kind == HALO_NFW) {
+      if (subtract_point_terms<true>(H.nfw.mass, H.nfw.Rmax2, x0, x1, screening, acc))
+        nfw_force<true, true>(H.nfw, tab, x0, x1, acc);
+    } else if (subtract_point_terms<true>(H.nsie.mass, H.nsie.Rmax2, x0, x1, screening, acc)) {
+      nsie_force<true>(H.nsie, x0, x1, acc);  // lens_halos.cpp:1938-2014 uses the flag only in force_point
+    }
   } else if (valid) {
     if (H.kind == HALO_NFW)
       nfw_force<true>(H.nfw, tab, x0, x1, acc);
@@ -1184,7 +1193,7 @@ int glb_tree_destroy(glb_tree *t) {
 }
 
 static int force_generic(const HaloDev &H, int device, cudaStream_t s, size_t n, const double *xcm, double *alpha,
-                         double *kappa, double *gamma, double *phi) {
+                         double *kappa, double *gamma, double *phi, int subtract = 0, double screening = 1.0) {
   if (n == 0) return 0;
   if (!xcm) return fail(GLB_ERR_ARG, "null positions");
   if (int rc = set_dev(device)) return rc;
@@ -1195,7 +1204,7 @@ static int force_generic(const HaloDev &H, int device, cudaStream_t s, size_t n,
   CKR(dx.alloc(2 * n));
   CKR(dout.alloc(6 * n));
   CKR(cudaMemcpyAsync(dx.p, xcm, 2 * n * sizeof(double), cudaMemcpyHostToDevice, s));
-  k_halo_force<<<nblk(n, 128), 128, 0, s>>>(H, tab, n, dx.p, dout.p);
+  k_halo_force<<<nblk(n, 128), 128, 0, s>>>(H, tab, n, dx.p, dout.p, subtract, screening);
   CKR(cudaGetLastError());
   std::vector<double> o(6 * n);
   CKR(cudaMemcpyAsync(o.data(), dout.p, 6 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -1485,6 +1494,11 @@ int glb_halo_set_theta(glb_halo *h, double tx, double ty) {
 
 int glb_halo_force(glb_halo *h, size_t n, const double *xcm, double *alpha, double *kappa, double *gamma,
                    double *phi) {
+  return glb_halo_force_ex(h, n, xcm, alpha, kappa, gamma, phi, 0, 1.0);
+}
+
+int glb_halo_force_ex(glb_halo *h, size_t n, const double *xcm, double *alpha, double *kappa, double *gamma,
+                      double *phi, int subtract_point, double screening) {
   if (!h) return fail(GLB_ERR_ARG, "null halo");
   HaloDev H = make_halo_dev(*h);
   if (h->kind == HALO_PARTICLES && h->tree->nparticles == 0) {
@@ -1496,7 +1510,7 @@ int glb_halo_force(glb_halo *h, size_t n, const double *xcm, double *alpha, doub
     }
     return 0;
   }
-  int rc = force_generic(H, h->device, h->stream, n, xcm, alpha, kappa, gamma, phi);
+  int rc = force_generic(H, h->device, h->stream, n, xcm, alpha, kappa, gamma, phi, subtract_point, screening);
   if (rc) return rc;
   if (h->kind == HALO_PARTICLES && alpha)  // LensHaloParticles::force_halo negates alpha
     for (size_t i = 0; i < 2 * n; ++i) alpha[i] = -alpha[i];

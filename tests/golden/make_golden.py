@@ -54,6 +54,22 @@ def halo_fixture():
     np.savez_compressed(os.path.join(OUT, "halos.npz"), **data)
 
 
+def halo_subtract_fixture():
+    """force_halo(..., subtract_point = true, screening) of the reference
+    (MultiPlane/lens_halos.cpp:1528-1640) for NFW and NSIE haloes, positions
+    inside and beyond Rmax."""
+    rng = np.random.default_rng(15)
+    x = rng.uniform(-1.0, 1.0, size=(64, 2)) * np.logspace(-4, 0.4, 64)[:, None]
+    R = H.RefDriver()
+    halos = {"nfw": synth.NFWHalo(1e14, 0.864, 0.3, 5.0), "nsie_sis": synth.NSIEHalo(1e13, 0.5, 250.0, 0.0, 1.0, 0.0),
+             "nsie_rot": synth.NSIEHalo(1e12, 0.5, 200.0, 0.0, 0.6, 0.3)}
+    data = {"x": x}
+    for k, h in halos.items():
+        for s in (1.0, 0.25):
+            data[f"{k}_{s}"] = R.halo_force(h, x, screening=s)[0]
+    np.savez_compressed(os.path.join(OUT, "halos_subtract.npz"), **data)
+
+
 def lens_fixture():
     spec = synth.light_cone(seed=13, n_total=6000, n_planes=3, halos_per_plane=3)
     spec.halos.append(synth.NFWHalo(3e13, 0.4, 0.7, 6.0, theta=(2e-5, -1e-5)))
@@ -254,7 +270,7 @@ if __name__ == "__main__":
         sys.exit("oracle/_ref/glamer_ref missing: run `make -C oracle` where the reference tree exists")
     fixtures = {"tree": tree_fixture, "halos": halo_fixture, "lens": lens_fixture, "field": field_fixture,
                 "sources": source_fixture, "adaptive": adaptive_fixture, "smoothing": smoothing_fixture,
-                "uniform": uniform_fixture}
+                "uniform": uniform_fixture, "subtract": halo_subtract_fixture}
     for name in (sys.argv[1:] or fixtures):
         fixtures[name]()
     print("golden fixtures written to", OUT)

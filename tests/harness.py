@@ -427,15 +427,18 @@ class RefDriver:
             return out, np.fromfile(ef).reshape(-1, 16)
         return out
 
-    def halo_force(self, h, xcm):
+    def halo_force(self, h, xcm, screening=None):
+        """force_halo of an NFW / NSIE halo; screening given: with
+        subtract_point = true and that screening."""
         xcm = np.ascontiguousarray(xcm, dtype=np.float64).reshape(-1, 2)
         xf = self._file(xcm)
         of = self._file()
+        sub = "" if screening is None else f" {float(screening)!r}"
         if isinstance(h, synth.NFWHalo):
-            cmd = f"nfw {h.mass!r} {h.rsize!r} {h.z!r} {h.conc!r} 1 0 {xf} {len(xcm)} {of}"
+            cmd = f"nfw {h.mass!r} {h.rsize!r} {h.z!r} {h.conc!r} 1 0 {xf} {len(xcm)} {of}{sub}"
         else:
             cmd = (f"nsie {h.mass!r} {h.z!r} {h.sigma!r} {h.rcore!r} {h.fratio!r} {h.pa!r} "
-                   f"{xf} {len(xcm)} {of}")
+                   f"{xf} {len(xcm)} {of}{sub}")
         self.run([cmd])
         o = np.fromfile(of)
         return o[:-3].reshape(-1, 7), tuple(o[-3:])

@@ -146,6 +146,22 @@ def test_analytic_halos_match_reference(golden):
         np.testing.assert_allclose(h.params(), d[k + "_params"], rtol=1e-6, err_msg=k)
 
 
+def test_analytic_halos_subtract_point_match_reference(golden):
+    """force_halo(..., subtract_point = true, screening) against the
+    reference's own output (golden halos_subtract.npz): the screened point
+    mass of force_point inside Rmax plus, for NFW, force_halo_sym's unscreened
+    one; nothing beyond Rmax."""
+    d = golden("halos_subtract.npz")
+    halos = {"nfw": glb.LensHaloNFW(1e14, 0.864, 0.3, 5.0),
+             "nsie_sis": glb.LensHaloRealNSIE(1e13, 0.5, 250.0, 0.0, 1.0, 0.0),
+             "nsie_rot": glb.LensHaloRealNSIE(1e12, 0.5, 200.0, 0.0, 0.6, 0.3)}
+    for k, h in halos.items():
+        for s in (1.0, 0.25):
+            f = pack(*h.force_halo(d["x"], subtract_point=True, screening=s))
+            m, cols = force_err(f, d[f"{k}_{s}"])
+            assert m < (1e-8 if k == "nfw" else RTOL64), (k, s, cols)
+
+
 def test_particle_halo_force_matches_oracle():
     rng = np.random.default_rng(6)
     p = synth.nfw_particles(rng, 5000, 1e13, 6.0, 0.5, 5e-4)
