@@ -672,6 +672,55 @@ template <int PREC, bool COUNT = false, bool FIELD = false>
 __global__ void __launch_bounds__(128) k_plane_step(StepArgs a) {
   plane_step<PREC, COUNT, FIELD>(a);
 }
+// plane_step_split_ptree for two rays per thread: slots 2g and 2g + 1 (g the
+// thread's global index; neighbours in the Morton order), walked together by
+// walk_split2.  Shared memory per thread: the two rays' FP64 totals (stride
+// 5 in two halves) and their positions on the plane.
+__device__ __forceinline__ void plane_step_split_ptree2(const StepArgs &a, double *sacc, double *sxy) {
+  const size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  const size_t k0 = 2 * g, k1 = 2 * g + 1;
+  const bool in0 = k0 < a.n, in1 = k1 < a.n;
+  const int jmax0 = (a.jmax_ray && in0) ? a.jmax_ray[k0] : a.jmax;
+  const int jmax1 = (a.jmax_ray && in1) ? a.jmax_ray[k1] : a.jmax;
+  const bool v0 = in0 && a.j < jmax0, v1 = in1 && a.j < jmax1;
+  if (!__any_sync(kFull, v0 || v1)) return;
+  double *acc0 = sacc + 5 * threadIdx.x, *acc1 = sacc + 5 * (blockDim.x + threadIdx.x);
+  double *rxy = sxy + 4 * threadIdx.x;
+  for (int c = 0; c < 5; ++c) acc0[c] = acc1[c] = 0.0;
+  const double D = a.planes[a.j].Dphys;
+  rxy[0] = v0 ? a.st[k0] * D - a.tree_px : 0.0;
+  rxy[1] = v0 ? a.st[a.n + k0] * D - a.tree_py : 0.0;
+  rxy[2] = v1 ? a.st[k1] * D - a.tree_px : 0.0;
+  rxy[3] = v1 ? a.st[a.n + k1] * D - a.tree_py : 0.0;
+  walk_split2(a.tree, rxy, v0, v1, acc0, acc1);
+  for (int r = 0; r < 2; ++r) {
+    const bool v = r ? v1 : v0;
+    if (!v) continue;
+    const size_t k = r ? k1 : k0;
+    const double *acc = r ? acc1 : acc0;
+    double al0 = acc[0], al1 = acc[1], kap = acc[2], g0 = acc[3], g1 = acc[4];
+    const PlaneDev &P = a.planes[a.j];
+    for (int h = 0; h < P.nhalo; ++h) {
+      const HaloDev *H = a.halos + P.halo0 + h;
+      if (H->kind == HALO_PARTICLES) continue;
+      const Force5 f = analytic_halo(H, &a.tab, a.st[k] * P.Dphys - H->px, a.st[a.n + k] * P.Dphys - H->py);
+      al0 -= f.a0;
+      al1 -= f.a1;
+      kap += f.k;
+      g0 += f.g0;
+      g1 += f.g1;
+    }
+    recursion_step(a, k, al0, al1, kap, g0, g1);
+  }
+}
+
+// Two rays per thread: n / 2 threads (rounded up), blocks of 128.
+__global__ void __launch_bounds__(128, 8) k_plane_step_split2(const __grid_constant__ StepArgs a) {
+  __shared__ double sacc[10 * 128];
+  __shared__ double sxy[4 * 128];
+  plane_step_split_ptree2(a, sacc, sxy);
+}
+
 // PTREE: the plane holds exactly one particle halo, whose tree is a.tree
 // (no field plane on such a launch).
 template <bool FIELD = false, bool PTREE = false>
@@ -1039,7 +1088,7 @@ int launch_plane_steps(const glb_lens *l, StepArgs &a, int jmax_launch, int prec
     else if (precision == GLB_PREC_SPLIT && fld)
       k_plane_step_split<true><<<nblk(n, 128), 128, 0, s>>>(a);
     else if (precision == GLB_PREC_SPLIT && ptree)
-      k_plane_step_split<false, true><<<nblk(n, 128), 128, 0, s>>>(a);
+      k_plane_step_split2<<<nblk((n + 1) / 2, 128), 128, 0, s>>>(a);
     else if (precision == GLB_PREC_SPLIT)
       k_plane_step_split<<<nblk(n, 128), 128, 0, s>>>(a);
     else if (fld)

@@ -355,4 +355,177 @@ __device__ __forceinline__ void walk_split(const TreeDev &T, double rx, double r
   }
 }
 
+// The split walk for two rays per lane (a warp walks 64 neighbouring rays):
+// each ray keeps its own opening decisions, offsets, partial sums and resume
+// point exactly as walk_split<false> does for one, while the node rows, the
+// warp vote, the loop control and the leaf particles are loaded and executed
+// once for both.  rxy: {rx0, ry0, rx1, ry1} (the rays' FP64 positions, read
+// only on the rare FP64 paths); acc0 / acc1: the rays' FP64 totals.
+__device__ __forceinline__ void far_term(const float4 &c1, const float4 &c2, float2 d, float r2f, bool screen,
+                                         float ns2l, float piaf, F32Acc &fa, double *acc) {
+  const float scr = screen ? ex2_approx(r2f * ns2l) : 1.0f;
+  const float ir2 = rcp_approx(r2f);
+  const float ms = c1.z * scr;
+  const float sir4 = scr * ir2 * ir2;
+  const float qx = fmaf(c2.w, d.x, c2.y * d.y), qy = fmaf(c2.x, d.y, c2.y * d.x);
+  const float qd = fmaf(qx, d.x, qy * d.y);
+  const float t = fmaf(c1.z, piaf, -ms * ir2) + 4.f * qd * sir4 * ir2;
+  fa.a = __ffma2_rn(f2(t), d, fa.a);
+  fa.a = __ffma2_rn(f2(-sir4), make_float2(qx, qy), fa.a);
+  const float2 dd = __fmul2_rn(d, d);
+  fa.g = __ffma2_rn(f2(-ms * ir2 * ir2), make_float2(dd.x - dd.y, d.x * d.y), fa.g);
+  if (++fa.cnt >= 32) fa.flush(acc);
+}
+
+__device__ __forceinline__ void leaf_term(const TreeDev &T, float4 P, int p, float2 d, const double *rxy, bool nearc,
+                                          bool screen, float s2f, float ns2l, float piaf, bool sheet, float wu,
+                                          int node, F32Acc &fa, double *acc) {
+  const float2 x = __fadd2_rn(make_float2(P.x, P.y), d);
+  const float2 xx = __fmul2_rn(x, x);
+  const float r2 = xx.x + xx.y;
+  if (r2 < P.w) {  // within two softening lengths (or coincident)
+    const float4 Q = __ldg(T.parts + p);
+    if (r2 < 1e-12f || !(Q.w < wu)) {
+      const Near64 o = near_particle_f64(Q, rxy[0], rxy[1], T.screen2, sheet ? T.inv_area : 0.0, nearc,
+                                         T.nodes[node].width);
+      acc[0] += o.a0;
+      acc[1] += o.a1;
+      acc[2] += o.k;
+      acc[3] += o.g0;
+      acc[4] += o.g1;
+      return;
+    }
+    if (nearc && r2 < 4.f * Q.w * Q.w) {
+      softened_f32(x, r2, Q.z, Q.w, s2f, fa);
+      if (sheet) fa.a = __ffma2_rn(f2(-piaf * P.z), x, fa.a);
+      return;
+    }
+  }
+  const float scr = screen ? ex2_approx(r2 * ns2l) : 1.0f;
+  const float ir2 = rcp_approx(r2);
+  const float npre = P.z * scr * ir2;
+  fa.a = __ffma2_rn(f2(npre), x, fa.a);
+  fa.g = __ffma2_rn(f2(npre * ir2), make_float2(xx.x - xx.y, x.x * x.y), fa.g);
+  if (sheet) fa.a = __ffma2_rn(f2(-piaf * P.z), x, fa.a);
+}
+
+__device__ __forceinline__ void walk_split2(const TreeDev &T, const double *rxy, bool valid0, bool valid1,
+                                            double *acc0, double *acc1) {
+  const bool screen = T.screen2 != 0.0;
+  const float s2f = (float)T.screen2;
+  const float ns2l = -s2f * kLog2e;
+  const bool closed = T.sheet_closed;
+  const bool sheet = T.inv_area != 0.0 && !closed;
+  const float piaf = sheet ? (float)(kPi * T.inv_area) : 0.f;
+  float2 nrh[2], nrl[2];
+  for (int r = 0; r < 2; ++r) {
+    const double rx = rxy[2 * r], ry = rxy[2 * r + 1];
+    const float rxh = (float)rx, ryh = (float)ry;
+    nrh[r] = make_float2(-rxh, -ryh);
+    nrl[r] = make_float2(-(float)(rx - (double)rxh), -(float)(ry - (double)ryh));
+  }
+  F32Acc fa0, fa1;
+  fa0.zero();
+  fa1.zero();
+  int resume0 = valid0 ? 0 : 0x7fffffff, resume1 = valid1 ? 0 : 0x7fffffff;
+  int node = 0;
+  const int nn = T.nnodes;
+  while (node < nn) {
+    const float4 *sp = reinterpret_cast<const float4 *>(T.snodes + node);
+    const float4 c0 = __ldg(sp), c1 = __ldg(sp + 1);
+    const int4 c3 = __ldg(reinterpret_cast<const int4 *>(sp + 3));
+    const int skip = c3.x;
+    const bool act0 = node >= resume0, act1 = node >= resume1;
+    const float2 cc = make_float2(c0.x, c0.y), cl = make_float2(c0.z, c0.w);
+    const float2 d0 = __fadd2_rn(__fadd2_rn(cc, nrh[0]), __fadd2_rn(cl, nrl[0]));
+    const float2 d1 = __fadd2_rn(__fadd2_rn(cc, nrh[1]), __fadd2_rn(cl, nrl[1]));
+    const float2 dd0 = __fmul2_rn(d0, d0), dd1 = __fmul2_rn(d1, d1);
+    const float r2f0 = dd0.x + dd0.y, r2f1 = dd1.x + dd1.y;
+    bool open0 = false, open1 = false;
+    if (act0) {
+      const float e = r2f0 - c1.x;
+      open0 = e < 0.f;
+      if (fabsf(e) <= c1.w) open0 = node_test_f64(T.nodes + node, rxy[0], rxy[1], 0);
+    }
+    if (act1) {
+      const float e = r2f1 - c1.x;
+      open1 = e < 0.f;
+      if (fabsf(e) <= c1.w) open1 = node_test_f64(T.nodes + node, rxy[2], rxy[3], 0);
+    }
+    const bool far0 = act0 && !open0, far1 = act1 && !open1;
+    if (far0 || far1) {
+      const float4 c2 = __ldg(sp + 2);
+      if (far0) {
+        far_term(c1, c2, d0, r2f0, screen, ns2l, piaf, fa0, acc0);
+        resume0 = skip;
+      }
+      if (far1) {
+        far_term(c1, c2, d1, r2f1, screen, ns2l, piaf, fa1, acc1);
+        resume1 = skip;
+      }
+    }
+    if (!__any_sync(kFull, open0 || open1)) {
+      node = skip;
+      continue;
+    }
+    bool nearc0 = false, nearc1 = false;
+    if (open0) {
+      const float e = r2f0 - c1.y;
+      nearc0 = e < 0.f;
+      if (fabsf(e) <= kAmbiguous * c1.y) nearc0 = node_test_f64(T.nodes + node, rxy[0], rxy[1], 1);
+    }
+    if (open1) {
+      const float e = r2f1 - c1.y;
+      nearc1 = e < 0.f;
+      if (fabsf(e) <= kAmbiguous * c1.y) nearc1 = node_test_f64(T.nodes + node, rxy[2], rxy[3], 1);
+    }
+    if (c3.y) {  // leaf
+      const int p0 = c3.z, p1 = p0 + c3.w;
+      const float wu = __ldg(sp + 2).z;
+      if (open0 && fa0.cnt) fa0.flush(acc0);
+      if (open1 && fa1.cnt) fa1.flush(acc1);
+      for (int q0 = p0; q0 < p1; q0 += 32) {
+        const int q1 = min(q0 + 32, p1);
+        for (int p = q0; p < q1; ++p) {
+          const float4 P = __ldg(T.prel + p);
+          if (open0) leaf_term(T, P, p, d0, rxy, nearc0, screen, s2f, ns2l, piaf, sheet, wu, node, fa0, acc0);
+          if (open1) leaf_term(T, P, p, d1, rxy + 2, nearc1, screen, s2f, ns2l, piaf, sheet, wu, node, fa1, acc1);
+        }
+        if (open0) fa0.flush(acc0);
+        if (open1) fa1.flush(acc1);
+      }
+      node = skip;
+    } else {
+      if (__any_sync(kFull, nearc0 || nearc1)) {
+        const int b0 = c3.z, b1 = b0 + c3.w;
+        for (int b = b0; b < b1; ++b) {
+          const float4 P = __ldg(T.bigs + b);
+          for (int r = 0; r < 2; ++r) {
+            if (!(r ? nearc1 : nearc0)) continue;
+            const double x0 = (double)P.x - rxy[2 * r], x1 = (double)P.y - rxy[2 * r + 1];
+            double rcm2 = x0 * x0 + x1 * x1;
+            if (rcm2 < 1e-20) rcm2 = 1e-20;
+            const double size = (double)P.w;
+            if (rcm2 < 4 * size * size) bspline_f64<false>(x0, x1, sqrt(rcm2), (double)P.z, size, 0.0, r ? acc1 : acc0);
+          }
+        }
+      }
+      node = node + 1;
+    }
+  }
+  fa0.flush(acc0);
+  fa1.flush(acc1);
+  if (T.inv_area != 0.0 && nn > 0) {
+    const double s = T.inv_area * T.root_mass;
+    for (int r = 0; r < 2; ++r) {
+      double *acc = r ? acc1 : acc0;
+      acc[2] -= s;
+      if (closed) {
+        acc[0] += s * (T.root_cx - rxy[2 * r]);
+        acc[1] += s * (T.root_cy - rxy[2 * r + 1]);
+      }
+    }
+  }
+}
+
 }  // namespace glb

@@ -239,13 +239,13 @@ int main(int argc, char **argv) {
     const double ap = a[0];
     hp.force_halo(a, &k, gm3, &ph, xcm);
     REQUIRE(a[0] == ap);
-    bool threw = false;
-    try {
-      nfw.force_halo(a, &k, gm3, &ph, xcm, true);
-    } catch (const std::runtime_error &) {
-      threw = true;
-    }
-    REQUIRE(threw);
+    // subtract_point with screening (LensHalo::force_point / force_halo_sym):
+    // inside Rmax the screened and the unscreened point mass are both added
+    double as[2] = {0, 0}, ks = 0, gs[3] = {0, 0, 0}, phs = 0;
+    nfw.force_halo(as, &ks, gs, &phs, xcm, true, 0.5);
+    const double r2 = xcm[0] * xcm[0] + xcm[1] * xcm[1];
+    const double point = (double)5e13f / r2 / 3.141592653589793;  // the float mass member
+    REQUIRE(std::fabs(as[0] - (a1 + 1.5 * point * xcm[0])) <= 1e-9 * std::fabs(as[0]) && ks == k1);
   }
 
   // TreeQuadParticles: one ray at a time equals the batched call
