@@ -11,7 +11,7 @@ Lines printed by rank 0 (one JSON line):
          GPUs, inputs resident in HBM, CUDA events on the launching stream;
   e2e    the same metric through the host C ABI (glb_lens_rayshoot: host
          x in, host y and A out, copies inside the timed region);
-  roofline of the plane-step kernel (algorithmic FP32 flops from the counted
+  roofline of the plane-step kernel (k_plane_step_split2; algorithmic FP32 flops from the counted
          interactions / kernel time vs the FP32 CUDA-core peak);
   cpu_baseline: the reference compiled in place (oracle/_ref) on host cores.
 
@@ -750,7 +750,7 @@ def main():
                          "frac": achieved / peak, "traffic": DRAM_BYTES_PER_RAY_PLANE * n,
                          "traffic_note": "dram read+write bytes per plane launch: ncu capture of one 1536^2 launch "
                                          "(177 B/ray) scaled by rays",
-                         "kernel": "k_plane_step_split", "kernel_ms_per_step": k_ms,
+                         "kernel": "k_plane_step_split2", "kernel_ms_per_step": k_ms,
                          "peak_note": "FP32 CUDA-core FMA rate at the sampled SM clock (148 SMs x 128 lanes x 2)",
                          "alg_flops_per_step": alg_flops,
                          "counts": {"V": V, "F": F, "P": P, "B": B, "S": S},

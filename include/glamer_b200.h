@@ -364,12 +364,13 @@ int glb_batch_destroy(glb_batch *b);
  * max_rays_per_batch rays; a batch launches as soon as one of `nslots` slots
  * is free, so requests that arrive while others run are batched and overlap
  * on the GPU.  Admission is by device memory: at every dispatch the server
- * reads the HBM free at that moment (plus memory its stream-ordered pool
+ * reads the HBM free at that moment (plus memory its own stream-ordered pool
  * holds unused), keeps 5 % of the device free, and admits the requests whose
- * batch memory (about 170 bytes per ray) fits; a batch takes its memory when
- * it launches and gives it back when its results are copied out, so a request
- * that does not fit waits until batches in flight finish (GLB_ERR_OOM from
- * glb_server_wait if none is in flight).  A request's results do not depend
+ * batch memory (about 170 bytes per ray) fits; a batch takes its memory from
+ * the pool when it launches and gives it back when its results are copied
+ * out, so a request that does not fit waits until batches in flight finish
+ * (GLB_ERR_OOM from glb_server_wait if none is in flight).  The pool keeps
+ * what it has reserved until the server is destroyed.  A request's results do not depend
  * on what it is batched with.  The lenses must outlive the server. */
 typedef struct glb_server glb_server;
 int glb_server_create(glb_lens *const *models, int nmodels, size_t max_rays_per_batch, int precision, int nslots,

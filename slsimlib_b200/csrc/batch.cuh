@@ -593,7 +593,10 @@ struct glb_server {
   size_t cap = 0;  // rays per batch at most (max_rays_per_batch; the pinned staging of a slot)
   size_t reserve = 0;  // device bytes admission leaves free for everything else
   size_t total_bytes = 0;
-  cudaMemPool_t pool = nullptr;  // the device's default stream-ordered pool
+  // the server's own stream-ordered pool: it keeps the memory it has reserved
+  // (release threshold at its maximum), so batches reuse it instead of mapping
+  // new memory each time; admission counts what it holds unused as free
+  cudaMemPool_t pool = nullptr;
   std::vector<glb_lens *> models;
   DBuf<LensDev> d_lenses;
   NFWTables tab{};
@@ -834,7 +837,14 @@ int glb_server_create(glb_lens *const *models, int nmodels, size_t max_rays_per_
   CKR(cudaMemGetInfo(&freeb, &totb));
   S->reserve = totb / 20;  // 5 % of HBM stays free for other work
   S->total_bytes = totb;
-  CKR(cudaDeviceGetDefaultMemPool(&S->pool, S->device));
+  cudaMemPoolProps props;
+  memset(&props, 0, sizeof(props));
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = S->device;
+  CKR(cudaMemPoolCreate(&S->pool, &props));
+  unsigned long long keep = ~0ull;  // cudaMemPoolAttrReleaseThreshold is a 64-bit value
+  CKR(cudaMemPoolSetAttribute(S->pool, cudaMemPoolAttrReleaseThreshold, &keep));
   std::vector<LensDev> L(nmodels);
   for (int i = 0; i < nmodels; ++i) {
     if (!models[i] || models[i]->device != S->device) return fail(GLB_ERR_ARG, "models must be lenses on one device");
@@ -983,6 +993,7 @@ int glb_server_destroy(glb_server *S) {
     cudaEventDestroy(sl->ev);
     cudaStreamDestroy(sl->s);
   }
+  if (S->pool) cudaMemPoolDestroy(S->pool);
   delete S;
   return 0;
 }

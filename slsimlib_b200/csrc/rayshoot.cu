@@ -454,7 +454,7 @@ struct StepArgs {
   double charge;
   unsigned long long *counts;  // V F P B S Wn Wp totals (counting launches only)
   // The plane's particle tree and its offset (posHalo * Dist) when the plane
-  // holds exactly one particle halo (k_plane_step_split with PTREE): read from
+  // holds exactly one particle halo (k_plane_step_split2): read from
   // kernel parameter space, so the walk's pointers and scalars are uniform
   // operands rather than per-thread registers.
   TreeDev tree;
@@ -513,47 +513,6 @@ __device__ __forceinline__ void recursion_step(const StepArgs &a, size_t k, doub
   st[9 * n + k] = s1;
   st[10 * n + k] = s2;
   st[11 * n + k] = s3;
-}
-
-// Split-form plane step for a plane holding exactly one particle halo (its
-// tree in a.tree) and any number of analytic halos.  Only the ray slot stays
-// live across the tree walk: the walk's FP64 totals sit in shared memory
-// (sacc, five doubles per thread at a stride of five, which maps a half-warp's
-// 64-bit accesses onto distinct banks), and the recursion reloads theta, the
-// plane constants and the source-plane scalars after the walk.  The particle
-// halo's terms are added first, then the analytic halos' in insertion order.
-__device__ __forceinline__ void plane_step_split_ptree(const StepArgs &a, double *sacc) {
-  const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  const bool inrange = k < a.n;
-  const int jmax = (a.jmax_ray && inrange) ? a.jmax_ray[k] : a.jmax;
-  const bool valid = inrange && a.j < jmax;
-  if (!__any_sync(kFull, valid)) return;
-  double *acc = sacc + 5 * threadIdx.x;
-  for (int c = 0; c < 5; ++c) acc[c] = 0.0;
-  double rx = 0, ry = 0;
-  if (valid) {
-    const double D = a.planes[a.j].Dphys;
-    rx = a.st[k] * D - a.tree_px;
-    ry = a.st[a.n + k] * D - a.tree_py;
-  }
-  particle_halo_acc<GLB_PREC_SPLIT, false>(a.tree, rx, ry, valid, acc);
-  if (!valid) return;
-  // LensHaloParticles::force_halo negates alpha (particle_halo.h:432-433) and
-  // LensPlaneSingular::force subtracts it
-  double al0 = acc[0], al1 = acc[1], kap = acc[2], g0 = acc[3], g1 = acc[4];
-  const PlaneDev &P = a.planes[a.j];
-  for (int h = 0; h < P.nhalo; ++h) {
-    const HaloDev *H = a.halos + P.halo0 + h;
-    if (H->kind == HALO_PARTICLES) continue;
-    const double D = P.Dphys;
-    const Force5 f = analytic_halo(H, &a.tab, a.st[k] * D - H->px, a.st[a.n + k] * D - H->py);
-    al0 -= f.a0;
-    al1 -= f.a1;
-    kap += f.k;
-    g0 += f.g0;
-    g1 += f.g1;
-  }
-  recursion_step(a, k, al0, al1, kap, g0, g1);
 }
 
 // One lens plane for every ray: LensPlaneSingular::force + the recursion of
@@ -672,10 +631,58 @@ template <int PREC, bool COUNT = false, bool FIELD = false>
 __global__ void __launch_bounds__(128) k_plane_step(StepArgs a) {
   plane_step<PREC, COUNT, FIELD>(a);
 }
-// plane_step_split_ptree for two rays per thread: slots 2g and 2g + 1 (g the
-// thread's global index; neighbours in the Morton order), walked together by
-// walk_split2.  Shared memory per thread: the two rays' FP64 totals (stride
-// 5 in two halves) and their positions on the plane.
+// One ray per thread: the form for grids too small to fill the GPU with
+// k_plane_step_split2 (see launch_plane_steps).  A plane holding exactly one
+// particle halo (its tree in a.tree) and any number of analytic halos.  Only the ray slot stays
+// live across the tree walk: the walk's FP64 totals sit in shared memory
+// (sacc, five doubles per thread at a stride of five, which maps a half-warp's
+// 64-bit accesses onto distinct banks), and the recursion reloads theta, the
+// plane constants and the source-plane scalars after the walk.  The particle
+// halo's terms are added first, then the analytic halos' in insertion order.
+__device__ __forceinline__ void plane_step_split_ptree(const StepArgs &a, double *sacc) {
+  const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  const bool inrange = k < a.n;
+  const int jmax = (a.jmax_ray && inrange) ? a.jmax_ray[k] : a.jmax;
+  const bool valid = inrange && a.j < jmax;
+  if (!__any_sync(kFull, valid)) return;
+  double *acc = sacc + 5 * threadIdx.x;
+  for (int c = 0; c < 5; ++c) acc[c] = 0.0;
+  double rx = 0, ry = 0;
+  if (valid) {
+    const double D = a.planes[a.j].Dphys;
+    rx = a.st[k] * D - a.tree_px;
+    ry = a.st[a.n + k] * D - a.tree_py;
+  }
+  particle_halo_acc<GLB_PREC_SPLIT, false>(a.tree, rx, ry, valid, acc);
+  if (!valid) return;
+  // LensHaloParticles::force_halo negates alpha (particle_halo.h:432-433) and
+  // LensPlaneSingular::force subtracts it
+  double al0 = acc[0], al1 = acc[1], kap = acc[2], g0 = acc[3], g1 = acc[4];
+  const PlaneDev &P = a.planes[a.j];
+  for (int h = 0; h < P.nhalo; ++h) {
+    const HaloDev *H = a.halos + P.halo0 + h;
+    if (H->kind == HALO_PARTICLES) continue;
+    const double D = P.Dphys;
+    const Force5 f = analytic_halo(H, &a.tab, a.st[k] * D - H->px, a.st[a.n + k] * D - H->py);
+    al0 -= f.a0;
+    al1 -= f.a1;
+    kap += f.k;
+    g0 += f.g0;
+    g1 += f.g1;
+  }
+  recursion_step(a, k, al0, al1, kap, g0, g1);
+}
+
+// Split-form plane step for a plane holding exactly one particle halo (its
+// tree in a.tree, a kernel parameter) and any number of analytic halos, two
+// rays per thread: slots 2g and 2g + 1 (g the thread's global index;
+// neighbours in the Morton order, so a warp walks 64 neighbouring rays),
+// walked together by walk_split2.  Only the slots stay live across the walk:
+// the rays' FP64 totals (stride 5 in two halves: a half-warp's 64-bit
+// accesses on distinct banks) and their plane positions sit in shared memory,
+// and the recursion reloads theta, the plane constants and the source-plane
+// scalars after the walk.  The particle halo's terms are added first, then
+// the analytic halos' in insertion order.
 __device__ __forceinline__ void plane_step_split_ptree2(const StepArgs &a, double *sacc, double *sxy) {
   const size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   const size_t k0 = 2 * g, k1 = 2 * g + 1;
@@ -714,15 +721,19 @@ __device__ __forceinline__ void plane_step_split_ptree2(const StepArgs &a, doubl
   }
 }
 
-// Two rays per thread: n / 2 threads (rounded up), blocks of 128.
-__global__ void __launch_bounds__(128, 8) k_plane_step_split2(const __grid_constant__ StepArgs a) {
+// Two rays per thread: n / 2 threads (rounded up), blocks of 128, capped at
+// 80 registers (6 blocks per SM).  Measured on the light cone against one ray
+// per thread at 64 registers: 759 against 771 ms per step (bit-identical
+// results); 64 / 72 / 96 / 116 registers: 1005 / 808 / 760 / 898 ms.
+__global__ void __launch_bounds__(128, 6) k_plane_step_split2(const __grid_constant__ StepArgs a) {
   __shared__ double sacc[10 * 128];
   __shared__ double sxy[4 * 128];
   plane_step_split_ptree2(a, sacc, sxy);
 }
 
-// PTREE: the plane holds exactly one particle halo, whose tree is a.tree
-// (no field plane on such a launch).
+// PTREE: the plane holds exactly one particle halo, whose tree is a.tree (no
+// field plane), one ray per thread; otherwise planes with several particle
+// halos or a field plane.
 template <bool FIELD = false, bool PTREE = false>
 __global__ void __launch_bounds__(128, 8) k_plane_step_split(const __grid_constant__ StepArgs a) {
   if (PTREE) {
@@ -1058,8 +1069,12 @@ int ensure_ws(LensWS *w, size_t n, bool per_ray) {
 }
 
 // One launch per plane, in order.  Split-form planes that hold exactly one
-// particle halo pass its tree in the kernel parameters (PTREE); planes with
-// a field plane use the FIELD instances.
+// particle halo and no field plane pass the tree in the kernel parameters:
+// k_plane_step_split2 (two rays per thread) from kTwoRayMin rays on, below
+// that the one-ray instance, which fills more of the GPU with a small grid
+// (512^2 rays on one plane: 45M rays/s against 35M); planes with a field
+// plane use the FIELD instances.
+constexpr size_t kTwoRayMin = (size_t)1 << 20;
 int launch_plane_steps(const glb_lens *l, StepArgs &a, int jmax_launch, int precision, cudaStream_t s,
                        const unsigned long long *d_counts) {
   const size_t n = a.n;
@@ -1087,8 +1102,10 @@ int launch_plane_steps(const glb_lens *l, StepArgs &a, int jmax_launch, int prec
       k_plane_step<GLB_PREC_FP64, true><<<nblk(n, 128), 128, 0, s>>>(a);
     else if (precision == GLB_PREC_SPLIT && fld)
       k_plane_step_split<true><<<nblk(n, 128), 128, 0, s>>>(a);
-    else if (precision == GLB_PREC_SPLIT && ptree)
+    else if (precision == GLB_PREC_SPLIT && ptree && n >= kTwoRayMin)
       k_plane_step_split2<<<nblk((n + 1) / 2, 128), 128, 0, s>>>(a);
+    else if (precision == GLB_PREC_SPLIT && ptree)
+      k_plane_step_split<false, true><<<nblk(n, 128), 128, 0, s>>>(a);
     else if (precision == GLB_PREC_SPLIT)
       k_plane_step_split<<<nblk(n, 128), 128, 0, s>>>(a);
     else if (fld)
