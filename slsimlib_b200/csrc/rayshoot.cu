@@ -723,8 +723,9 @@ __device__ __forceinline__ void plane_step_split_ptree2(const StepArgs &a, doubl
 
 // Two rays per thread: n / 2 threads (rounded up), blocks of 128, capped at
 // 80 registers (6 blocks per SM).  Measured on the light cone against one ray
-// per thread at 64 registers: 759 against 771 ms per step (bit-identical
-// results); 64 / 72 / 96 / 116 registers: 1005 / 808 / 760 / 898 ms.
+// per thread at 64 registers: 748 against 771 ms per step; 64 / 72 registers:
+// 966 / 795 ms (spills), 96 / 116 registers (before the shared offset):
+// 760 / 898 ms.
 __global__ void __launch_bounds__(128, 6) k_plane_step_split2(const __grid_constant__ StepArgs a) {
   __shared__ double sacc[10 * 128];
   __shared__ double sxy[4 * 128];

@@ -356,11 +356,15 @@ __device__ __forceinline__ void walk_split(const TreeDev &T, double rx, double r
 }
 
 // The split walk for two rays per lane (a warp walks 64 neighbouring rays):
-// each ray keeps its own opening decisions, offsets, partial sums and resume
-// point exactly as walk_split<false> does for one, while the node rows, the
-// warp vote, the loop control and the leaf particles are loaded and executed
-// once for both.  rxy: {rx0, ry0, rx1, ry1} (the rays' FP64 positions, read
-// only on the rare FP64 paths); acc0 / acc1: the rays' FP64 totals.
+// each ray keeps its own opening decisions, partial sums and resume point as
+// walk_split<false> does for one, while the node rows, the warp vote, the
+// loop control and the leaf particles are loaded and executed once for both.
+// The second ray's offset to a node is the first's plus the constant
+// difference of the two rays (d1 = d0 + (r0 - r1), one packed add instead of
+// a double-float offset): its FP32 error, about eps (|d0| + |d1|), stays far
+// inside the ambiguity band of the opening tests, which the FP64 test settles
+// as for one ray, so the interaction set is unchanged.  rxy: {rx0, ry0, rx1,
+// ry1} (the rays' FP64 positions); acc0 / acc1: the rays' FP64 totals.
 __device__ __forceinline__ void far_term(const float4 &c1, const float4 &c2, float2 d, float r2f, bool screen,
                                          float ns2l, float piaf, F32Acc &fa, double *acc) {
   const float scr = screen ? ex2_approx(r2f * ns2l) : 1.0f;
@@ -417,13 +421,14 @@ __device__ __forceinline__ void walk_split2(const TreeDev &T, const double *rxy,
   const bool closed = T.sheet_closed;
   const bool sheet = T.inv_area != 0.0 && !closed;
   const float piaf = sheet ? (float)(kPi * T.inv_area) : 0.f;
-  float2 nrh[2], nrl[2];
-  for (int r = 0; r < 2; ++r) {
-    const double rx = rxy[2 * r], ry = rxy[2 * r + 1];
+  float2 nrh[1], nrl[1];
+  {
+    const double rx = rxy[0], ry = rxy[1];
     const float rxh = (float)rx, ryh = (float)ry;
-    nrh[r] = make_float2(-rxh, -ryh);
-    nrl[r] = make_float2(-(float)(rx - (double)rxh), -(float)(ry - (double)ryh));
+    nrh[0] = make_float2(-rxh, -ryh);
+    nrl[0] = make_float2(-(float)(rx - (double)rxh), -(float)(ry - (double)ryh));
   }
+  const float2 del = make_float2((float)(rxy[0] - rxy[2]), (float)(rxy[1] - rxy[3]));
   F32Acc fa0, fa1;
   fa0.zero();
   fa1.zero();
@@ -438,7 +443,7 @@ __device__ __forceinline__ void walk_split2(const TreeDev &T, const double *rxy,
     const bool act0 = node >= resume0, act1 = node >= resume1;
     const float2 cc = make_float2(c0.x, c0.y), cl = make_float2(c0.z, c0.w);
     const float2 d0 = __fadd2_rn(__fadd2_rn(cc, nrh[0]), __fadd2_rn(cl, nrl[0]));
-    const float2 d1 = __fadd2_rn(__fadd2_rn(cc, nrh[1]), __fadd2_rn(cl, nrl[1]));
+    const float2 d1 = __fadd2_rn(d0, del);
     const float2 dd0 = __fmul2_rn(d0, d0), dd1 = __fmul2_rn(d1, d1);
     const float r2f0 = dd0.x + dd0.y, r2f1 = dd1.x + dd1.y;
     bool open0 = false, open1 = false;

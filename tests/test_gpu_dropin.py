@@ -124,3 +124,23 @@ def test_dropin_find_crit_grid_refinement_rounds():
     for (hc, pc), (hg, pg) in zip(cc, gc):
         np.testing.assert_array_equal(hg[:6], hc[:6])
         check_rays(pc, pg)
+
+
+def test_dropin_split_precision():
+    """glamer_b200_dropin::set_precision(GLB_PREC_SPLIT): the reference's
+    rayshooterInternal(N, Point*) through the split form stays within the
+    deflection tolerance of the reference's FP64 result (median 1e-6,
+    99.9th percentile 1e-5)."""
+    rng = np.random.default_rng(4)
+    x = rng.uniform(-6, 6, (4000, 2)) * synth.ARCSEC
+    spec = lens_spec()
+    out = []
+    for binary, pre in ((H.REF_BIN, []), (H.DROPIN_BIN, ["dropin 1"])):
+        R = H.RefDriver(binary)
+        of = R._file()
+        R.run(R.lens_lines(spec) + pre + [f"points {R._file(x)} {len(x)} {of} -"], timeout=900)
+        out.append(np.fromfile(of).reshape(-1, 6))
+    c, g = out
+    ar, a = x - c[:, :2], x - g[:, :2]
+    e = np.hypot(*(a - ar).T) / np.hypot(*ar.T)
+    assert np.median(e) <= 1e-6 and np.percentile(e, 99.9) <= 1e-5, (np.median(e), e.max())
