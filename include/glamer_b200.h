@@ -57,7 +57,10 @@ enum {
 /* Precision of the tree walk. */
 enum {
   GLB_PREC_FP64 = 0,  /* plain FP64 walk, the reference's arithmetic */
-  GLB_PREC_SPLIT = 1, /* FP32 walk with compensated sums, FP64 offsets and recursion */
+  GLB_PREC_SPLIT = 1, /* FP32 walk with compensated sums, FP64 offsets and recursion; in
+                         calls of 2^20 rays or more a ray's result can change at the
+                         rounding level (~1e-9) with its neighbour in the call (pairs of
+                         rays share node offsets); the FP64 form is per-ray exact */
   GLB_PREC_FP32 = 2   /* plain FP32 tree walk (tree-force calls only; the precision sweep) */
 };
 
