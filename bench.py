@@ -756,8 +756,9 @@ def main():
                          "counts": {"V": V, "F": F, "P": P, "B": B, "S": S},
                          "lane_efficiency": {"nodes": V / max(Wn, 1), "leaf_particles": P / max(Wp, 1)}},
             # per step: ray bbox, Morton keys, the 6 kernels of the CUB radix sort compiled into the
-            # library, state init, one plane step per plane, finish (ncu launch list)
-            "gpu_launches": args.steps * (10 + nplanes),
+            # library, and per slab of rays (two from 2^21 rays on) state init, one plane step per
+            # plane, finish (ncu launch list)
+            "gpu_launches": args.steps * (8 + (2 if n >= (1 << 21) else 1) * (2 + nplanes)),
             "clocks": clocks,
         }
         if cpu:

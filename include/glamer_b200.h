@@ -58,9 +58,11 @@ enum {
 enum {
   GLB_PREC_FP64 = 0,  /* plain FP64 walk, the reference's arithmetic */
   GLB_PREC_SPLIT = 1, /* FP32 walk with compensated sums, FP64 offsets and recursion; in
-                         calls of 2^20 rays or more a ray's result can change at the
-                         rounding level (~1e-9) with its neighbour in the call (pairs of
-                         rays share node offsets); the FP64 form is per-ray exact */
+                         ray-shooting calls of 2^20 rays or more (and served requests of
+                         that size) a ray's result can change at the rounding level
+                         (~1e-9) with its neighbour in the call (pairs of spatially sorted
+                         rays share node offsets); tree-force calls and the FP64 form are
+                         per-ray exact */
   GLB_PREC_FP32 = 2   /* plain FP32 tree walk (tree-force calls only; the precision sweep) */
 };
 
@@ -93,8 +95,9 @@ int glb_tree_force2D_recur(glb_tree *t, size_t n, const double *rays, double *al
 /* force2D_recur for n rays already on the device (2n doubles, physical Mpc),
  * in any precision form; out_dev gets 5 doubles per ray {alpha0, alpha1,
  * kappa, gamma0, gamma1} (no potential).  Enqueued on `stream` (NULL: the
- * tree's own stream).  Rays are walked 32 to a warp in the given order, so
- * spatially sorted rays walk fastest. */
+ * tree's own stream).  Rays are walked 32 to a warp in the given order (64,
+ * two per thread, in the split form from 2^20 rays on with opening angles
+ * under 0.2), so spatially sorted rays walk fastest. */
 int glb_tree_force_device(glb_tree *t, size_t n, const double *rays_dev, double *out_dev, int precision,
                           void *stream);
 
@@ -369,12 +372,16 @@ int glb_batch_destroy(glb_batch *b);
  * on the GPU.  Admission is by device memory: at every dispatch the server
  * reads the HBM free at that moment (plus memory its own stream-ordered pool
  * holds unused), keeps 5 % of the device free, and admits the requests whose
- * batch memory (about 170 bytes per ray) fits; a batch takes its memory from
+ * batch memory (about 250 bytes per ray) fits; a batch takes its memory from
  * the pool when it launches and gives it back when its results are copied
  * out, so a request that does not fit waits until batches in flight finish
  * (GLB_ERR_OOM from glb_server_wait if none is in flight).  The pool keeps
- * what it has reserved until the server is destroyed.  A request's results do not depend
- * on what it is batched with.  The lenses must outlive the server. */
+ * what it has reserved until the server is destroyed.  Requests of fewer than
+ * 2^20 rays run in 32-ray chunks of the batched kernel; larger ones through
+ * the per-plane kernels of glb_lens_rayshoot on the batch's stream, so their
+ * results are those of glb_lens_rayshoot for the same rays and source
+ * redshift.  A request's results do not depend on what it is batched with.
+ * The lenses must outlive the server. */
 typedef struct glb_server glb_server;
 int glb_server_create(glb_lens *const *models, int nmodels, size_t max_rays_per_batch, int precision, int nslots,
                       glb_server **out);

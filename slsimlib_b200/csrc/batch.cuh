@@ -564,10 +564,20 @@ double now_s() {
 
 // Device memory of one batch, in bytes per ray: x, sorted x, y, A (10
 // doubles), two 64-bit sort keys, three 32-bit index arrays, the radix sort's
-// temporary storage (bounded by kSortBytesPerRay per ray plus a constant) and
-// the 32-ray chunks.
+// temporary storage (bounded by kSortBytesPerRay per ray plus a constant), the
+// 32-ray chunks and the recursion state of requests that take the per-plane
+// kernels (12 doubles).
 constexpr size_t kSortBytesPerRay = 32;
-constexpr size_t kBatchBytesPerRay = 10 * 8 + 2 * 8 + 3 * 4 + kSortBytesPerRay + 8;
+constexpr size_t kBatchBytesPerRay = 10 * 8 + 2 * 8 + 3 * 4 + kSortBytesPerRay + 8 + 12 * 8;
+// Requests of at least this many rays run through the per-plane kernels
+// (one launch per plane over the request's rays, the lens path's kernels,
+// which fill the GPU for several waves from this size on); smaller ones go
+// through k_batch's 32-ray chunks, whose persistent queue balances uneven
+// requests better (a stream of 1e3-5e5-ray requests on light cones at 60
+// requests/s: 3.84M rays/s all on k_batch against 3.70M with requests from
+// 16,384 rays on per plane).  The choice depends only on the request, so its
+// result is the same alone and in any mix.
+constexpr size_t kServePerPlaneMin = (size_t)1 << 20;
 constexpr size_t kBatchBytesFixed = (size_t)4 << 20;
 
 struct Slot {
@@ -598,6 +608,7 @@ struct glb_server {
   // new memory each time; admission counts what it holds unused as free
   cudaMemPool_t pool = nullptr;
   std::vector<glb_lens *> models;
+  std::vector<LensDev> h_lenses;  // host copies (source-plane defaults of each model)
   DBuf<LensDev> d_lenses;
   NFWTables tab{};
   int grid = 0;
@@ -623,6 +634,50 @@ struct glb_server {
 namespace {
 
 size_t batch_bytes(size_t n) { return kBatchBytesFixed + n * kBatchBytesPerRay; }
+
+// Source-plane scalars of a request: zs >= 0 as Lens::FindSourcePlane
+// (MultiPlane/lens.cpp:2659-2680, the host twin of k_batch's
+// find_source_plane), zs < 0 the model's own source plane.
+void request_source(const glb_lens *l, const LensDev &d, double zs, int &jmax, double &dls, double &dds) {
+  if (zs < 0) {
+    jmax = d.jmax_default;
+    dls = d.dls_default;
+    dds = d.dds_default;
+    return;
+  }
+  const double Ds = coordist(l->cosmo, zs);
+  double Dls;
+  if (zs <= l->plane_z[0]) {
+    jmax = 0;
+    Dls = Ds;
+  } else {
+    jmax = (int)l->planes.size();
+    while (l->plane_z[jmax - 1] > zs) --jmax;
+    Dls = coordist2(l->cosmo, l->plane_z[jmax - 1], zs);
+  }
+  dls = Dls / Ds;
+  dds = jmax > 0 ? l->Dl[jmax - 1] / Ds : 0.0;
+}
+
+// The recursion state of rays already in sorted order (theta = SumPrevAlphas
+// = x, A = SumPrevAG = I; the layout of k_init_state).
+__global__ void k_init_sorted(const double *xs, size_t n, double *st) {
+  const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const double t0 = xs[2 * k], t1 = xs[2 * k + 1];
+  st[k] = t0;
+  st[n + k] = t1;
+  st[2 * n + k] = t0;
+  st[3 * n + k] = t1;
+  st[4 * n + k] = 1;
+  st[5 * n + k] = 0;
+  st[6 * n + k] = 0;
+  st[7 * n + k] = 1;
+  st[8 * n + k] = 1;
+  st[9 * n + k] = 0;
+  st[10 * n + k] = 0;
+  st[11 * n + k] = 1;
+}
 
 // Device memory available to a new batch now: free HBM plus memory the
 // stream-ordered pool holds but no allocation uses, less the reserve.
@@ -654,8 +709,14 @@ int launch_slot(glb_server *S, Slot &sl) {
   sl.n = n;
   // the batch's device memory, carved from one stream-ordered allocation
   std::vector<Chunk> C;
+  size_t big_max = 0;
+  auto per_plane = [S](const Req &q) { return q.n >= kServePerPlaneMin && !S->models[q.model]->planes.empty(); };
   for (size_t r = 0; r < nr; ++r) {
     Req &q = *sl.reqs[r];
+    if (per_plane(q)) {
+      big_max = std::max(big_max, q.n);
+      continue;
+    }
     for (size_t c = 0; c < q.n; c += 32) {
       Chunk k;
       memset(&k, 0, sizeof(k));
@@ -677,7 +738,8 @@ int launch_slot(glb_server *S, Slot &sl) {
   const size_t o_bb = o_A + al(32 * n), o_k = o_bb + al(32 * nr), o_k2 = o_k + al(8 * n);
   const size_t o_idx = o_k2 + al(8 * n), o_perm = o_idx + al(4 * n), o_req = o_perm + al(4 * n);
   const size_t o_ch = o_req + al(4 * n), o_cnt = o_ch + al(C.size() * sizeof(Chunk)), o_tmp = o_cnt + 256;
-  sl.dbytes = o_tmp + al(tb);
+  const size_t o_st = o_tmp + al(tb);
+  sl.dbytes = o_st + al(12 * big_max * sizeof(double));
   CKR(cudaMallocFromPoolAsync((void **)&sl.dmem, sl.dbytes, S->pool, s));
   char *m = sl.dmem;
   double *dx = (double *)(m + o_x), *dxs = (double *)(m + o_xs), *dy = (double *)(m + o_y), *dA = (double *)(m + o_A);
@@ -695,13 +757,38 @@ int launch_slot(glb_server *S, Slot &sl) {
   // chunks: requests stay contiguous in sorted order; 32 rays per chunk
   CKR(cudaMemcpyAsync(dch, C.data(), C.size() * sizeof(Chunk), cudaMemcpyHostToDevice, s));
   CKR(cudaMemsetAsync(counter, 0, sizeof(int), s));
-  if (S->precision == GLB_PREC_SPLIT)
-    k_batch<GLB_PREC_SPLIT><<<S->grid, 128, batch_smem_bytes(128), s>>>(dch, (int)C.size(), S->d_lenses.p, S->tab, dxs, perm, dy, dA,
-                                                    counter);
-  else
-    k_batch<GLB_PREC_FP64><<<S->grid, 128, batch_smem_bytes(128), s>>>(dch, (int)C.size(), S->d_lenses.p, S->tab, dxs, perm, dy, dA,
-                                                   counter);
-  CKR(cudaGetLastError());
+  if (!C.empty()) {
+    if (S->precision == GLB_PREC_SPLIT)
+      k_batch<GLB_PREC_SPLIT><<<S->grid, 128, batch_smem_bytes(128), s>>>(dch, (int)C.size(), S->d_lenses.p, S->tab,
+                                                                         dxs, perm, dy, dA, counter);
+    else
+      k_batch<GLB_PREC_FP64><<<S->grid, 128, batch_smem_bytes(128), s>>>(dch, (int)C.size(), S->d_lenses.p, S->tab,
+                                                                        dxs, perm, dy, dA, counter);
+    CKR(cudaGetLastError());
+  }
+  // large requests: the lens path's per-plane kernels over the request's rays
+  // (contiguous in sorted order), results scattered to their batch slots
+  double *st = (double *)(m + o_st);
+  for (size_t r = 0; r < nr; ++r) {
+    Req &q = *sl.reqs[r];
+    if (!per_plane(q)) continue;
+    const glb_lens *l = S->models[q.model];
+    const LensDev &d = S->h_lenses[q.model];
+    const size_t nq = q.n, off = sl.offs[r];
+    StepArgs a;
+    memset(&a, 0, sizeof(a));
+    a.planes = d.planes;
+    a.halos = d.halos;
+    a.tab = S->tab;
+    a.st = st;
+    a.n = nq;
+    a.charge = d.charge;
+    request_source(l, d, q.zs, a.jmax, a.dls_ds, a.d_ds);
+    k_init_sorted<<<nblk(nq, 256), 256, 0, s>>>(dxs + 2 * off, nq, st);
+    if (int rc = launch_plane_steps(l, a, a.jmax, S->precision, s, nullptr, nq >= kTwoRayMin)) return rc;
+    k_finish<<<nblk(nq, 256), 256, 0, s>>>(st, perm + off, nq, dy, dA);
+    CKR(cudaGetLastError());
+  }
   CKR(cudaMemcpyAsync(sl.hy, dy, 2 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
   CKR(cudaMemcpyAsync(sl.hA, dA, 4 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
   CKR(cudaFreeAsync(sl.dmem, s));
@@ -850,6 +937,7 @@ int glb_server_create(glb_lens *const *models, int nmodels, size_t max_rays_per_
     if (!models[i] || models[i]->device != S->device) return fail(GLB_ERR_ARG, "models must be lenses on one device");
     if (int rc = make_lens_dev(models[i], L[i])) return rc;
     S->models.push_back(models[i]);
+    S->h_lenses.push_back(L[i]);
   }
   CKR(S->d_lenses.alloc(nmodels));
   CKR(cudaMemcpy(S->d_lenses.p, L.data(), nmodels * sizeof(LensDev), cudaMemcpyHostToDevice));

@@ -65,6 +65,7 @@ struct Tree {
   int nnodes = 0;
   size_t nparticles = 0;
   size_t nbranches = 0;            // including empty children (reference count)
+  double theta = 0.1;              // opening angle the tree was built with
   std::vector<double> export_rows; // 16 doubles per branch when requested
   float build_ms = 0;
 };

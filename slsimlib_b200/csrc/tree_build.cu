@@ -505,6 +505,7 @@ Status build_tree(const glb_particle_rec *hp, size_t n, const TreeParams &prm, b
                   cudaStream_t st, std::unique_ptr<Tree> &out) {
   auto T = std::make_unique<Tree>();
   T->nparticles = n;
+  T->theta = prm.theta;
   const int multimass = prm.mass_fixed <= 0 ? 1 : 0;  // quadTree.h:272-273
   const int multiradius = prm.size_fixed <= 0 ? 1 : 0;
   T->dev.inv_area = prm.inv_area;

@@ -124,6 +124,41 @@ def test_server_request_same_alone_and_in_the_mix(precision):
     srv.close()
 
 
+@pytest.mark.parametrize("precision", [glb.PREC_FP64, glb.PREC_SPLIT])
+def test_server_large_requests_take_the_lens_path(precision):
+    """Requests of at least 2^20 rays run through the lens path's per-plane
+    kernels inside the server: their results are the lens path's (the same
+    kernels on the same rays), alone and mixed with small requests."""
+    specs = _specs()[:3]
+    models = [make_lens(s) for s in specs]
+    rng = np.random.default_rng(11)
+    srv = glb.Server(models, max_rays_per_batch=3_000_000, precision=precision, nslots=2)
+    big = [(m, rng.normal(0, 6 * synth.ARCSEC, size=(n, 2)), zs)
+           for m, n, zs in ((0, 1 << 20, -1.0), (1, (1 << 20) + 4001, 2.0), (2, (1 << 20) + 1, 1.1))]
+    small = [(int(rng.integers(0, 3)), rng.normal(0, 6 * synth.ARCSEC, size=(int(rng.integers(1, 3000)), 2)),
+              float(rng.uniform(1, 3))) for _ in range(6)]
+    tickets = [srv.submit(m, x, zs) for m, x, zs in big + small]
+    out = [srv.wait(t, timeout=240) for t in tickets]
+    for (m, x, zs), (y, A, _) in zip(big, out[:3]):
+        yl, Al = models[m].rayshooterInternal(x, None if zs < 0 else np.full(len(x), zs), precision)
+        if precision == glb.PREC_FP64:
+            assert np.max(rel_err(y, yl)) < 1e-12 and np.max(np.abs(A - Al)) < 1e-12
+        else:
+            e = defl_err(x, y, yl)
+            assert np.median(e) <= 1e-6 and np.percentile(e, 99) <= 1e-5
+    if precision == glb.PREC_FP64:  # every request against the oracle (its first 2,000 rays)
+        for (m, x, zs), (y, A, _) in zip(big + small, out):
+            k = min(len(x), 2000)
+            yo, Ao = H.OracleLens(specs[m]).rayshoot(x[:k], None if zs < 0 else np.full(k, zs))
+            assert np.max(rel_err(y[:k], yo)) < 1e-9 and np.max(np.abs(A[:k] - Ao)) < 1e-9
+    # the same large request alone gives the same bits
+    m, x, zs = big[1]
+    y1, A1, _ = srv.wait(srv.submit(m, x, zs), timeout=240)
+    np.testing.assert_array_equal(y1, out[1][0])
+    np.testing.assert_array_equal(A1, out[1][1])
+    srv.close()
+
+
 def test_server_rejects_oversized_and_unknown():
     models = [make_lens(_specs()[0])]
     srv = glb.Server(models, max_rays_per_batch=1000, precision=glb.PREC_FP64, nslots=1)

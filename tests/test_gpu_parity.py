@@ -366,6 +366,39 @@ def test_tree_force_device_forms_and_direct_sum():
     assert np.max(vec_err(o.cpu().numpy()[:, :2], ds[:, :2])) < 1e-10
 
 
+def test_split_tree_force_two_rays_per_thread():
+    """From 2^20 rays on (opening angle under 0.2) the split tree force walks
+    two rays per thread: each ray's result is bit-identical to the one-ray
+    kernel's (calls under 2^20 rays), in any ray order, including an odd
+    count that leaves the last thread one ray; the split tolerance against
+    the FP64 form holds."""
+    import torch
+    rng = np.random.default_rng(31)
+    p = synth.nfw_particles(rng, 200000, 1e14, 5.0, 0.3, 1e-3)
+    t = glb.TreeQuadParticles(p, bucket=5, theta_force=0.1)
+    n = (1 << 20) + 1
+    rays = np.concatenate([rng.normal(0, 0.02, (n // 2, 2)), rng.uniform(-0.3, 0.3, (n - n // 2, 2))])
+    rays = rays[rng.permutation(n)]  # arbitrary order: pairs of rays far apart
+    dr = torch.from_numpy(rays).cuda()
+
+    def force(lo, hi, prec):
+        o = torch.zeros((hi - lo, 5), dtype=torch.float64, device="cuda")
+        d = dr[lo:hi].contiguous()
+        torch.cuda.synchronize()
+        t.force_device(hi - lo, d.data_ptr(), o.data_ptr(), prec, None)
+        torch.cuda.synchronize()
+        return o.cpu().numpy()
+
+    two = force(0, n, glb.PREC_SPLIT)
+    h = 1 << 19
+    one = np.concatenate([force(0, h, glb.PREC_SPLIT), force(h, n, glb.PREC_SPLIT)])
+    np.testing.assert_array_equal(two, one)
+    ref = np.concatenate([force(0, h, glb.PREC_FP64), force(h, n, glb.PREC_FP64)])
+    for name, e in (("alpha", vec_err(two[:, :2], ref[:, :2])), ("kappa", scal_err(two[:, 2], ref[:, 2], 1e-6)),
+                    ("gamma", vec_err(two[:, 3:5], ref[:, 3:5]))):
+        assert np.median(e) <= 1e-6 and np.percentile(e, 99.9) <= 1e-5, (name, np.median(e), e.max())
+
+
 @pytest.mark.parametrize("inv_area,screen,negative", [(0.0, 0.0, False), (4.0, 0.0, False), (0.0, 1.0, False),
                                                      (4.0, 30.0, False), (4.0, 1.0, True)])
 def test_split_tree_force_softened_regime(inv_area, screen, negative):
