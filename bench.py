@@ -41,9 +41,9 @@ FIELD_ARCSEC = 60.0
 # B-spline corrections S) and per ray-plane recursion
 FLOPS = {"V": 8, "F": 60, "P": 29, "B": 8, "S": 65, "rec": 50}
 # DRAM bytes (read + write) per ray of one split plane launch, from an ncu capture of
-# `bench.py --no-cpu --no-served --n1d 1536` (418.5 MB for 2,359,296 rays): the 96 B ray
-# state read and written once and the plane's L2-resident tree
-DRAM_BYTES_PER_RAY_PLANE = 177
+# `bench.py --no-cpu --no-served --n1d 1536` (185.5 MB for one 1,179,648-ray slab of a
+# plane): the 96 B ray state read and written once and the plane's L2-resident tree
+DRAM_BYTES_PER_RAY_PLANE = 157
 
 
 def workload(small: bool):
@@ -748,8 +748,8 @@ def main():
                     "d2h_bytes_per_step": 48 * n},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": DRAM_BYTES_PER_RAY_PLANE * n,
-                         "traffic_note": "dram read+write bytes per plane launch: ncu capture of one 1536^2 launch "
-                                         "(177 B/ray) scaled by rays",
+                         "traffic_note": "dram read+write bytes per plane (both slabs): ncu capture of one "
+                                         "1,179,648-ray slab launch at 1536^2 (157 B/ray) scaled by rays",
                          "kernel": "k_plane_step_split2", "kernel_ms_per_step": k_ms,
                          "peak_note": "FP32 CUDA-core FMA rate at the sampled SM clock (148 SMs x 128 lanes x 2)",
                          "alg_flops_per_step": alg_flops,
