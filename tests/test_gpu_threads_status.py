@@ -1,6 +1,6 @@
 """Concurrent use of one lens from several host threads, and the per-ray
 status output (skip flags for the reference's in_image == MAYBE points,
-non-finite results), through the C ABI."""
+non-finite results), and large calls cut into slabs, through the C ABI."""
 import threading
 
 import numpy as np
@@ -8,6 +8,7 @@ import pytest
 
 import slsimlib_b200 as glb
 from slsimlib_b200 import synth
+from tests import harness as H
 
 pytestmark = pytest.mark.gpu
 
@@ -87,3 +88,34 @@ def test_per_ray_status_and_skip():
     np.testing.assert_array_equal(y[skip], y0[skip])
     assert np.all(st[skip] == glb.RAY_SKIPPED) and st[17] == glb.RAY_NONFINITE
     np.testing.assert_array_equal(y[keep], x[keep])
+
+
+def test_large_call_in_slabs_matches_small_calls():
+    """Calls of 2^21 rays or more run as two slabs of sorted rays on two
+    streams.  The FP64 form gives each ray the same bits as the same rays
+    shot in calls small enough to run in one piece, with per-ray source
+    redshifts, skip flags and status bytes across the slab boundary; the
+    split form keeps the deflection tolerance."""
+    spec = synth.light_cone(seed=5, n_total=12000, n_planes=3, halos_per_plane=2, zs=2.2)
+    L = glb.lens_from_spec(spec)
+    rng = np.random.default_rng(17)
+    n = (1 << 21) + 4097
+    x = rng.uniform(-20, 20, (n, 2)) * synth.ARCSEC
+    zs = rng.uniform(1.0, 3.0, n)
+    skip = np.zeros(n, dtype=bool)
+    skip[::11] = True
+    y0 = np.full((n, 2), 5.0)
+    A0 = np.full((n, 4), 7.0)
+    y, A, st = L.rayshooterInternal_status(x, source_zs=zs, skip=skip, y=y0, A=A0)
+    np.testing.assert_array_equal(y[skip], y0[skip])
+    np.testing.assert_array_equal(A[skip], A0[skip])
+    assert np.all(st[skip] == glb.RAY_SKIPPED) and np.all(st[~skip] == glb.RAY_OK)
+    for idx in np.array_split(np.arange(n), 5):  # about 420,000 rays a call: one piece
+        ys, As = L.rayshooterInternal(x[idx], source_zs=zs[idx])
+        k = ~skip[idx]
+        np.testing.assert_array_equal(y[idx][k], ys[k])
+        np.testing.assert_array_equal(A[idx][k], As[k])
+    y64, A64 = L.rayshooterInternal(x, source_zs=zs)
+    y32, A32 = L.rayshooterInternal(x, source_zs=zs, precision=glb.PREC_SPLIT)
+    e = H.error_stats(x, y32, A32, y64, A64)["alpha"]
+    assert e["median"] <= 1e-6 and e["p999"] <= 1e-5, e
