@@ -650,6 +650,22 @@ def main():
     def shoot(prec):
         lens.rayshoot_device(n, x.data_ptr(), None, y.data_ptr(), A.data_ptr(), prec, stream.cuda_stream)
 
+    served = None
+    if rank == 0 and not args.no_served:
+        # the served form on a few resident models: this light cone and three
+        # more of the same kind (seeds 5000-5002), two Poisson rates; measured
+        # first, with its own clock record
+        import multiprocessing as mp
+        with mp.get_context("spawn").Pool(3) as pool:
+            extra = pool.map(_c5_model, [5000, 5001, 5002] if not args.small else [5000])
+        models = [lens] + [make_lens(sp) for sp in extra]
+        with ClockSampler(local) as sclk:
+            sw, sst, serr = served_sweep(models, (20.0, 60.0), 120 if not args.small else 20)
+        served = {"models": len(models), "sweep": sw, "server": sst, "errors_vs_fp64_alpha": serr,
+                  "request_rays": "log-uniform 1e3-5e5 in 1-8 Gaussian blobs (0.05-1 arcsec), z_s uniform 1-3",
+                  "latency": "submit to results on the host (ms)", "clocks": sclk.summary()}
+        del models, extra
+
     # FP64 form (the error reference) and its timing
     shoot(glb.PREC_FP64)
     torch.cuda.synchronize()
@@ -688,19 +704,6 @@ def main():
     y32, A32 = y.cpu().numpy(), A.cpu().numpy()
     errs = error_stats(x_host, y32, A32, y64, A64)
     attrib = attribution(spec, lens, x_host) if rank == 0 and not args.small else None
-    served = None
-    if rank == 0 and not args.no_served:
-        # the served form on a few resident models: this light cone and three
-        # more of the same kind (seeds 5000-5002), two Poisson rates
-        import multiprocessing as mp
-        with mp.get_context("spawn").Pool(3) as pool:
-            extra = pool.map(_c5_model, [5000, 5001, 5002] if not args.small else [5000])
-        models = [lens] + [make_lens(sp) for sp in extra]
-        sw, sst, serr = served_sweep(models, (20.0, 60.0), 60 if not args.small else 20)
-        served = {"models": len(models), "sweep": sw, "server": sst, "errors_vs_fp64_alpha": serr,
-                  "request_rays": "log-uniform 1e3-5e5 in 1-8 Gaussian blobs (0.05-1 arcsec), z_s uniform 1-3",
-                  "latency": "submit to results on the host (ms)"}
-        del models, extra
 
     # end to end through the host C ABI (pinned host buffers, copies timed)
     xp = torch.from_numpy(x_host).pin_memory()

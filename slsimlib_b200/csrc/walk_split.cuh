@@ -498,12 +498,16 @@ __device__ __forceinline__ void walk_split2(const TreeDev &T, const double *rxy,
       continue;
     }
     bool nearc0 = false, nearc1 = false;
-    if (open0) {
+    // the near-field test matters at a leaf and at an internal node with big
+    // particles (c3.w of them) only; skipping it elsewhere measured 1.3 %
+    // faster per light-cone step (the one-ray walk spills more when it skips)
+    const bool need_near = c3.y || c3.w > 0;
+    if (open0 && need_near) {
       const float e = r2f0 - c1.y;
       nearc0 = e < 0.f;
       if (fabsf(e) <= kAmbiguous * c1.y) nearc0 = node_test_f64(T.nodes + node, rxy[0], rxy[1], 1);
     }
-    if (open1) {
+    if (open1 && need_near) {
       const float e = r2f1 - c1.y;
       nearc1 = e < 0.f;
       if (fabsf(e) <= (DELTA ? fmaf(kAmbiguous, c1.y, xb1) : kAmbiguous * c1.y))
@@ -532,7 +536,7 @@ __device__ __forceinline__ void walk_split2(const TreeDev &T, const double *rxy,
       }
       node = skip;
     } else {
-      if (__any_sync(kFull, nearc0 || nearc1)) {
+      if (c3.w > 0 && __any_sync(kFull, nearc0 || nearc1)) {
         const int b0 = c3.z, b1 = b0 + c3.w;
         for (int b = b0; b < b1; ++b) {
           const float4 P = __ldg(T.bigs + b);
