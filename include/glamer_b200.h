@@ -214,6 +214,10 @@ int glb_lens_rayshoot(glb_lens *l, size_t n, const double *x, const double *zs, 
  * buffers on the lens, created on its first call and freed with the lens.
  * Successive device-buffer calls of one thread are ordered on the GPU even
  * when they name different streams (they share that thread's buffers).
+ * A call of 2^21 rays or more runs its second half of the sorted rays on a
+ * second stream of the thread's workspace, forked from and joined back to
+ * `stream` through events, so work enqueued on `stream` after the call still
+ * sees its results.
  * Adding halos or resetting the source plane while another thread shoots rays
  * through the same lens is not supported (as in the reference). */
 int glb_lens_rayshoot_device(glb_lens *l, size_t n, const double *x_dev, const double *zs_dev,
