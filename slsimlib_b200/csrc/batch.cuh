@@ -68,7 +68,7 @@ __device__ __forceinline__ void plane_force(const PlaneDev &P, const HaloDev *ha
     double a[5];
     if (H->kind == HALO_PARTICLES) {
       for (int c = 0; c < 5; ++c) h[c] = 0.0;
-      particle_halo_acc<PREC, false>(H->tree, xc0, xc1, valid, h);
+      particle_halo_acc<PREC, false, false, true>(H->tree, xc0, xc1, valid, h);
       // force_halo negates the walk's alpha (particle_halo.h:432-433)
       a[0] = -h[0];
       a[1] = -h[1];

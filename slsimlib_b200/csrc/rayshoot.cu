@@ -407,7 +407,7 @@ __global__ void k_grid(size_t N1d, double c0, double c1, double range, double *x
   x[2 * i + 1] = c1 + range * (1.0 * (double)(i / N1d) / (double)(N1d - 1) - 0.5);
 }
 
-template <int PREC, bool PHI, bool COUNT = false>
+template <int PREC, bool PHI, bool COUNT = false, bool SKIPNEAR = false>
 __device__ __forceinline__ void particle_halo_acc(const TreeDev &T, double rx, double ry, bool valid, double *acc,
                                                   WalkCount *wc = nullptr) {
   if (T.periodic) {
@@ -419,7 +419,7 @@ __device__ __forceinline__ void particle_halo_acc(const TreeDev &T, double rx, d
         else if (PREC == GLB_PREC_FP32)
           walk_split<true>(T, rx + i * T.period_x, ry + j * T.period_y, valid, acc);
         else
-          walk_split<false>(T, rx + i * T.period_x, ry + j * T.period_y, valid, acc);
+          walk_split<false, SKIPNEAR>(T, rx + i * T.period_x, ry + j * T.period_y, valid, acc);
       }
   } else {
     if (PREC == GLB_PREC_FP64)
@@ -427,7 +427,7 @@ __device__ __forceinline__ void particle_halo_acc(const TreeDev &T, double rx, d
     else if (PREC == GLB_PREC_FP32)
       walk_split<true>(T, rx, ry, valid, acc);
     else
-      walk_split<false>(T, rx, ry, valid, acc);
+      walk_split<false, SKIPNEAR>(T, rx, ry, valid, acc);
   }
 }
 
