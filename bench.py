@@ -41,7 +41,7 @@ FIELD_ARCSEC = 60.0
 # B-spline corrections S) and per ray-plane recursion
 FLOPS = {"V": 8, "F": 60, "P": 29, "B": 8, "S": 65, "rec": 50}
 # DRAM bytes (read + write) per ray of one split plane launch, from an ncu capture of
-# `bench.py --no-cpu --no-served --n1d 1536` (185.5 MB for one 1,179,648-ray slab of a
+# `bench.py --no-cpu --no-served --n1d 1536` (184.8 MB for one 1,179,648-ray slab of a
 # plane): the 96 B ray state read and written once and the plane's L2-resident tree
 DRAM_BYTES_PER_RAY_PLANE = 157
 
