@@ -58,11 +58,12 @@ enum {
 enum {
   GLB_PREC_FP64 = 0,  /* plain FP64 walk, the reference's arithmetic */
   GLB_PREC_SPLIT = 1, /* FP32 walk with compensated sums, FP64 offsets and recursion; in
-                         ray-shooting calls of 2^20 rays or more (and served requests of
-                         that size) a ray's result can change at the rounding level
-                         (~1e-9) with its neighbour in the call (pairs of spatially sorted
-                         rays share node offsets); tree-force calls and the FP64 form are
-                         per-ray exact */
+                         ray shooting, rays are walked in blocks of 128 spatially sorted
+                         rays that share the classification of the tree's cells, so a
+                         ray's result can change at the rounding level (~1e-9; the order
+                         of its terms) with the other rays of its block, never its set of
+                         interactions; tree-force calls and the FP64 form are per-ray
+                         exact */
   GLB_PREC_FP32 = 2   /* plain FP32 tree walk (tree-force calls only; the precision sweep) */
 };
 

@@ -15,7 +15,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libglamer_b200.so")
 SOURCES = ["tree_build.cu", "rayshoot.cu", "field_plane.cu", "smoothing.cu"]
-HEADERS = ["cosmology.h", "glb_internal.h", "glb_host.h", "halos.cuh", "walk.cuh", "walk_split.cuh", "walk_halos.cuh", "batch.cuh"]
+HEADERS = ["cosmology.h", "glb_internal.h", "glb_host.h", "halos.cuh", "walk.cuh", "walk_split.cuh", "walk_group.cuh", "walk_halos.cuh", "batch.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

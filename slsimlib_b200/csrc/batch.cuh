@@ -785,7 +785,7 @@ int launch_slot(glb_server *S, Slot &sl) {
     a.charge = d.charge;
     request_source(l, d, q.zs, a.jmax, a.dls_ds, a.d_ds);
     k_init_sorted<<<nblk(nq, 256), 256, 0, s>>>(dxs + 2 * off, nq, st);
-    if (int rc = launch_plane_steps(l, a, a.jmax, S->precision, s, nullptr, nq >= kTwoRayMin)) return rc;
+    if (int rc = launch_plane_steps(l, a, a.jmax, S->precision, s, nullptr)) return rc;
     k_finish<<<nblk(nq, 256), 256, 0, s>>>(st, perm + off, nq, dy, dA);
     CKR(cudaGetLastError());
   }

@@ -25,6 +25,7 @@
 #include "halos.cuh"
 #include "walk.cuh"
 #include "walk_split.cuh"
+#include "walk_group.cuh"
 #include "walk_halos.cuh"
 
 using namespace glb;
@@ -407,7 +408,7 @@ __global__ void k_grid(size_t N1d, double c0, double c1, double range, double *x
   x[2 * i + 1] = c1 + range * (1.0 * (double)(i / N1d) / (double)(N1d - 1) - 0.5);
 }
 
-template <int PREC, bool PHI, bool COUNT = false, bool SKIPNEAR = false>
+template <int PREC, bool PHI, bool COUNT = false, bool SKIPNEAR = false, bool MERGE = true>
 __device__ __forceinline__ void particle_halo_acc(const TreeDev &T, double rx, double ry, bool valid, double *acc,
                                                   WalkCount *wc = nullptr) {
   if (T.periodic) {
@@ -419,7 +420,7 @@ __device__ __forceinline__ void particle_halo_acc(const TreeDev &T, double rx, d
         else if (PREC == GLB_PREC_FP32)
           walk_split<true>(T, rx + i * T.period_x, ry + j * T.period_y, valid, acc);
         else
-          walk_split<false, SKIPNEAR>(T, rx + i * T.period_x, ry + j * T.period_y, valid, acc);
+          walk_split<false, SKIPNEAR, MERGE>(T, rx + i * T.period_x, ry + j * T.period_y, valid, acc);
       }
   } else {
     if (PREC == GLB_PREC_FP64)
@@ -427,7 +428,7 @@ __device__ __forceinline__ void particle_halo_acc(const TreeDev &T, double rx, d
     else if (PREC == GLB_PREC_FP32)
       walk_split<true>(T, rx, ry, valid, acc);
     else
-      walk_split<false, SKIPNEAR>(T, rx, ry, valid, acc);
+      walk_split<false, SKIPNEAR, MERGE>(T, rx, ry, valid, acc);
   }
 }
 
@@ -462,7 +463,7 @@ struct StepArgs {
   double charge;
   unsigned long long *counts;  // V F P B S Wn Wp totals (counting launches only)
   // The plane's particle tree and its offset (posHalo * Dist) when the plane
-  // holds exactly one particle halo (k_plane_step_split2): read from
+  // holds exactly one particle halo (k_plane_step_split_g): read from
   // kernel parameter space, so the walk's pointers and scalars are uniform
   // operands rather than per-thread registers.
   TreeDev tree;
@@ -639,21 +640,28 @@ template <int PREC, bool COUNT = false, bool FIELD = false>
 __global__ void __launch_bounds__(128) k_plane_step(StepArgs a) {
   plane_step<PREC, COUNT, FIELD>(a);
 }
-// One ray per thread: the form for grids too small to fill the GPU with
-// k_plane_step_split2 (see launch_plane_steps).  A plane holding exactly one
-// particle halo (its tree in a.tree) and any number of analytic halos.  Only the ray slot stays
-// live across the tree walk: the walk's FP64 totals sit in shared memory
-// (sacc, five doubles per thread at a stride of five, which maps a half-warp's
-// 64-bit accesses onto distinct banks), and the recursion reloads theta, the
-// plane constants and the source-plane scalars after the walk.  The particle
-// halo's terms are added first, then the analytic halos' in insertion order.
-__device__ __forceinline__ void plane_step_split_ptree(const StepArgs &a, double *sacc) {
-  const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+// Split-form plane step with the block-level group walk (walk_group.cuh) for
+// a plane holding exactly one particle halo (its tree in a.tree, a kernel
+// parameter) and any number of analytic halos: one ray per thread, 128
+// neighbouring rays per block sharing the classification of the tree's
+// cells.  Each ray's FP64 totals sit in shared memory (sacc, five doubles per
+// thread at a stride of five: a half-warp's 64-bit accesses on distinct
+// banks), and the recursion reloads theta, the plane constants and the
+// source-plane scalars after the walk.  The particle halo's terms are added
+// first, then the analytic halos' in insertion order.  Measured per 2048^2
+// light-cone step against the per-ray walks: 638 ms against 718 (two rays
+// per thread) and 771 (one); 512^2 single plane 5.56 against 5.88 ms.
+__global__ void __launch_bounds__(128, 6) k_plane_step_split_g(const __grid_constant__ StepArgs a) {
+  __shared__ double sacc[5 * 128];
+  __shared__ double sxy[2 * 128];
+  __shared__ GroupLists G;
+  __shared__ double wbox[4][4];
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const size_t k = blockIdx.x * (size_t)blockDim.x + t;
   const bool inrange = k < a.n;
   const int jmax = (a.jmax_ray && inrange) ? a.jmax_ray[k] : a.jmax;
   const bool valid = inrange && a.j < jmax;
-  if (!__any_sync(kFull, valid)) return;
-  double *acc = sacc + 5 * threadIdx.x;
+  double *acc = sacc + 5 * t;
   for (int c = 0; c < 5; ++c) acc[c] = 0.0;
   double rx = 0, ry = 0;
   if (valid) {
@@ -661,10 +669,45 @@ __device__ __forceinline__ void plane_step_split_ptree(const StepArgs &a, double
     rx = a.st[k] * D - a.tree_px;
     ry = a.st[a.n + k] * D - a.tree_py;
   }
-  particle_halo_acc<GLB_PREC_SPLIT, false>(a.tree, rx, ry, valid, acc);
+  sxy[2 * t] = rx;
+  sxy[2 * t + 1] = ry;
+  double b0 = valid ? rx : 1e300, b1 = valid ? rx : -1e300, b2 = valid ? ry : 1e300, b3 = valid ? ry : -1e300;
+  for (int o = 16; o > 0; o >>= 1) {
+    b0 = fmin(b0, __shfl_xor_sync(kFull, b0, o));
+    b1 = fmax(b1, __shfl_xor_sync(kFull, b1, o));
+    b2 = fmin(b2, __shfl_xor_sync(kFull, b2, o));
+    b3 = fmax(b3, __shfl_xor_sync(kFull, b3, o));
+  }
+  if (lane == 0) {
+    wbox[warp][0] = b0;
+    wbox[warp][1] = b1;
+    wbox[warp][2] = b2;
+    wbox[warp][3] = b3;
+  }
+  __syncthreads();
+  if (t == 0) {
+    double x0 = wbox[0][0], x1 = wbox[0][1], y0 = wbox[0][2], y1 = wbox[0][3];
+    for (int w = 1; w < 4; ++w) {
+      x0 = fmin(x0, wbox[w][0]);
+      x1 = fmax(x1, wbox[w][1]);
+      y0 = fmin(y0, wbox[w][2]);
+      y1 = fmax(y1, wbox[w][3]);
+    }
+    G.box[0] = x0;
+    G.box[1] = x1;
+    G.box[2] = y0;
+    G.box[3] = y1;
+    G.any = x0 <= x1 ? 1 : 0;
+    G.q[0] = 0;
+    G.qhead = 0;
+    G.qtail = 1;
+    G.nfar = G.nleaf = G.nbig = G.nmixed = 0;
+    G.done = 0;
+  }
+  __syncthreads();
+  if (!G.any) return;
+  walk_group(a.tree, sxy + 2 * t, valid, acc, G);
   if (!valid) return;
-  // LensHaloParticles::force_halo negates alpha (particle_halo.h:432-433) and
-  // LensPlaneSingular::force subtracts it
   double al0 = acc[0], al1 = acc[1], kap = acc[2], g0 = acc[3], g1 = acc[4];
   const PlaneDev &P = a.planes[a.j];
   for (int h = 0; h < P.nhalo; ++h) {
@@ -681,76 +724,11 @@ __device__ __forceinline__ void plane_step_split_ptree(const StepArgs &a, double
   recursion_step(a, k, al0, al1, kap, g0, g1);
 }
 
-// Split-form plane step for a plane holding exactly one particle halo (its
-// tree in a.tree, a kernel parameter) and any number of analytic halos, two
-// rays per thread: slots 2g and 2g + 1 (g the thread's global index;
-// neighbours in the Morton order, so a warp walks 64 neighbouring rays),
-// walked together by walk_split2.  Only the slots stay live across the walk:
-// the rays' FP64 totals (stride 5 in two halves: a half-warp's 64-bit
-// accesses on distinct banks) and their plane positions sit in shared memory,
-// and the recursion reloads theta, the plane constants and the source-plane
-// scalars after the walk.  The particle halo's terms are added first, then
-// the analytic halos' in insertion order.
-__device__ __forceinline__ void plane_step_split_ptree2(const StepArgs &a, double *sacc, double *sxy) {
-  const size_t g = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  const size_t k0 = 2 * g, k1 = 2 * g + 1;
-  const bool in0 = k0 < a.n, in1 = k1 < a.n;
-  const int jmax0 = (a.jmax_ray && in0) ? a.jmax_ray[k0] : a.jmax;
-  const int jmax1 = (a.jmax_ray && in1) ? a.jmax_ray[k1] : a.jmax;
-  const bool v0 = in0 && a.j < jmax0, v1 = in1 && a.j < jmax1;
-  if (!__any_sync(kFull, v0 || v1)) return;
-  double *acc0 = sacc + 5 * threadIdx.x, *acc1 = sacc + 5 * (blockDim.x + threadIdx.x);
-  double *rxy = sxy + 4 * threadIdx.x;
-  for (int c = 0; c < 5; ++c) acc0[c] = acc1[c] = 0.0;
-  const double D = a.planes[a.j].Dphys;
-  rxy[0] = v0 ? a.st[k0] * D - a.tree_px : 0.0;
-  rxy[1] = v0 ? a.st[a.n + k0] * D - a.tree_py : 0.0;
-  rxy[2] = v1 ? a.st[k1] * D - a.tree_px : 0.0;
-  rxy[3] = v1 ? a.st[a.n + k1] * D - a.tree_py : 0.0;
-  walk_split2(a.tree, rxy, v0, v1, acc0, acc1);
-  for (int r = 0; r < 2; ++r) {
-    const bool v = r ? v1 : v0;
-    if (!v) continue;
-    const size_t k = r ? k1 : k0;
-    const double *acc = r ? acc1 : acc0;
-    double al0 = acc[0], al1 = acc[1], kap = acc[2], g0 = acc[3], g1 = acc[4];
-    const PlaneDev &P = a.planes[a.j];
-    for (int h = 0; h < P.nhalo; ++h) {
-      const HaloDev *H = a.halos + P.halo0 + h;
-      if (H->kind == HALO_PARTICLES) continue;
-      const Force5 f = analytic_halo(H, &a.tab, a.st[k] * P.Dphys - H->px, a.st[a.n + k] * P.Dphys - H->py);
-      al0 -= f.a0;
-      al1 -= f.a1;
-      kap += f.k;
-      g0 += f.g0;
-      g1 += f.g1;
-    }
-    recursion_step(a, k, al0, al1, kap, g0, g1);
-  }
-}
-
-// Two rays per thread: n / 2 threads (rounded up), blocks of 128, capped at
-// 80 registers (6 blocks per SM).  Measured on the light cone against one ray
-// per thread at 64 registers: 748 against 771 ms per step; 64 / 72 registers:
-// 966 / 795 ms (spills), 96 / 116 registers (before the shared offset):
-// 760 / 898 ms.
-__global__ void __launch_bounds__(128, 6) k_plane_step_split2(const __grid_constant__ StepArgs a) {
-  __shared__ double sacc[10 * 128];
-  __shared__ double sxy[4 * 128];
-  plane_step_split_ptree2(a, sacc, sxy);
-}
-
-// PTREE: the plane holds exactly one particle halo, whose tree is a.tree (no
-// field plane), one ray per thread; otherwise planes with several particle
-// halos or a field plane.
-template <bool FIELD = false, bool PTREE = false>
+// Split-form plane step of planes with several particle halos or a field
+// plane, one ray per thread.
+template <bool FIELD = false>
 __global__ void __launch_bounds__(128, 8) k_plane_step_split(const __grid_constant__ StepArgs a) {
-  if (PTREE) {
-    __shared__ double sacc[5 * 128];
-    plane_step_split_ptree(a, sacc);
-  } else {
-    plane_step<GLB_PREC_SPLIT, false, FIELD>(a);
-  }
+  plane_step<GLB_PREC_SPLIT, false, FIELD>(a);
 }
 
 // force2D_recur / force_halo at arbitrary positions (walk-level API, with phi).
@@ -801,7 +779,7 @@ __device__ __forceinline__ void tree_force(const TreeDev &T, size_t n, const dou
     x1 = x[2 * k + 1];
   }
   double acc[6] = {0, 0, 0, 0, 0, 0};
-  particle_halo_acc<PREC, false>(T, x0, x1, valid, acc);
+  particle_halo_acc<PREC, false, false, false, false>(T, x0, x1, valid, acc);  // a flush per opened leaf
   if (!valid) return;
   for (int c = 0; c < 5; ++c) out[5 * k + c] = acc[c];
 }
@@ -820,8 +798,9 @@ __global__ void __launch_bounds__(128, 6) k_tree_force_lo(const __grid_constant_
 // The split form with two rays per thread (rays 2g and 2g + 1; a warp walks
 // 64 rays, sharing node rows, votes and leaf particles between each pair),
 // the rays' positions and FP64 totals in shared memory.  Rays come in the
-// caller's order, so each ray forms its own double-float offsets
-// (walk_split2<false>): every result is bit-identical to k_tree_force_lo's.
+// caller's order; each ray forms its own double-float offsets and sums each
+// opened leaf on its own (walk_split2): every result is bit-identical to
+// k_tree_force_lo's.
 __global__ void __launch_bounds__(128, 6) k_tree_force_split2(const __grid_constant__ TreeDev T, size_t n,
                                                               const double *x, double *out) {
   __shared__ double sacc[10 * 128];
@@ -837,7 +816,7 @@ __global__ void __launch_bounds__(128, 6) k_tree_force_split2(const __grid_const
   rxy[1] = v0 ? x[2 * k0 + 1] : 0.0;
   rxy[2] = v1 ? x[2 * k1] : 0.0;
   rxy[3] = v1 ? x[2 * k1 + 1] : 0.0;
-  walk_split2<false>(T, rxy, v0, v1, acc0, acc1);
+  walk_split2(T, rxy, v0, v1, acc0, acc1);
   if (v0)
     for (int c = 0; c < 5; ++c) out[5 * k0 + c] = acc0[c];
   if (v1)
@@ -1107,17 +1086,12 @@ int ensure_ws(LensWS *w, size_t n, bool per_ray) {
 }
 
 // One launch per plane, in order.  Split-form planes that hold exactly one
-// particle halo and no field plane pass the tree in the kernel parameters:
-// k_plane_step_split2 (two rays per thread) in calls of kTwoRayMin rays or
-// more, below that the one-ray instance, which fills more of the GPU with a
-// small grid (512^2 rays on one plane: 45M rays/s against 35M); planes with a
-// field plane use the FIELD instances.
-constexpr size_t kTwoRayMin = (size_t)1 << 20;
-// pairs: two rays per thread on single-particle-halo planes (the caller's
-// choice, from the size of the whole call, so that a call cut into slabs
-// pairs its rays as an uncut one would)
+// particle halo and no field plane run the group walk (k_plane_step_split_g,
+// the tree in the kernel parameters); planes with a field plane use the FIELD
+// instances.
+constexpr size_t kTwoRayMin = (size_t)1 << 20;  // two-ray tree-force kernel from this many rays on
 int launch_plane_steps(const glb_lens *l, StepArgs &a, int jmax_launch, int precision, cudaStream_t s,
-                       const unsigned long long *d_counts, bool pairs) {
+                       const unsigned long long *d_counts) {
   const size_t n = a.n;
   for (int j = 0; j < jmax_launch; ++j) {
     a.j = j;
@@ -1143,10 +1117,8 @@ int launch_plane_steps(const glb_lens *l, StepArgs &a, int jmax_launch, int prec
       k_plane_step<GLB_PREC_FP64, true><<<nblk(n, 128), 128, 0, s>>>(a);
     else if (precision == GLB_PREC_SPLIT && fld)
       k_plane_step_split<true><<<nblk(n, 128), 128, 0, s>>>(a);
-    else if (precision == GLB_PREC_SPLIT && ptree && pairs)
-      k_plane_step_split2<<<nblk((n + 1) / 2, 128), 128, 0, s>>>(a);
     else if (precision == GLB_PREC_SPLIT && ptree)
-      k_plane_step_split<false, true><<<nblk(n, 128), 128, 0, s>>>(a);
+      k_plane_step_split_g<<<nblk(n, 128), 128, 0, s>>>(a);
     else if (precision == GLB_PREC_SPLIT)
       k_plane_step_split<<<nblk(n, 128), 128, 0, s>>>(a);
     else if (fld)
@@ -1164,8 +1136,9 @@ int launch_plane_steps(const glb_lens *l, StepArgs &a, int jmax_launch, int prec
 // launches depend only on its own earlier ones, so while one slab's launch
 // drains its last blocks the other slab's blocks fill the idle SMs, and the
 // per-plane launch tails overlap instead of adding up.  Measured on the
-// 2048^2 light cone (split form): 740 ms per step in one piece, 728 ms in two
-// slabs, 729 ms in four; results bit-identical.
+// 2048^2 light cone (split form) with the two-ray walk: 740 ms per step in one
+// piece, 728 ms in two slabs, 729 ms in four; with the group walk 647 ms in
+// one piece, 644 ms in two; results bit-identical.
 constexpr int kMaxSlabs = 2;
 constexpr size_t kSlabMin = (size_t)1 << 20;
 
@@ -1261,7 +1234,7 @@ int rayshoot_device(glb_lens *l, LensWS *w, size_t n, const double *x, const dou
     ai.n = mi;
     ai.jmax_ray = zs ? w->jmax_ray.p + o : nullptr;
     ai.src_ray = zs ? w->src_ray.p + 2 * o : nullptr;
-    if (int rc = launch_plane_steps(l, ai, jmax_launch, precision, si, d_counts, n >= kTwoRayMin)) return rc;
+    if (int rc = launch_plane_steps(l, ai, jmax_launch, precision, si, d_counts)) return rc;
     k_finish<<<nblk(mi, 256), 256, 0, si>>>(ai.st, w->perm.p + o, mi, y, A, status, skip);
     if (i > 0) {
       CKR(cudaEventRecord(w->join[i - 1], si));
@@ -2528,7 +2501,7 @@ extern "C" int glb_lens_rayshoot_noalloc(glb_lens *l, size_t n, const double *x_
       jmax_launch = jm;
     }
   }
-  if (int rc = launch_plane_steps(l, a, jmax_launch, precision, s, nullptr, n >= kTwoRayMin)) return rc;
+  if (int rc = launch_plane_steps(l, a, jmax_launch, precision, s, nullptr)) return rc;
   k_finish<<<nblk(n, 256), 256, 0, s>>>(st, perm, n, y_dev, A_dev);
   CKR(cudaGetLastError());
   CKR(cudaEventRecord(g_noalloc_ev[l->device], s));

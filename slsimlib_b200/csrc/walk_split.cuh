@@ -189,7 +189,11 @@ __device__ __forceinline__ void bspline_f32(float x0, float x1, float r, float M
 // nodes with big particles).  Same results; it pays in the batched kernel
 // (+1.1 % on 256 uneven lenses) but makes the one-ray plane step spill far
 // more (45M -> 27M rays/s on a 512^2 single plane), so only k_batch sets it.
-template <bool PURE = false, bool SKIPNEAR = false>
+// MERGE: far leaves join the running partial sums (below); without it every
+// opened leaf is summed on its own, flushed before and after (the one-ray
+// tree-force kernel: merging made it spill 232 / 420 B against 76 / 192 B and
+// run 9 % slower at opening angle 0.3).
+template <bool PURE = false, bool SKIPNEAR = false, bool MERGE = true>
 __device__ __forceinline__ void walk_split(const TreeDev &T, double rx, double ry, bool valid, double *acc) {
   const bool screen = T.screen2 != 0.0;
   const float s2f = (float)T.screen2;
@@ -269,7 +273,7 @@ __device__ __forceinline__ void walk_split(const TreeDev &T, double rx, double r
       // partial sum with other leaves' (merging those too raised the kappa
       // p99.9 of a softened, sheeted tree from under 1e-5 to 1.4e-5).
       // Leaves of more than 32 particles go in chunks of 32.
-      if (!PURE && open && (nearc ? fa.cnt > 0 : fa.cnt + min(c3.w, 32) > 32)) fa.flush(acc);
+      if (!PURE && open && ((nearc || !MERGE) ? fa.cnt > 0 : fa.cnt + min(c3.w, 32) > 32)) fa.flush(acc);
       for (int q0 = p0; q0 < p1; q0 += 32) {
         const int q1 = min(q0 + 32, p1);
 #pragma unroll 2  // two independent particles in flight (measured: 6.6 % faster at 64 registers)
@@ -326,7 +330,7 @@ __device__ __forceinline__ void walk_split(const TreeDev &T, double rx, double r
         }
         if (!PURE && open) {
           fa.cnt += q1 - q0;
-          if (nearc || q1 < p1) fa.flush(acc);
+          if (nearc || !MERGE || q1 < p1) fa.flush(acc);
         }
       }
       node = skip;
@@ -369,27 +373,8 @@ __device__ __forceinline__ void walk_split(const TreeDev &T, double rx, double r
   }
 }
 
-// The split walk for two rays per lane (a warp walks 64 neighbouring rays):
-// each ray keeps its own opening decisions, partial sums and resume point as
-// walk_split<false> does for one, while the node rows, the warp vote, the
-// loop control and the leaf particles are loaded and executed once for both.
-// DELTA (rays in spatial order, as the plane steps sort them): the second
-// ray's offset to a node is the first's plus the constant difference of the
-// two rays (d1 = d0 + del, del = r0 - r1 rounded to FP32: one packed add
-// instead of a double-float offset).  Its error per component is at most
-// about 2^-23 (|d1| + |del|), so the error of its squared distance is at most
-// about 2^-23 sqrt(2) (r2 + |del|^2) (2 |d1| |del| <= r2 + |del|^2).  The
-// second ray's opening tests widen the ambiguity band by four times that,
-// 2^-20 (r2 + |del|^2): a pair of neighbouring rays (|del| small against the
-// cells it opens) almost never needs the FP64 test more often than one ray,
-// and a pair far apart (a jump in the rays' order) takes it where its FP32
-// offset cannot decide, so every ray's interaction set is that of the FP64
-// form.  The terms themselves carry the extra 2^-23 |del| in their offsets,
-// harmless for neighbouring rays (a grid spacing against the softening
-// length) but not for rays in arbitrary order, so callers without a spatial
-// order use DELTA = false: both rays form double-float offsets and the second
-// ray's result is bit-identical to walk_split<false>'s.  rxy: {rx0, ry0, rx1,
-// ry1} (the rays' FP64 positions); acc0 / acc1: the rays' FP64 totals.
+// One far-field term (monopole + quadrupole, quadTree.h:1090-1123) into the
+// FP32 partial sums, flushed every 32 terms.
 __device__ __forceinline__ void far_term(const float4 &c1, const float4 &c2, float2 d, float r2f, bool screen,
                                          float ns2l, float piaf, F32Acc &fa, double *acc) {
   const float scr = screen ? ex2_approx(r2f * ns2l) : 1.0f;
@@ -406,6 +391,10 @@ __device__ __forceinline__ void far_term(const float4 &c1, const float4 &c2, flo
   if (++fa.cnt >= 32) fa.flush(acc);
 }
 
+// One leaf particle for one ray (the split forms of quadTree.h:1017-1077):
+// FP64 where the particle (nearly) coincides with the ray or its correction
+// belongs to an ancestor, the closed-form softened mass within two softening
+// lengths of a near leaf, else the point mass.
 __device__ __forceinline__ void leaf_term(const TreeDev &T, float4 P, int p, float2 d, const double *rxy, bool nearc,
                                           bool screen, float s2f, float ns2l, float piaf, bool sheet, float wu,
                                           int node, F32Acc &fa, double *acc) {
@@ -438,7 +427,15 @@ __device__ __forceinline__ void leaf_term(const TreeDev &T, float4 P, int p, flo
   if (sheet) fa.a = __ffma2_rn(f2(-piaf * P.z), x, fa.a);
 }
 
-template <bool DELTA = true>
+// The split walk for two rays per lane (a warp walks 64 neighbouring rays):
+// each ray keeps its own opening decisions, partial sums and resume point as
+// walk_split<false> does for one, while the node rows, the warp vote, the
+// loop control and the leaf particles are loaded and executed once for both.
+// Each ray forms its own double-float offsets, so its terms, decisions and
+// FP64 totals are walk_split<false, false, false>'s: a leaf opened by a ray is
+// summed on its own, flushed before and after, and the results are
+// bit-identical to the one-ray walk's.  rxy: {rx0, ry0, rx1, ry1} (the rays'
+// FP64 positions); acc0 / acc1: the rays' FP64 totals.
 __device__ __forceinline__ void walk_split2(const TreeDev &T, const double *rxy, bool valid0, bool valid1,
                                             double *acc0, double *acc1) {
   const bool screen = T.screen2 != 0.0;
@@ -447,15 +444,13 @@ __device__ __forceinline__ void walk_split2(const TreeDev &T, const double *rxy,
   const bool closed = T.sheet_closed;
   const bool sheet = T.inv_area != 0.0 && !closed;
   const float piaf = sheet ? (float)(kPi * T.inv_area) : 0.f;
-  float2 nrh[2], nrl[2];  // negated rays, hi and lo (the second only without DELTA)
-  for (int r = 0; r < (DELTA ? 1 : 2); ++r) {
+  float2 nrh[2], nrl[2];  // negated rays, hi and lo
+  for (int r = 0; r < 2; ++r) {
     const double rx = rxy[2 * r], ry = rxy[2 * r + 1];
     const float rxh = (float)rx, ryh = (float)ry;
     nrh[r] = make_float2(-rxh, -ryh);
     nrl[r] = make_float2(-(float)(rx - (double)rxh), -(float)(ry - (double)ryh));
   }
-  const float2 del = DELTA ? make_float2((float)(rxy[0] - rxy[2]), (float)(rxy[1] - rxy[3])) : make_float2(0.f, 0.f);
-  const float dband = DELTA ? 0x1p-20f * fmaf(del.x, del.x, del.y * del.y) : 0.f;  // the pair's widening of the band
   F32Acc fa0, fa1;
   fa0.zero();
   fa1.zero();
@@ -470,7 +465,7 @@ __device__ __forceinline__ void walk_split2(const TreeDev &T, const double *rxy,
     const bool act0 = node >= resume0, act1 = node >= resume1;
     const float2 cc = make_float2(c0.x, c0.y), cl = make_float2(c0.z, c0.w);
     const float2 d0 = __fadd2_rn(__fadd2_rn(cc, nrh[0]), __fadd2_rn(cl, nrl[0]));
-    const float2 d1 = DELTA ? __fadd2_rn(d0, del) : __fadd2_rn(__fadd2_rn(cc, nrh[1]), __fadd2_rn(cl, nrl[1]));
+    const float2 d1 = __fadd2_rn(__fadd2_rn(cc, nrh[1]), __fadd2_rn(cl, nrl[1]));
     const float2 dd0 = __fmul2_rn(d0, d0), dd1 = __fmul2_rn(d1, d1);
     const float r2f0 = dd0.x + dd0.y, r2f1 = dd1.x + dd1.y;
     bool open0 = false, open1 = false;
@@ -479,11 +474,10 @@ __device__ __forceinline__ void walk_split2(const TreeDev &T, const double *rxy,
       open0 = e < 0.f;
       if (fabsf(e) <= c1.w) open0 = node_test_f64(T.nodes + node, rxy[0], rxy[1], 0);
     }
-    const float xb1 = DELTA ? fmaf(r2f1, 0x1p-20f, dband) : 0.f;  // the second ray's extra band
     if (act1) {
       const float e = r2f1 - c1.x;
       open1 = e < 0.f;
-      if (fabsf(e) <= (DELTA ? c1.w + xb1 : c1.w)) open1 = node_test_f64(T.nodes + node, rxy[2], rxy[3], 0);
+      if (fabsf(e) <= c1.w) open1 = node_test_f64(T.nodes + node, rxy[2], rxy[3], 0);
     }
     const bool far0 = act0 && !open0, far1 = act1 && !open1;
     if (far0 || far1) {
@@ -504,7 +498,7 @@ __device__ __forceinline__ void walk_split2(const TreeDev &T, const double *rxy,
     bool nearc0 = false, nearc1 = false;
     // the near-field test matters at a leaf and at an internal node with big
     // particles (c3.w of them) only; skipping it elsewhere measured 1.3 %
-    // faster per light-cone step (the one-ray walk spills more when it skips)
+    // faster on the light-cone plane step when this walk served it
     const bool need_near = c3.y || c3.w > 0;
     if (open0 && need_near) {
       const float e = r2f0 - c1.y;
@@ -514,14 +508,13 @@ __device__ __forceinline__ void walk_split2(const TreeDev &T, const double *rxy,
     if (open1 && need_near) {
       const float e = r2f1 - c1.y;
       nearc1 = e < 0.f;
-      if (fabsf(e) <= (DELTA ? fmaf(kAmbiguous, c1.y, xb1) : kAmbiguous * c1.y))
-        nearc1 = node_test_f64(T.nodes + node, rxy[2], rxy[3], 1);
+      if (fabsf(e) <= kAmbiguous * c1.y) nearc1 = node_test_f64(T.nodes + node, rxy[2], rxy[3], 1);
     }
     if (c3.y) {  // leaf
       const int p0 = c3.z, p1 = p0 + c3.w;
       const float wu = __ldg(sp + 2).z;
-      if (open0 && (nearc0 ? fa0.cnt > 0 : fa0.cnt + min(c3.w, 32) > 32)) fa0.flush(acc0);
-      if (open1 && (nearc1 ? fa1.cnt > 0 : fa1.cnt + min(c3.w, 32) > 32)) fa1.flush(acc1);
+      if (open0 && fa0.cnt) fa0.flush(acc0);
+      if (open1 && fa1.cnt) fa1.flush(acc1);
       for (int q0 = p0; q0 < p1; q0 += 32) {
         const int q1 = min(q0 + 32, p1);
         for (int p = q0; p < q1; ++p) {
@@ -529,14 +522,8 @@ __device__ __forceinline__ void walk_split2(const TreeDev &T, const double *rxy,
           if (open0) leaf_term(T, P, p, d0, rxy, nearc0, screen, s2f, ns2l, piaf, sheet, wu, node, fa0, acc0);
           if (open1) leaf_term(T, P, p, d1, rxy + 2, nearc1, screen, s2f, ns2l, piaf, sheet, wu, node, fa1, acc1);
         }
-        if (open0) {
-          fa0.cnt += q1 - q0;
-          if (nearc0 || q1 < p1) fa0.flush(acc0);
-        }
-        if (open1) {
-          fa1.cnt += q1 - q0;
-          if (nearc1 || q1 < p1) fa1.flush(acc1);
-        }
+        if (open0) fa0.flush(acc0);
+        if (open1) fa1.flush(acc1);
       }
       node = skip;
     } else {
