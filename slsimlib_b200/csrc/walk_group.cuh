@@ -278,14 +278,18 @@ __device__ __forceinline__ void walk_group(const TreeDev &T, const double *rxy, 
         if (valid && (nearc ? fa.cnt > 0 : fa.cnt + min(c3.w, 32) > 32)) fa.flush(acc);
         for (int q0 = p0; q0 < p1; q0 += 32) {
           const int q1 = min(q0 + 32, p1);
+          // the chunk's particles, one per lane, into the warp's rows
+          if (q0 + lane < q1) wrow[lane] = __ldg(T.prel + q0 + lane);
+          __syncwarp();
           for (int p = q0; p < q1; ++p) {
-            const float4 P = __ldg(T.prel + p);
+            const float4 P = wrow[p - q0];
             if (valid) leaf_term(T, P, p, d, rxy, nearc, screen, s2f, ns2l, piaf, sheet, wu, node, fa, acc);
           }
           if (valid) {
             fa.cnt += q1 - q0;
             if (nearc || q1 < p1) fa.flush(acc);
           }
+          __syncwarp();
         }
       }
       // internal cells every ray opens that carry big particles
