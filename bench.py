@@ -41,9 +41,10 @@ FIELD_ARCSEC = 60.0
 # B-spline corrections S) and per ray-plane recursion
 FLOPS = {"V": 8, "F": 60, "P": 29, "B": 8, "S": 65, "rec": 50}
 # DRAM bytes (read + write) per ray of one split plane launch, from an ncu capture of
-# `bench.py --no-cpu --no-served --n1d 1536` (184.8 MB for one 1,179,648-ray slab of a
-# plane): the 96 B ray state read and written once and the plane's L2-resident tree
-DRAM_BYTES_PER_RAY_PLANE = 157
+# `bench.py --no-cpu --no-served --n1d 1536` (184.3 MB for one 1,179,648-ray slab of a
+# plane, k_plane_step_split_g): the 96 B ray state read and written once and the plane's
+# L2-resident tree
+DRAM_BYTES_PER_RAY_PLANE = 156
 
 
 def workload(small: bool):
@@ -765,7 +766,7 @@ def main():
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": DRAM_BYTES_PER_RAY_PLANE * n,
                          "traffic_note": "dram read+write bytes per plane (both slabs): ncu capture of one "
-                                         "1,179,648-ray slab launch at 1536^2 (157 B/ray) scaled by rays",
+                                         "1,179,648-ray slab launch at 1536^2 (156 B/ray) scaled by rays",
                          "kernel": "k_plane_step_split_g", "kernel_ms_per_step": k_ms,
                          "peak_note": "FP32 CUDA-core FMA rate at the sampled SM clock (148 SMs x 128 lanes x 2)",
                          "alg_flops_per_step": alg_flops,
