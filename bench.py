@@ -11,7 +11,7 @@ Lines printed by rank 0 (one JSON line):
          GPUs, inputs resident in HBM, CUDA events on the launching stream;
   e2e    the same metric through the host C ABI (glb_lens_rayshoot: host
          x in, host y and A out, copies inside the timed region);
-  roofline of the plane-step kernel (k_plane_step_split2; algorithmic FP32 flops from the counted
+  roofline of the plane-step kernel (k_plane_step_split_g; algorithmic FP32 flops from the counted
          interactions / kernel time vs the FP32 CUDA-core peak);
   cpu_baseline: the reference compiled in place (oracle/_ref) on host cores.
 

@@ -142,7 +142,8 @@ __device__ __forceinline__ bool group_classify(const TreeDev &T, GroupLists &G) 
 // split form only), adding into fa / acc.
 __device__ __forceinline__ void group_subtree(const TreeDev &T, const double *rxy, bool valid, float2 nrh, float2 nrl,
                                               int node0, int end, bool screen, float s2f, float ns2l, float piaf,
-                                              bool sheet, F32Acc &fa, double *acc) {
+                                              bool sheet, F32Acc &fa, double *acc, float4 *wrow) {
+  const int lane = threadIdx.x & 31;
   int resume = valid ? node0 : 0x7fffffff;
   int node = node0;
   while (node < end) {
@@ -180,14 +181,18 @@ __device__ __forceinline__ void group_subtree(const TreeDev &T, const double *rx
       if (open && (nearc ? fa.cnt > 0 : fa.cnt + min(c3.w, 32) > 32)) fa.flush(acc);
       for (int q0 = p0; q0 < p1; q0 += 32) {
         const int q1 = min(q0 + 32, p1);
+        // the whole warp is here (some lane opened the leaf): stage its particles
+        if (q0 + lane < q1) wrow[lane] = __ldg(T.prel + q0 + lane);
+        __syncwarp();
         for (int p = q0; p < q1; ++p) {
-          const float4 P = __ldg(T.prel + p);
+          const float4 P = wrow[p - q0];
           if (open) leaf_term(T, P, p, d, rxy, nearc, screen, s2f, ns2l, piaf, sheet, wu, node, fa, acc);
         }
         if (open) {
           fa.cnt += q1 - q0;
           if (nearc || q1 < p1) fa.flush(acc);
         }
+        __syncwarp();
       }
       node = skip;
     } else {
@@ -322,7 +327,7 @@ __device__ __forceinline__ void walk_group(const TreeDev &T, const double *rxy, 
       // subtrees the rays disagree on: per-ray walks
       for (int i = 0; i < nmixed; ++i) {
         const int r = G.mixed[i];
-        group_subtree(T, rxy, valid, nrh, nrl, r, T.nodes[r].skip, screen, s2f, ns2l, piaf, sheet, fa, acc);
+        group_subtree(T, rxy, valid, nrh, nrl, r, T.nodes[r].skip, screen, s2f, ns2l, piaf, sheet, fa, acc, wrow);
       }
       __syncthreads();
       if (threadIdx.x == 0) G.nfar = G.nleaf = G.nbig = G.nmixed = 0;
