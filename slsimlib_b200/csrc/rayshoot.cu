@@ -1103,7 +1103,7 @@ int launch_plane_steps(const glb_lens *l, StepArgs &a, int jmax_launch, int prec
         ++npart;
         ph = h;
       }
-    const bool ptree = npart == 1 && ph->tree && !fld;
+    const bool ptree = npart == 1 && ph->tree && !fld && !ph->tree->dev.periodic;  // the group walk has no periodic images
     memset(&a.tree, 0, sizeof(a.tree));
     a.tree_px = a.tree_py = 0;
     if (ptree) {
