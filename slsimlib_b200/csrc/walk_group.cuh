@@ -14,10 +14,11 @@
 // at each: the interaction sets are those of the FP64 form.  The box tests
 // are FP64 with a relative margin of 1e-12 (far beyond the rounding of the
 // per-ray test), on the monotone distances of the box's nearest and farthest
-// points.  The other warps then evaluate the shared lists for their rays
-// without opening tests or votes; lists that fill up are evaluated and
-// cleared, and a queue that would overflow hands its cells to the per-ray
-// walks.  Each ray's terms are summed as by walk_split (FP32 partial sums of
+// points (restated and checked in tests/test_group_bounds.py).  All four
+// warps then evaluate the shared lists for their rays without opening tests
+// or votes, the cells' rows and the leaves' particles read through per-warp
+// shared memory; lists that fill up are evaluated and cleared, and a queue
+// that would overflow hands its cells to the per-ray walks.  Each ray's terms are summed as by walk_split (FP32 partial sums of
 // at most 32 terms, near leaves on their own), in the order of the lists.
 #pragma once
 #include "walk_split.cuh"
